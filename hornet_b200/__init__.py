@@ -1,0 +1,602 @@
+"""hornet_b200: B200-native Hornet dynamic-graph hot path.
+
+Python binding over the C ABI in include/hornet_b200.h (libhornet_b200.so,
+built in-tree by hornet_b200/build.py).  The classes mirror the reference's
+C++ names and argument meaning:
+
+* ``HornetInit`` / ``Hornet`` (``HornetGPU``): hornet::HornetInit and
+  hornet::gpu::Hornet (hornet/include/Core/Hornet.cuh:56-131);
+* ``BatchUpdate``: hornet::gpu::BatchUpdate over a BatchUpdatePtr
+  (hornet/include/Core/BatchUpdate/BatchUpdate.cuh:77-272);
+* ``BfsTopDown``, ``TriangleCounting2``, ``CC``, ``KTruss``: the
+  hornetsnest StaticAlgorithm subclasses (primitives/HornetAlg.cuh:51-150).
+
+Arrays are numpy arrays (host) or CUDA tensors / objects exposing
+``data_ptr()`` and ``is_cuda`` (device).  There is no CPU fallback: without
+the compiled library every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Tuple
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libhornet_b200.so")
+
+HN_OK = 0
+HN_ERR_INVALID = 1
+HN_ERR_OOM = 2
+HN_ERR_CAPACITY = 3
+HN_ERR_TIMEOUT = 4
+HN_ERR_CUDA = 5
+HN_ERR_STATE = 6
+
+HN_MEM_HOST = 0
+HN_MEM_DEVICE = 1
+HN_CSR_SORTED = 1
+HN_DEDUP_BATCH = 1
+HN_DEDUP_GRAPH = 2
+HN_CC_MIN_ID = 0
+HN_CC_REFERENCE = 1
+HN_LB_BINARY_SEARCH = 0
+HN_LB_VERTEX_BASED = 1
+
+INF = 2147483647
+
+
+class HornetError(RuntimeError):
+    """A C-ABI call returned an HN_ERR_* status."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class BfsStats(ctypes.Structure):
+    _fields_ = [("levels", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("visited", ctypes.c_int64), ("edges_scanned", ctypes.c_int64)]
+
+
+class DeviceView(ctypes.Structure):
+    _fields_ = [("nV", ctypes.c_int32), ("pad", ctypes.c_int32), ("nE", ctypes.c_int64),
+                ("vtab", ctypes.c_void_p), ("pool", ctypes.c_void_p)]
+
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_U32 = ctypes.c_uint32
+_U64 = ctypes.c_uint64
+_INT = ctypes.c_int
+_D = ctypes.c_double
+
+# name -> argtypes (all return int unless listed in _RESTYPES)
+_SIGNATURES = {
+    "hn_last_error_string": [],
+    "hn_version": [],
+    "hn_kernel_launches": [],
+    "hn_profile_enable": [_INT],
+    "hn_profile_report": [_P, _I64],
+    "hn_graph_create_csr": [_I32, _I64, _P, _P, _U32, _INT, _INT, _P],
+    "hn_graph_create_csr64": [_I32, _I64, _P, _P, _U32, _INT, _INT, _P],
+    "hn_graph_reset_csr": [_P, _I32, _I64, _P, _P, _U32, _INT],
+    "hn_graph_destroy": [_P],
+    "hn_graph_set_stream": [_P, _P],
+    "hn_graph_nv": [_P, _P],
+    "hn_graph_ne": [_P, _P],
+    "hn_graph_max_degree": [_P, _P, _P],
+    "hn_graph_export_coo": [_P, _INT, _P, _P, _INT],
+    "hn_graph_export_csr": [_P, _P, _P, _INT],
+    "hn_graph_degrees": [_P, _P, _INT],
+    "hn_graph_device_view": [_P, _P],
+    "hn_graph_memory": [_P, _P, _P, _P],
+    "hn_batch_create": [_P, _I64, _P, _P, _INT, _P],
+    "hn_batch_reset": [_P, _I64, _P, _P, _INT],
+    "hn_batch_size": [_P, _P],
+    "hn_batch_destroy": [_P],
+    "hn_insert": [_P, _P, _U32, _P],
+    "hn_erase": [_P, _P, _U32, _P],
+    "hn_bfs": [_P, _I32, _P, _INT, _P],
+    "hn_bfs_multi": [_P, _P, _I32, _P, _INT, _P],
+    "hn_tc": [_P, _P, _INT, _P],
+    "hn_cc": [_P, _INT, _P, _INT, _P],
+    "hn_ktruss": [_P, _P, _P, _INT],
+    "hn_for_all_edges_count": [_P, _P, _I32, _INT, _INT, _P],
+    "hn_for_all_vertices_degree": [_P, _P],
+    "hn_gen_rmat_host": [_I32, _I32, _I64, _D, _D, _D, _U64, _P, _P],
+    "hn_gen_rmat_device": [_I32, _I32, _I64, _D, _D, _D, _U64, _P, _P, _INT],
+    "hn_coo_to_csr_device": [_I32, _I64, _P, _P, _INT, _P, _P, _P],
+    "hn_free_device": [_P],
+}
+_RESTYPES = {"hn_last_error_string": ctypes.c_char_p, "hn_kernel_launches": _I64}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libhornet_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m hornet_b200.build`")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, ctypes.c_int)
+        _lib = l
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != HN_OK:
+        msg = lib().hn_last_error_string()
+        raise HornetError(rc, msg.decode() if msg else "")
+
+
+def last_error() -> str:
+    return lib().hn_last_error_string().decode()
+
+
+def kernel_launches() -> int:
+    return int(lib().hn_kernel_launches())
+
+
+def profile_enable(on: bool = True) -> None:
+    """Bracket every library kernel with CUDA events (clears old records)."""
+    _check(lib().hn_profile_enable(1 if on else 0))
+
+
+def profile_report() -> dict:
+    """{kernel: {"launches": n, "ms": total}} since profile_enable."""
+    import json
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check(lib().hn_profile_report(buf, len(buf)))
+    return json.loads(buf.value.decode())
+
+
+# ---------------------------------------------------------------------------
+# array plumbing
+# ---------------------------------------------------------------------------
+
+def _is_device(a) -> bool:
+    return bool(getattr(a, "is_cuda", False))
+
+
+def _ptr(a, dtype=None):
+    """(pointer, mem_kind, keepalive) for a numpy array or CUDA tensor."""
+    if a is None:
+        return None, HN_MEM_HOST, None
+    if _is_device(a):
+        return ctypes.c_void_p(a.data_ptr()), HN_MEM_DEVICE, a
+    arr = np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data_as(ctypes.c_void_p), HN_MEM_HOST, arr
+
+
+def _out_ptr(a):
+    if _is_device(a):
+        return ctypes.c_void_p(a.data_ptr()), HN_MEM_DEVICE
+    assert isinstance(a, np.ndarray) and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.c_void_p), HN_MEM_HOST
+
+
+# ---------------------------------------------------------------------------
+# graph + batches
+# ---------------------------------------------------------------------------
+
+class HornetInit:
+    """hornet::HornetInit(nV, nE, csr_offsets, csr_edges)
+    (hornet/include/Core/HornetInitialize/HornetInit.cuh:70-73).  Borrows
+    the CSR until a Hornet is built from it."""
+
+    def __init__(self, nV: int, nE: int, offsets, edges, sorted_adjacency: bool = False):
+        self._nV = int(nV)
+        self._nE = int(nE)
+        self.offsets = offsets
+        self.edges = edges
+        self.sorted = bool(sorted_adjacency)
+
+    def nV(self) -> int:
+        return self._nV
+
+    def nE(self) -> int:
+        return self._nE
+
+
+class Hornet:
+    """hornet::gpu::Hornet<int> (hornet/include/Core/Hornet.cuh:56-131)."""
+
+    def __init__(self, init: HornetInit, device: int = 0):
+        self._h = ctypes.c_void_p()
+        self._device = device
+        self._build(init, create=True)
+
+    def _build(self, init: HornetInit, create: bool) -> None:
+        off = init.offsets
+        if _is_device(off):
+            use64 = str(off.dtype).endswith("int64")
+        else:
+            off = np.asarray(off)
+            use64 = off.dtype == np.int64 or init.nE() > 0x7FFFFFFF
+            off = np.ascontiguousarray(off, dtype=np.int64 if use64 else np.int32)
+        po, mem, keep_o = _ptr(off)
+        pa, mem_a, keep_a = _ptr(init.edges, np.int32)
+        assert mem == mem_a, "offsets and edges must live in the same memory"
+        flags = HN_CSR_SORTED if init.sorted else 0
+        if create:
+            fn = lib().hn_graph_create_csr64 if use64 else lib().hn_graph_create_csr
+            _check(fn(init.nV(), init.nE(), po, pa, flags, mem, self._device,
+                      ctypes.byref(self._h)))
+        else:
+            assert not use64, "reset takes int32 offsets"
+            _check(lib().hn_graph_reset_csr(self._h, init.nV(), init.nE(), po, pa, flags, mem))
+
+    def reset(self, init: HornetInit) -> None:
+        """gpu::Hornet::reset(HornetInit&) (HornetInitialize.i.cuh:190-204)."""
+        self._build(init, create=False)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.hn_graph_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    release = __del__
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def nV(self) -> int:
+        v = ctypes.c_int32()
+        _check(lib().hn_graph_nv(self._h, ctypes.byref(v)))
+        return v.value
+
+    def nE(self) -> int:
+        v = ctypes.c_int64()
+        _check(lib().hn_graph_ne(self._h, ctypes.byref(v)))
+        return v.value
+
+    def _maxdeg(self) -> Tuple[int, int]:
+        d, i = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().hn_graph_max_degree(self._h, ctypes.byref(d), ctypes.byref(i)))
+        return d.value, i.value
+
+    def max_degree(self) -> int:
+        return self._maxdeg()[0]
+
+    def max_degree_id(self) -> int:
+        return self._maxdeg()[1]
+
+    def getCOO(self, sort: bool = True, src=None, dst=None):
+        """getCOO(sort): (src, dst) sorted lexicographically
+        (HornetQuery.i.cuh:67-109).  Pass CUDA tensors to keep it on device."""
+        n = self.nE()
+        if src is None:
+            src = np.empty(n, np.int32)
+            dst = np.empty(n, np.int32)
+        ps, mem = _out_ptr(src)
+        pd, _ = _out_ptr(dst)
+        _check(lib().hn_graph_export_coo(self._h, int(sort), ps, pd, mem))
+        return src, dst
+
+    get_coo = getCOO
+
+    def getCSR(self):
+        """getCSR(true): (offsets[nV+1], edges[nE]) host arrays."""
+        off = np.empty(self.nV() + 1, np.int32)
+        adj = np.empty(self.nE(), np.int32)
+        _check(lib().hn_graph_export_csr(self._h, off.ctypes.data_as(_P),
+                                         adj.ctypes.data_as(_P), HN_MEM_HOST))
+        return off, adj
+
+    get_csr = getCSR
+
+    def degrees(self):
+        d = np.empty(self.nV(), np.int32)
+        _check(lib().hn_graph_degrees(self._h, d.ctypes.data_as(_P), HN_MEM_HOST))
+        return d
+
+    def device(self) -> DeviceView:
+        v = DeviceView()
+        _check(lib().hn_graph_device_view(self._h, ctypes.byref(v)))
+        return v
+
+    def memory(self) -> Tuple[int, int, int]:
+        a, b, c = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _check(lib().hn_graph_memory(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
+
+    def insert(self, batch: "BatchUpdate", removeBatchDuplicates: bool = False,
+               removeGraphDuplicates: bool = False) -> int:
+        """gpu::Hornet::insert (hornet/include/Core/HornetOperations/
+        HornetInsert.i.cuh:12-27).  Returns the number of edges added."""
+        flags = (HN_DEDUP_BATCH if removeBatchDuplicates else 0) | \
+                (HN_DEDUP_GRAPH if removeGraphDuplicates else 0)
+        applied = ctypes.c_int64()
+        _check(lib().hn_insert(self._h, batch.handle, flags, ctypes.byref(applied)))
+        return applied.value
+
+    def erase(self, batch: "BatchUpdate", removeBatchDuplicates: bool = False) -> int:
+        """gpu::Hornet::erase (HornetInsert.i.cuh:71-89).  Returns the number
+        of edges removed."""
+        flags = HN_DEDUP_BATCH if removeBatchDuplicates else 0
+        applied = ctypes.c_int64()
+        _check(lib().hn_erase(self._h, batch.handle, flags, ctypes.byref(applied)))
+        return applied.value
+
+
+HornetGPU = Hornet
+
+
+class BatchUpdate:
+    """gpu::BatchUpdate built from a BatchUpdatePtr<HOST|DEVICE>(n, src, dst)
+    (BatchUpdate.cuh:91-99); the batch owns a device copy."""
+
+    def __init__(self, hornet: Hornet, src, dst):
+        self._hornet = hornet
+        self._h = ctypes.c_void_p()
+        ps, mem, ks = _ptr(src, np.int32)
+        pd, _, kd = _ptr(dst, np.int32)
+        n = len(src) if not _is_device(src) else int(src.numel())
+        _check(lib().hn_batch_create(hornet.handle, n, ps, pd, mem, ctypes.byref(self._h)))
+
+    def reset(self, src, dst) -> None:
+        ps, mem, ks = _ptr(src, np.int32)
+        pd, _, kd = _ptr(dst, np.int32)
+        n = len(src) if not _is_device(src) else int(src.numel())
+        _check(lib().hn_batch_reset(self._h, n, ps, pd, mem))
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        return self._h
+
+    def size(self) -> int:
+        n = ctypes.c_int64()
+        _check(lib().hn_batch_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    nE = size
+
+    def __del__(self):
+        if getattr(self, "_h", None) and self._h.value and _lib is not None:
+            _lib.hn_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+
+# ---------------------------------------------------------------------------
+# StaticAlgorithm family (primitives/HornetAlg.cuh:51-150)
+# ---------------------------------------------------------------------------
+
+class StaticAlgorithm:
+    def __init__(self, hornet: Hornet):
+        self.hornet = hornet
+
+    def run(self):
+        raise NotImplementedError
+
+    def reset(self):
+        raise NotImplementedError
+
+    def release(self):
+        pass
+
+    def validate(self) -> bool:
+        raise NotImplementedError
+
+
+class BfsTopDown(StaticAlgorithm):
+    """hornetsnest BfsTopDown (TopDown.cuh:52-70): set_parameters(src), run().
+    validate() checks against the CPU oracle when it is importable (the
+    reference's own validate() is a stub returning true, TopDown.cu:113-128)."""
+
+    def __init__(self, hornet: Hornet):
+        super().__init__(hornet)
+        self.source = 0
+        self.distances: Optional[np.ndarray] = None
+        self.stats = BfsStats()
+
+    def reset(self):
+        self.distances = None
+
+    def set_parameters(self, source: int):
+        self.source = int(source)
+
+    def run(self, out=None):
+        n = self.hornet.nV()
+        if out is None:
+            out = np.empty(n, np.int32)
+        p, mem = _out_ptr(out)
+        _check(lib().hn_bfs(self.hornet.handle, self.source, p, mem, ctypes.byref(self.stats)))
+        self.distances = out
+        return out
+
+    def run_multi(self, sources, out=None):
+        srcs = np.ascontiguousarray(sources, np.int32)
+        n = self.hornet.nV()
+        if out is None:
+            out = np.empty((len(srcs), n), np.int32)
+        p, mem = _out_ptr(out)
+        stats = (BfsStats * max(1, len(srcs)))()
+        _check(lib().hn_bfs_multi(self.hornet.handle, srcs.ctypes.data_as(_P), len(srcs), p, mem,
+                                  stats))
+        return out, [stats[i] for i in range(len(srcs))]
+
+    def getLevels(self) -> int:
+        return self.stats.levels
+
+
+class TriangleCounting2(StaticAlgorithm):
+    """hornetsnest TriangleCounting2 (triangle2.cuh:18-37): init(), run(),
+    countTriangles(), copyTCToHost()."""
+
+    def __init__(self, hornet: Hornet):
+        super().__init__(hornet)
+        self._per_vertex = None
+        self._total = 0
+
+    def init(self):
+        self.reset()
+
+    def reset(self):
+        self._per_vertex = None
+        self._total = 0
+
+    def run(self, per_vertex: bool = False):
+        total = ctypes.c_uint64()
+        if per_vertex:
+            pv = np.empty(self.hornet.nV(), np.uint64)
+            _check(lib().hn_tc(self.hornet.handle, pv.ctypes.data_as(_P), HN_MEM_HOST,
+                               ctypes.byref(total)))
+            self._per_vertex = pv
+        else:
+            _check(lib().hn_tc(self.hornet.handle, None, HN_MEM_HOST, ctypes.byref(total)))
+        self._total = total.value
+        return self._total
+
+    def countTriangles(self) -> int:
+        return self._total
+
+    def copyTCToHost(self):
+        if self._per_vertex is None:
+            self.run(per_vertex=True)
+        return self._per_vertex
+
+
+class CC(StaticAlgorithm):
+    """hornetsnest CC (CC.cuh:53-69).  labels: min vertex id per component;
+    reference_colors(): the colours CC::run itself produces."""
+
+    def __init__(self, hornet: Hornet):
+        super().__init__(hornet)
+        self.labels: Optional[np.ndarray] = None
+        self.n_components = 0
+
+    def reset(self):
+        self.labels = None
+
+    def run(self, mode: int = HN_CC_MIN_ID, out=None):
+        n = self.hornet.nV()
+        if out is None:
+            out = np.empty(n, np.int32)
+        p, mem = _out_ptr(out)
+        nc = ctypes.c_int32()
+        _check(lib().hn_cc(self.hornet.handle, mode, p, mem, ctypes.byref(nc)))
+        self.n_components = nc.value
+        if mode == HN_CC_MIN_ID:
+            self.labels = out
+        return out
+
+    def reference_colors(self):
+        return self.run(HN_CC_REFERENCE)
+
+
+class KTruss(StaticAlgorithm):
+    """hornetsnest KTruss (KTruss.cuh:43-78): run(), getMaxK(); edge_truss
+    holds the truss number of every edge in sorted-COO order."""
+
+    def __init__(self, hornet: Hornet):
+        super().__init__(hornet)
+        self.max_k = 0
+        self.edge_truss: Optional[np.ndarray] = None
+
+    def init(self):
+        self.reset()
+
+    def reset(self):
+        self.max_k = 0
+        self.edge_truss = None
+
+    def run(self):
+        k = ctypes.c_int32()
+        et = np.empty(self.hornet.nE(), np.int32)
+        _check(lib().hn_ktruss(self.hornet.handle, ctypes.byref(k), et.ctypes.data_as(_P),
+                               HN_MEM_HOST))
+        self.max_k = k.value
+        self.edge_truss = et
+        return self.max_k
+
+    def getMaxK(self) -> int:
+        return self.max_k
+
+
+# ---------------------------------------------------------------------------
+# operator primitives with built-in operators
+# ---------------------------------------------------------------------------
+
+def for_all_edges_count(hornet: Hornet, out, vertices=None, lb: int = HN_LB_BINARY_SEARCH,
+                        vw: int = 1) -> None:
+    """forAllEdges(hornet, vertices, op=count-dst, lb) into the device int32
+    tensor `out` (accumulated)."""
+    pv, mem, keep = _ptr(vertices, np.int32)
+    n = 0 if vertices is None else (int(vertices.numel()) if _is_device(vertices) else len(vertices))
+    if vertices is not None:
+        assert mem == HN_MEM_DEVICE, "vertices must be a device array"
+    _check(lib().hn_for_all_edges_count(hornet.handle, pv, n, lb, vw, ctypes.c_void_p(out.data_ptr())))
+
+
+def for_all_vertices_degree(hornet: Hornet, out) -> None:
+    _check(lib().hn_for_all_vertices_degree(hornet.handle, ctypes.c_void_p(out.data_ptr())))
+
+
+# ---------------------------------------------------------------------------
+# synthetic inputs
+# ---------------------------------------------------------------------------
+
+RMAT_A, RMAT_B, RMAT_C = 0.57, 0.19, 0.19
+
+
+def gen_rmat_host(scale: int, n_pairs: int, seed: int, n_vertices: Optional[int] = None,
+                  a: float = RMAT_A, b: float = RMAT_B, c: float = RMAT_C):
+    """R-MAT pairs on the host; identical to gen_rmat_device."""
+    n = n_vertices if n_vertices is not None else (1 << scale)
+    src = np.empty(n_pairs, np.int32)
+    dst = np.empty(n_pairs, np.int32)
+    _check(lib().hn_gen_rmat_host(scale, n, n_pairs, a, b, c, seed & (2**64 - 1),
+                                  src.ctypes.data_as(_P), dst.ctypes.data_as(_P)))
+    return src, dst
+
+
+def gen_rmat_device(scale: int, n_pairs: int, seed: int, src, dst, n_vertices: Optional[int] = None,
+                    a: float = RMAT_A, b: float = RMAT_B, c: float = RMAT_C, device: int = 0):
+    n = n_vertices if n_vertices is not None else (1 << scale)
+    _check(lib().hn_gen_rmat_device(scale, n, n_pairs, a, b, c, seed & (2**64 - 1),
+                                    ctypes.c_void_p(src.data_ptr()),
+                                    ctypes.c_void_p(dst.data_ptr()), device))
+
+
+class DeviceCSR:
+    """Undirected CSR built on the device (owns two cudaMalloc buffers)."""
+
+    def __init__(self, nV: int, off_ptr: int, adj_ptr: int, nE: int):
+        self.nV, self.nE = nV, nE
+        self.off_ptr, self.adj_ptr = off_ptr, adj_ptr
+
+    def __del__(self):
+        if _lib is not None:
+            for p in (self.off_ptr, self.adj_ptr):
+                if p:
+                    _lib.hn_free_device(ctypes.c_void_p(p))
+            self.off_ptr = self.adj_ptr = 0
+
+
+def coo_to_csr_device(nV: int, src, dst, device: int = 0) -> DeviceCSR:
+    po, pa, ne = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_int64()
+    _check(lib().hn_coo_to_csr_device(nV, int(src.numel()), ctypes.c_void_p(src.data_ptr()),
+                                      ctypes.c_void_p(dst.data_ptr()), device, ctypes.byref(po),
+                                      ctypes.byref(pa), ctypes.byref(ne)))
+    return DeviceCSR(nV, po.value or 0, pa.value or 0, ne.value)
+
+
+def hornet_from_device_csr(csr: DeviceCSR, device: int = 0) -> Hornet:
+    """Build a Hornet straight from a DeviceCSR (sorted, int32 offsets)."""
+    h = Hornet.__new__(Hornet)
+    h._h = ctypes.c_void_p()
+    h._device = device
+    _check(lib().hn_graph_create_csr(csr.nV, csr.nE, ctypes.c_void_p(csr.off_ptr),
+                                     ctypes.c_void_p(csr.adj_ptr), HN_CSR_SORTED, HN_MEM_DEVICE,
+                                     device, ctypes.byref(h._h)))
+    return h

@@ -1,0 +1,178 @@
+// Internal graph / batch objects behind the C ABI handles.
+#pragma once
+
+#include <atomic>
+#include <cstddef>
+#include <cstdint>
+
+#include "hn_internal.cuh"
+
+namespace hn {
+
+void count_launch(int n = 1);
+
+// Optional per-kernel timing with CUDA events recorded on the launching
+// stream (enabled by hn_profile_enable; off by default).
+extern bool g_profiling;
+void profile_begin(cudaStream_t s, cudaEvent_t* a);
+void profile_end(const char* name, cudaStream_t s, cudaEvent_t a);
+
+// Launch a kernel on `stream` and count it.  Grids of size 0 are skipped.
+#define HN_LAUNCH(kernel, grid, block, smem, stream, ...)                    \
+    do {                                                                     \
+        long long _g = (long long)(grid);                                    \
+        if (_g > 0) {                                                        \
+            cudaEvent_t _ev0 = nullptr;                                      \
+            if (::hn::g_profiling) ::hn::profile_begin((stream), &_ev0);     \
+            kernel<<<(unsigned)_g, (block), (smem), (stream)>>>(__VA_ARGS__);\
+            if (_ev0) ::hn::profile_end(#kernel, (stream), _ev0);            \
+            ::hn::count_launch();                                            \
+            HN_CUDA(cudaGetLastError());                                     \
+        }                                                                    \
+    } while (0)
+
+// Stream-ordered temporary device buffer (cudaMallocAsync on the graph's
+// stream; the memory returns to the device pool, not to the driver).
+template <typename T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DevBuf() = default;
+    DevBuf(size_t count, cudaStream_t st) { alloc(count, st); }
+    void alloc(size_t count, cudaStream_t st) {
+        release();
+        s = st;
+        n = count;
+        if (count) HN_CUDA(cudaMallocAsync((void**)&p, count * sizeof(T), st));
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    T* get() const { return p; }
+};
+
+// Grow-only persistent device buffer (kept across calls on one graph).
+struct Persist {
+    void* p = nullptr;
+    size_t bytes = 0;
+    template <typename T>
+    T* ensure(size_t count, cudaStream_t st) {
+        size_t need = count * sizeof(T);
+        if (need > bytes) {
+            if (p) HN_CUDA(cudaFreeAsync(p, st));
+            size_t nb = need + need / 4 + 256;
+            HN_CUDA(cudaMallocAsync(&p, nb, st));
+            bytes = nb;
+        }
+        return (T*)p;
+    }
+    void release(cudaStream_t st) {
+        if (p) cudaFreeAsync(p, st);
+        p = nullptr;
+        bytes = 0;
+    }
+};
+
+struct DeviceInfo {
+    int sms = 148;
+    int max_threads_per_sm = 2048;
+};
+
+}  // namespace hn
+
+// C ABI bodies: exceptions become HN_ERR_* codes, never process exits.
+#define HN_API_BEGIN try {
+#define HN_API_END                                                   \
+    }                                                                \
+    catch (const hn::Error& e) {                                     \
+        hn::set_last_error(e.what());                                \
+        return e.code;                                               \
+    }                                                                \
+    catch (const std::bad_alloc&) {                                  \
+        hn::set_last_error("host allocation failed");                \
+        return HN_ERR_OOM;                                           \
+    }                                                                \
+    catch (const std::exception& e) {                                \
+        hn::set_last_error(e.what());                                \
+        return HN_ERR_CUDA;                                          \
+    }                                                                \
+    return HN_OK;
+#define HN_REQUIRE(cond, msg) \
+    do { if (!(cond)) throw hn::Error(HN_ERR_INVALID, msg); } while (0)
+
+struct hn_graph {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    hn::DeviceInfo info;
+
+    int32_t nV = 0;
+    int64_t nE = 0;
+    int key_bits = 1;              // bits needed for a vertex id
+
+    hn::VRec* vtab = nullptr;      // nV records
+    int32_t* pool = nullptr;       // edge pool
+    unsigned long long pool_cap = 0;
+
+    hn::AllocState* alloc = nullptr;      // device
+    hn::AllocState* h_alloc = nullptr;    // pinned host mirror
+    long long* fl[hn::kNumClasses] = {};  // free lists (block offsets)
+    int fl_cap[hn::kNumClasses] = {};
+    long long** d_fl = nullptr;           // device copy of fl[]
+    int fl_count[hn::kNumClasses] = {};   // free blocks per class (host-owned)
+    unsigned long long bump_host = 0;     // first never-used pool slot
+
+    long long* h_scalar = nullptr;        // pinned host scalars (16)
+    long long* d_scalar = nullptr;        // device scalars (16)
+
+    hn::Persist scratch[8];               // reusable device scratch
+};
+
+struct hn_batch {
+    hn_graph* g = nullptr;
+    int64_t n = 0;
+    int32_t* src = nullptr;  // device copies (owned)
+    int32_t* dst = nullptr;
+    size_t cap = 0;
+};
+
+namespace hn {
+
+// Grid size for a grid-stride loop over n items.
+inline long long grid_for(const hn_graph* g, long long n, int block, int per_sm = 8) {
+    long long need = (n + block - 1) / block;
+    long long lim = (long long)g->info.sms * per_sm;
+    return need < lim ? need : lim;
+}
+
+// Read device scalars back to the host (synchronises the graph stream).
+void read_scalars(hn_graph* g, int count);
+
+// (Re)build the vertex table and pool from a device CSR with int64
+// offsets; adjacency is sorted when `sorted` is false.
+void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
+                    const int32_t* d_adj, bool sorted);
+
+// Device exclusive prefix of degrees over `verts` (or all vertices when
+// verts == nullptr), n+1 entries written to `prefix`.
+void degree_prefix(hn_graph* g, const int32_t* verts, int32_t n, long long* prefix);
+
+// Check the device error word; throws on error (synchronises).
+void check_device_error(hn_graph* g);
+
+// Ensure the pool holds at least `slots` slots (grows by copy).
+void ensure_pool(hn_graph* g, unsigned long long slots);
+// Ensure free list c can hold `count` entries.
+void ensure_free_list(hn_graph* g, int c, long long count);
+
+// Scratch export of the graph as a contiguous CSR (device, int64 offsets).
+void export_csr64(hn_graph* g, long long* off /*nV+1*/, int32_t* adj /*nE*/);
+
+}  // namespace hn

@@ -1,0 +1,260 @@
+// k-truss (hornetsnest/src/Static/KTruss/KTruss.cu:90-174,
+// KTrussSupport.cu:375-468, KTrussOperators.cuh:16-38).
+//
+// Reference semantics: max_K starts at 3; findTrussOfK repeatedly
+// recomputes every edge's support (triangles through it) from scratch and
+// deletes all edges with support < max_K - 2 through a BatchUpdate erase,
+// until a pass deletes nothing; if no edge is left max_K-- and stop,
+// otherwise max_K++ on the peeled graph.  (The reference k-truss does not
+// compile against the current core; the definition is what is kept.)
+//
+// Here the supports are computed once and then maintained incrementally:
+// a round deletes the current frontier F (edges with support < K-2) and,
+// for every triangle (e, e1, e2) of a frontier edge e whose other two edges
+// are still alive, decrements the supports it destroys exactly once — if
+// neither e1 nor e2 is in F both lose one; if exactly one of them is in F
+// the remaining edge loses one, charged to the smaller of the two frontier
+// edges; if both are in F nothing remains to update.  An edge whose support
+// crosses from K-2 to K-3 joins the next frontier.  After the rounds the
+// supports equal the from-scratch supports of the peeled graph, so the
+// surviving edge sets, truss numbers and max_K are those of the reference
+// loop.  Edge ids are positions in the sorted CSR; undirected edge state
+// lives on the (u < v) position.
+#include "hn_graph.cuh"
+
+namespace hn {
+namespace {
+
+constexpr int kB = 256;
+
+__global__ void k_kt_src(const long long* __restrict__ off, int nV, int32_t* __restrict__ src) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nV;
+         u += (long long)gridDim.x * blockDim.x)
+        for (long long e = off[u]; e < off[u + 1]; e++) src[e] = (int)u;
+}
+
+// canonical (u < v) position of every directed edge; checks simplicity and
+// symmetry.
+__global__ void k_kt_canon(const long long* __restrict__ off, const int32_t* __restrict__ adj,
+                           const int32_t* __restrict__ src, long long m,
+                           int32_t* __restrict__ canon, int* __restrict__ err) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x) {
+        int u = src[e], v = adj[e];
+        bool bad = (u == v) || (e > off[u] && adj[e - 1] == v);
+        long long c = e;
+        if (u > v) {
+            long long p = off[v] + lower_bound_dev(adj + off[v], off[v + 1] - off[v], u);
+            if (p >= off[v + 1] || adj[p] != u) bad = true;
+            c = p;
+        }
+        canon[e] = (int)c;
+        if (bad) atomicExch(err, 1);
+    }
+}
+
+// support of each canonical edge = |N(u) ∩ N(v)|
+__global__ void k_kt_support(const long long* __restrict__ off, const int32_t* __restrict__ adj,
+                             const int32_t* __restrict__ src, long long m,
+                             int32_t* __restrict__ sup, unsigned char* __restrict__ alive,
+                             int* __restrict__ nalive) {
+    int mine = 0;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x) {
+        int u = src[e], v = adj[e];
+        if (u >= v) { alive[e] = 0; continue; }
+        const int32_t* A = adj + off[u];
+        long long la = off[u + 1] - off[u];
+        const int32_t* B = adj + off[v];
+        long long lb = off[v + 1] - off[v];
+        if (la > lb) { const int32_t* T = A; A = B; B = T; long long t = la; la = lb; lb = t; }
+        int cnt = 0;
+        long long lo = 0;
+        for (long long i = 0; i < la && lo < lb; i++) {
+            long long p = lo + lower_bound_dev(B + lo, lb - lo, A[i]);
+            if (p < lb && B[p] == A[i]) { cnt++; lo = p + 1; } else lo = p;
+        }
+        sup[e] = cnt;
+        alive[e] = 1;
+        mine++;
+    }
+    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(nalive, mine);
+}
+
+__global__ void k_kt_frontier(long long m, int K, const int32_t* __restrict__ sup,
+                              const unsigned char* __restrict__ alive,
+                              unsigned char* __restrict__ inF, int32_t* __restrict__ F,
+                              int* __restrict__ nF) {
+    for (long long e0 = blockIdx.x * (long long)blockDim.x; e0 < m;
+         e0 += (long long)gridDim.x * blockDim.x) {
+        long long e = e0 + threadIdx.x;
+        bool take = e < m && alive[e] && sup[e] < K - 2;
+        int p = warp_append(nF, take);
+        if (take) {
+            F[p] = (int)e;
+            inF[e] = 1;
+        }
+    }
+}
+
+__device__ __forceinline__ void kt_dec(int x, int K, int32_t* sup, int32_t* NF, int* nNF) {
+    int old = atomicSub(sup + x, 1);
+    if (old == K - 2) NF[atomicAdd(nNF, 1)] = x;
+}
+
+__global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __restrict__ adj,
+                          const int32_t* __restrict__ src, const int32_t* __restrict__ canon,
+                          const int32_t* __restrict__ F, int nF, int K,
+                          const unsigned char* __restrict__ alive,
+                          const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
+                          int32_t* __restrict__ NF, int* __restrict__ nNF) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nF;
+         f += (long long)gridDim.x * blockDim.x) {
+        int e = F[f];
+        int u = src[e], v = adj[e];
+        long long au = off[u], la = off[u + 1] - au;
+        long long bv = off[v], lb = off[v + 1] - bv;
+        bool swapped = la > lb;
+        long long pa = swapped ? bv : au, pb = swapped ? au : bv;
+        long long na = swapped ? lb : la, nb = swapped ? la : lb;
+        long long lo = 0;
+        for (long long i = 0; i < na && lo < nb; i++) {
+            int w = adj[pa + i];
+            long long p = lo + lower_bound_dev(adj + pb + lo, nb - lo, w);
+            lo = p;
+            if (p >= nb || adj[pb + p] != w) continue;
+            lo = p + 1;
+            int e1 = canon[pa + i], e2 = canon[pb + p];
+            if (!alive[e1] || !alive[e2]) continue;
+            bool f1 = inF[e1], f2 = inF[e2];
+            if (!f1 && !f2) {
+                kt_dec(e1, K, sup, NF, nNF);
+                kt_dec(e2, K, sup, NF, nNF);
+            } else if (f1 && !f2) {
+                if (e < e1) kt_dec(e2, K, sup, NF, nNF);
+            } else if (!f1 && f2) {
+                if (e < e2) kt_dec(e1, K, sup, NF, nNF);
+            }
+        }
+    }
+}
+
+__global__ void k_kt_retire(const int32_t* __restrict__ F, int nF, const int32_t* __restrict__ NF,
+                            const int* __restrict__ nNF, int K, unsigned char* __restrict__ alive,
+                            unsigned char* __restrict__ inF, int32_t* __restrict__ truss) {
+    int nn = *nNF;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nF || i < nn;
+         i += (long long)gridDim.x * blockDim.x) {
+        if (i < nF) {
+            int e = F[i];
+            alive[e] = 0;
+            inF[e] = 0;
+            truss[e] = K - 1;
+        }
+    }
+}
+
+__global__ void k_kt_mark(const int32_t* __restrict__ NF, const int* __restrict__ nNF,
+                          unsigned char* __restrict__ inF) {
+    int nn = *nNF;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
+         i += (long long)gridDim.x * blockDim.x)
+        inF[NF[i]] = 1;
+}
+
+__global__ void k_kt_out(const int32_t* __restrict__ canon, const int32_t* __restrict__ truss,
+                         long long m, int32_t* __restrict__ out) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x)
+        out[e] = truss[canon[e]];
+}
+
+int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
+    cudaStream_t s = g->stream;
+    const int nV = g->nV;
+    const long long m = g->nE;
+    if (m > 0x7FFFFFFF) throw Error(HN_ERR_INVALID, "k-truss needs nE < 2^31");
+    if (m == 0) return 2;
+    DevBuf<long long> off((size_t)nV + 1, s);
+    DevBuf<int32_t> adj((size_t)m, s), src((size_t)m, s), canon((size_t)m, s), sup((size_t)m, s),
+        truss((size_t)m, s), F((size_t)m, s), NF((size_t)m, s);
+    DevBuf<unsigned char> alive((size_t)m, s), inF((size_t)m, s);
+    int* cnt = (int*)g->d_scalar;  // [0] err/alive, [1] nF, [2] nNF
+    export_csr64(g, off.get(), adj.get());
+    HN_LAUNCH(k_kt_src, grid_for(g, nV, kB), kB, 0, s, off.get(), nV, src.get());
+    HN_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
+    HN_LAUNCH(k_kt_canon, grid_for(g, m, kB), kB, 0, s, off.get(), adj.get(), src.get(), m,
+              canon.get(), cnt);
+    read_scalars(g, 1);
+    if (((int*)g->h_scalar)[0])
+        throw Error(HN_ERR_INVALID, "k-truss needs a simple symmetric graph");
+    HN_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
+    HN_CUDA(cudaMemsetAsync(inF.get(), 0, (size_t)m, s));
+    HN_LAUNCH(k_kt_support, grid_for(g, m, kB), kB, 0, s, off.get(), adj.get(), src.get(), m,
+              sup.get(), alive.get(), cnt);
+    // truss numbers start at 2 (0x02020202 per int is not 2; fill by kernel-free memset of 0
+    // then write on retirement: every edge is retired exactly once)
+    read_scalars(g, 1);
+    long long remaining = ((int*)g->h_scalar)[0];
+    int K = 3;
+    int* nF = cnt + 1;
+    int* nNF = cnt + 2;
+    const long long grid = grid_for(g, m, kB);
+    while (true) {
+        if (remaining <= 0) { K--; break; }
+        HN_CUDA(cudaMemsetAsync(nF, 0, sizeof(int), s));
+        HN_LAUNCH(k_kt_frontier, grid, kB, 0, s, m, K, sup.get(), alive.get(), inF.get(), F.get(),
+                  nF);
+        HN_CUDA(cudaMemcpyAsync(g->h_scalar, nF, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HN_CUDA(cudaStreamSynchronize(s));
+        int nf = ((int*)g->h_scalar)[0];
+        while (nf > 0) {
+            HN_CUDA(cudaMemsetAsync(nNF, 0, sizeof(int), s));
+            HN_LAUNCH(k_kt_peel, grid_for(g, nf, 128), 128, 0, s, off.get(), adj.get(), src.get(),
+                      canon.get(), F.get(), nf, K, alive.get(), inF.get(), sup.get(), NF.get(),
+                      nNF);
+            HN_LAUNCH(k_kt_retire, grid_for(g, nf, kB), kB, 0, s, F.get(), nf, NF.get(), nNF, K,
+                      alive.get(), inF.get(), truss.get());
+            HN_LAUNCH(k_kt_mark, grid_for(g, m, kB), kB, 0, s, NF.get(), nNF, inF.get());
+            remaining -= nf;
+            HN_CUDA(cudaMemcpyAsync(g->h_scalar, nNF, sizeof(int), cudaMemcpyDeviceToHost, s));
+            HN_CUDA(cudaStreamSynchronize(s));
+            nf = ((int*)g->h_scalar)[0];
+            std::swap(F.p, NF.p);
+        }
+        if (remaining <= 0) { K--; break; }
+        K++;
+    }
+    if (d_edge_truss)
+        HN_LAUNCH(k_kt_out, grid_for(g, m, kB), kB, 0, s, canon.get(), truss.get(), m,
+                  d_edge_truss);
+    HN_CUDA(cudaStreamSynchronize(s));
+    return K;
+}
+
+}  // namespace
+}  // namespace hn
+
+using namespace hn;
+
+extern "C" int hn_ktruss(hn_graph_t* g, int32_t* max_k, int32_t* edge_truss, int mem) {
+    HN_API_BEGIN
+    HN_REQUIRE(g != nullptr, "graph is null");
+    HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    DevBuf<int32_t> tmp;
+    int32_t* d_out = edge_truss;
+    if (edge_truss && mem == HN_MEM_HOST) {
+        tmp.alloc((size_t)g->nE, s);
+        d_out = tmp.get();
+    }
+    int K = ktruss_run(g, d_out);
+    if (edge_truss && mem == HN_MEM_HOST && g->nE)
+        HN_CUDA(cudaMemcpyAsync(edge_truss, d_out, sizeof(int32_t) * g->nE,
+                                cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
+    if (max_k) *max_k = K;
+    HN_API_END
+}

@@ -1,0 +1,22 @@
+// Degree-oriented graph used by triangle counting.
+#pragma once
+
+#include "hn_graph.cuh"
+
+namespace hn {
+
+struct Oriented {
+    DevBuf<long long> prefix;  // degree prefix of the undirected graph (nV+1)
+    DevBuf<long long> offp;    // oriented offsets (nV+1)
+    DevBuf<int32_t> fwd;       // oriented, sorted neighbour lists
+};
+
+// Build N+(u) = {v in N(u) : (deg u, u) < (deg v, v)} for every vertex.
+void build_oriented(hn_graph* g, Oriented& o);
+
+// Triangles of the oriented graph; per-vertex counts when d_per_vertex
+// is non-null (device array of nV entries).  Synchronises.
+unsigned long long count_triangles(hn_graph* g, const Oriented& o,
+                                   unsigned long long* d_per_vertex);
+
+}  // namespace hn

@@ -1,0 +1,525 @@
+// BatchUpdate insert / erase: a fused sort -> dedup -> block (re)allocation
+// -> scatter-merge pipeline with sorted adjacency lists.
+//
+// Reference pipeline (hornet/include/Core/BatchUpdate/BatchUpdate.i.cuh and
+// BatchUpdateKernels.cuh): two stable thrust sorts, unique_copy, a
+// load-balanced scan of every touched adjacency list for graph duplicates,
+// host allocator loops for reallocated vertices, append at old_degree
+// (insert) or tail-refill of holes (erase), with >= 6 host round trips.
+//
+// Here (one host synchronisation per batch, to size the pool):
+//   1. pack (src,dst) into one key of 2*key_bits bits; radix sort;
+//   2. mark: batch / graph duplicates (insert) or per-run deletions
+//      (erase) — graph membership by binary search in the SORTED adjacency;
+//   3. one scan of packed (kept, source-head) counters gives compacted
+//      positions and touched-vertex segments in a single pass;
+//   4. plan: per touched vertex the new degree and block class
+//      (cap = next power of two, the reference's Vertex::limit());
+//   5. host: serve block requests from the per-class free lists, the rest
+//      from the bump pointer (largest class first, so blocks >= 4 slots stay
+//      16-byte aligned); grow the pool / lists if needed;
+//   6. assign blocks (warp-aggregated per-class ranks);
+//   7. scatter-merge into the new block: old element A[r] goes to
+//      r + |{B < A[r]}|, batch element B[j] to j + |{A <= B[j]}| (insert);
+//      for erase a kept A[r] goes to r - |{B <= A[r]}|;
+//   8. commit vertex records and push old blocks on their free lists.
+// Every touched vertex is rewritten out of place, so no kernel ever reads
+// a slot another thread of the same launch writes.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+
+#include "hn_graph.cuh"
+
+namespace hn {
+namespace {
+
+constexpr int kB = 256;
+
+struct Plan {
+    int take[kNumClasses];                    // served from the free list
+    int pop_top[kNumClasses];                 // free-list size before pops
+    int push_base[kNumClasses];               // free-list size after pops
+    unsigned long long bump_base[kNumClasses];
+};
+
+__device__ __forceinline__ int pow2_ceil(int d) {
+    return d <= 1 ? d : (int)(1u << (32 - __clz(d - 1)));
+}
+
+// keys = src << L | dst; ids outside [0,nV) raise HN_ERR_INVALID.
+__global__ void k_pack(const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                       long long n, int nV, int L, unsigned long long* __restrict__ keys,
+                       AllocState* st) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        int u = src[i], v = dst[i];
+        if (u < 0 || u >= nV || v < 0 || v >= nV) {
+            atomicExch(&st->error, HN_ERR_INVALID);
+            u = 0;
+            v = 0;
+        }
+        keys[i] = ((unsigned long long)(unsigned)u << L) | (unsigned)v;
+    }
+}
+
+// Insert marking.  Packed counter value per element: (head << 32) | keep.
+//   keep = (first-of-run || !DEDUP_BATCH) && !(DEDUP_GRAPH && first-of-run
+//          && (u,x) already in the graph)
+// which is the reference's behaviour: remove_batch_duplicates keeps the
+// first of each run (thrust::unique_copy) and mark_duplicate_edges clears the
+// flag of the FIRST batch entry equal to each graph edge
+// (BatchUpdateKernels.cuh:27-58 with xlib lower_bound_left).
+__global__ void k_mark_insert(const unsigned long long* __restrict__ keys, long long n, int L,
+                              unsigned flags, const VRec* __restrict__ vtab,
+                              const int32_t* __restrict__ pool,
+                              unsigned long long* __restrict__ val) {
+    const unsigned long long mask = (1ull << L) - 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long k = keys[i];
+        unsigned long long kp = i ? keys[i - 1] : ~0ull;
+        bool first = (i == 0) || (k != kp);
+        bool head = (i == 0) || ((k >> L) != (kp >> L));
+        bool keep = first || !(flags & HN_DEDUP_BATCH);
+        if (keep && first && (flags & HN_DEDUP_GRAPH)) {
+            int u = (int)(k >> L);
+            int x = (int)(k & mask);
+            VRec r = vtab[u];
+            const int32_t* a = pool + r.off;
+            long long p = lower_bound_dev(a, (long long)r.deg, x);
+            if (p < r.deg && a[p] == x) keep = false;
+        }
+        val[i] = ((unsigned long long)head << 32) | (unsigned long long)keep;
+    }
+}
+
+// Erase marking: element i of a run of equal (u,x) deletes a copy iff its
+// rank in the run (after batch de-duplication) is below the graph
+// multiplicity c_g, so each run removes min(c_b, c_g) copies
+// (BatchUpdateKernels.cuh:263-300, :335-393).
+__global__ void k_mark_erase(const unsigned long long* __restrict__ keys, long long n, int L,
+                             unsigned flags, const VRec* __restrict__ vtab,
+                             const int32_t* __restrict__ pool,
+                             unsigned long long* __restrict__ val) {
+    const unsigned long long mask = (1ull << L) - 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long k = keys[i];
+        unsigned long long kp = i ? keys[i - 1] : ~0ull;
+        bool first = (i == 0) || (k != kp);
+        bool head = (i == 0) || ((k >> L) != (kp >> L));
+        bool del = false;
+        if (first || !(flags & HN_DEDUP_BATCH)) {
+            // rank inside the run of equal keys
+            long long rank = 0;
+            if (!first) rank = i - lower_bound_dev(keys, i, k);
+            int u = (int)(k >> L);
+            int x = (int)(k & mask);
+            VRec r = vtab[u];
+            const int32_t* a = pool + r.off;
+            long long lo = lower_bound_dev(a, (long long)r.deg, x);
+            long long cg = 0;
+            if (lo < r.deg && a[lo] == x) cg = upper_bound_dev(a, (long long)r.deg, x) - lo;
+            del = rank < cg;
+        }
+        val[i] = ((unsigned long long)head << 32) | (unsigned long long)del;
+    }
+}
+
+// Compaction + segments from the exclusive scan of the packed counters.
+//   kept element i  -> cdst[pos], cseg[pos]
+//   head element i  -> seg_u[seg], seg_kstart[seg]
+// Totals go to d_scalar[0] (kept) and d_scalar[1] (segments).
+__global__ void k_compact(const unsigned long long* __restrict__ keys,
+                          const unsigned long long* __restrict__ val,
+                          const unsigned long long* __restrict__ scan, long long n, int L,
+                          int32_t* __restrict__ cdst, int32_t* __restrict__ cseg,
+                          int32_t* __restrict__ seg_u, int32_t* __restrict__ seg_kstart,
+                          long long* __restrict__ totals) {
+    const unsigned long long mask = (1ull << L) - 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long v = val[i], s = scan[i];
+        long long pos = (long long)(s & 0xFFFFFFFFull);
+        long long seg = (long long)(s >> 32) + (long long)(v >> 32) - 1;  // inclusive heads - 1
+        unsigned long long k = keys[i];
+        if (v >> 32) {
+            seg_u[seg] = (int)(k >> L);
+            seg_kstart[seg] = (int)pos;
+        }
+        if (v & 1) {
+            cdst[pos] = (int)(k & mask);
+            cseg[pos] = (int)seg;
+        }
+        if (i == n - 1) {
+            long long kept = pos + (long long)(v & 1);
+            long long nseg = seg + 1;
+            totals[0] = kept;
+            totals[1] = nseg;
+            seg_kstart[nseg] = (int)kept;
+        }
+    }
+}
+
+// Per touched vertex: new degree / class; request and release counts.
+// seg_work[s] = old degree if the vertex changes, else 0.
+__global__ void k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
+                       const long long* __restrict__ totals, bool insert,
+                       const VRec* __restrict__ vtab, long long* __restrict__ seg_work,
+                       int32_t* __restrict__ seg_ncap, AllocState* st) {
+    long long nseg = totals[1];
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s <= nseg;
+         s += (long long)gridDim.x * blockDim.x) {
+        if (s == nseg) { seg_work[s] = 0; continue; }
+        int k = seg_kstart[s + 1] - seg_kstart[s];
+        int u = seg_u[s];
+        VRec r = vtab[u];
+        int ncap = -1;  // -1: vertex unchanged
+        if (k > 0) {
+            int nd = insert ? r.deg + k : r.deg - k;
+            ncap = pow2_ceil(nd);
+            if (ncap > 0) atomicAdd(&st->need[cap_class(ncap)], 1);
+            if (r.cap > 0) atomicAdd(&st->push[cap_class(r.cap)], 1);
+        }
+        seg_ncap[s] = ncap;
+        seg_work[s] = k > 0 ? r.deg : 0;
+    }
+}
+
+// Block assignment: per class, the first take[c] requests pop the free list,
+// the rest are carved from the bump region of the class.
+__global__ void k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
+                         long long* const* __restrict__ fl, AllocState* st,
+                         long long* __restrict__ seg_new_off) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg;
+         s += (long long)gridDim.x * blockDim.x) {
+        int ncap = seg_ncap[s];
+        int c = ncap > 0 ? cap_class(ncap) : -1;
+        unsigned mask = __activemask();
+        unsigned grp = __match_any_sync(mask, c);
+        int leader = __ffs(grp) - 1;
+        int lane = threadIdx.x & 31;
+        int base = 0;
+        if (c >= 0 && lane == leader) base = atomicAdd(&st->rank[c], __popc(grp));
+        base = __shfl_sync(mask, base, leader);
+        if (c >= 0) {
+            int r = base + __popc(grp & ((1u << lane) - 1));
+            long long off;
+            if (r < plan.take[c]) off = fl[c][plan.pop_top[c] - 1 - r];
+            else off = (long long)(plan.bump_base[c] +
+                                   ((unsigned long long)(r - plan.take[c]) << c));
+            seg_new_off[s] = off;
+        } else {
+            seg_new_off[s] = 0;
+        }
+    }
+}
+
+using Tile = LbTile<kB, 4>;
+
+// Old adjacency of every changed vertex -> its new block.
+template <bool INSERT>
+__global__ void __launch_bounds__(kB)
+k_scatter_old(const long long* __restrict__ prefix, long long nseg,
+              const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
+              const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
+              const VRec* __restrict__ vtab, int32_t* __restrict__ pool) {
+    __shared__ Tile t;
+    __shared__ long long s_old[Tile::TILE + 1];
+    __shared__ long long s_new[Tile::TILE + 1];
+    __shared__ int s_k0[Tile::TILE + 1];
+    __shared__ int s_k1[Tile::TILE + 1];
+    const long long total = prefix[nseg];
+    long long ntiles = (total + nseg + Tile::TILE - 1) / Tile::TILE;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int n = lb_tile_load(t, prefix, nseg, total, tile);
+        for (int b = threadIdx.x; b <= t.nends; b += kB) {
+            long long s = t.seg0 + b;
+            if (s < nseg) {
+                long long st0 = t.seg_start(b);
+                s_old[b] = vtab[seg_u[s]].off - st0;
+                s_new[b] = seg_new_off[s] - st0;
+                s_k0[b] = seg_kstart[s];
+                s_k1[b] = seg_kstart[s + 1];
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kB) {
+            long long e = t.item0 + i;   // global item; rank r = e - seg start
+            int b = t.seg[i];
+            int x = pool[s_old[b] + e];
+            const int32_t* B = cdst + s_k0[b];
+            long long nb = s_k1[b] - s_k0[b];
+            if (INSERT) {
+                long long j = lower_bound_dev(B, nb, x);
+                pool[s_new[b] + e + j] = x;
+            } else {
+                long long ub = upper_bound_dev(B, nb, x);
+                long long lb = ub;
+                if (ub > 0 && B[ub - 1] == x) lb = lower_bound_dev(B, ub, x);
+                long long cnt = ub - lb;  // copies of x to delete
+                bool keep = true;
+                if (cnt > 0) {
+                    // rank of this copy among equal values of the old list
+                    long long r = e - t.seg_start(b);
+                    const int32_t* A = pool + s_old[b] + t.seg_start(b);
+                    long long first = r;
+                    if (r > 0 && A[r - 1] == x) first = lower_bound_dev(A, r, x);
+                    keep = (r - first) >= cnt;
+                }
+                if (keep) pool[s_new[b] + e - ub] = x;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Batch edges -> their slot in the new block (insert only).
+__global__ void k_scatter_new(const int32_t* __restrict__ cdst, const int32_t* __restrict__ cseg,
+                              const long long* __restrict__ totals,
+                              const int32_t* __restrict__ seg_u,
+                              const int32_t* __restrict__ seg_kstart,
+                              const long long* __restrict__ seg_new_off,
+                              const VRec* __restrict__ vtab, int32_t* __restrict__ pool) {
+    long long kept = totals[0];
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < kept;
+         p += (long long)gridDim.x * blockDim.x) {
+        int s = cseg[p];
+        int x = cdst[p];
+        VRec r = vtab[seg_u[s]];
+        long long pos = upper_bound_dev(pool + r.off, (long long)r.deg, x);
+        pool[seg_new_off[s] + (p - seg_kstart[s]) + pos] = x;
+    }
+}
+
+// New vertex records; old blocks pushed on their class free list.
+__global__ void k_commit(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
+                         const int32_t* __restrict__ seg_ncap,
+                         const long long* __restrict__ seg_new_off, long long nseg, bool insert,
+                         Plan plan, long long* const* __restrict__ fl, AllocState* st,
+                         VRec* __restrict__ vtab) {
+    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg;
+         s += (long long)gridDim.x * blockDim.x) {
+        int ncap = seg_ncap[s];
+        if (ncap < 0) continue;
+        int u = seg_u[s];
+        int k = seg_kstart[s + 1] - seg_kstart[s];
+        VRec r = vtab[u];
+        if (r.cap > 0) {
+            int c = cap_class(r.cap);
+            int p = atomicAdd(&st->prank[c], 1);
+            fl[c][plan.push_base[c] + p] = r.off;
+        }
+        VRec nr;
+        nr.deg = insert ? r.deg + k : r.deg - k;
+        nr.cap = ncap;
+        nr.off = ncap > 0 ? seg_new_off[s] : 0;
+        vtab[u] = nr;
+    }
+}
+
+void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* applied) {
+    cudaStream_t s = g->stream;
+    const long long n = b->n;
+    if (applied) *applied = 0;
+    if (n == 0) return;
+    const int L = g->key_bits;
+    AllocState* st = g->alloc;
+
+    // 1. pack + sort
+    DevBuf<unsigned long long> keys(n, s), keys2(n, s);
+    HN_CUDA(cudaMemsetAsync(st, 0, sizeof(AllocState), s));
+    HN_LAUNCH(k_pack, grid_for(g, n, kB), kB, 0, s, b->src, b->dst, n, g->nV, L, keys.get(), st);
+    {
+        cub::DoubleBuffer<unsigned long long> db(keys.get(), keys2.get());
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)n, 0, 2 * L, s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, db, (int)n, 0, 2 * L, s));
+        count_launch();
+        if (db.Current() != keys.get()) std::swap(keys.p, keys2.p);
+    }
+    // 2. mark  (keys2 reused as the counter values)
+    unsigned long long* val = keys2.get();
+    if (insert)
+        HN_LAUNCH(k_mark_insert, grid_for(g, n, kB), kB, 0, s, keys.get(), n, L, flags, g->vtab,
+                  g->pool, val);
+    else
+        HN_LAUNCH(k_mark_erase, grid_for(g, n, kB), kB, 0, s, keys.get(), n, L, flags, g->vtab,
+                  g->pool, val);
+    // 3. scan + compact
+    DevBuf<unsigned long long> scan(n, s);
+    {
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, val, scan.get(), (int)n, s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, val, scan.get(), (int)n, s));
+        count_launch();
+    }
+    DevBuf<int32_t> cdst(n, s), cseg(n, s), seg_u(n, s), seg_kstart(n + 1, s), seg_ncap(n, s);
+    DevBuf<long long> seg_work(n + 1, s), seg_new_off(n, s);
+    long long* totals = g->d_scalar;
+    HN_LAUNCH(k_compact, grid_for(g, n, kB), kB, 0, s, keys.get(), val, scan.get(), n, L,
+              cdst.get(), cseg.get(), seg_u.get(), seg_kstart.get(), totals);
+    keys2.release();
+    scan.release();
+    // 4. plan
+    HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
+              insert, g->vtab, seg_work.get(), seg_ncap.get(), st);
+    // 5. host plan (the one synchronisation of the batch)
+    HN_CUDA(cudaMemcpyAsync(g->h_scalar, totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
+                            s));
+    HN_CUDA(cudaMemcpyAsync(g->h_alloc, st, sizeof(AllocState), cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
+    if (g->h_alloc->error) {
+        HN_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(int), s));
+        throw Error(HN_ERR_INVALID, "batch vertex id outside [0, nV)");
+    }
+    const long long kept = g->h_scalar[0];
+    const long long nseg = g->h_scalar[1];
+    if (kept == 0) return;
+
+    Plan plan;
+    unsigned long long bump = (g->bump_host + 3) & ~3ull;
+    for (int c = kNumClasses - 1; c >= 0; c--) {
+        int need = g->h_alloc->need[c];
+        int have = g->fl_count[c];
+        int take = need < have ? need : have;
+        plan.take[c] = take;
+        plan.pop_top[c] = have;
+        plan.push_base[c] = have - take;
+        plan.bump_base[c] = bump;
+        bump += (unsigned long long)(need - take) << c;
+    }
+    ensure_pool(g, bump);
+    for (int c = 0; c < kNumClasses; c++) {
+        long long after = (long long)plan.push_base[c] + g->h_alloc->push[c];
+        ensure_free_list(g, c, after);
+    }
+    // 6. assign blocks
+    HN_LAUNCH(k_assign, grid_for(g, nseg, kB), kB, 0, s, seg_ncap.get(), nseg, plan,
+              (long long* const*)g->d_fl, st, seg_new_off.get());
+    // 7. scatter-merge
+    {
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, seg_work.get(), seg_work.get(),
+                                              (int)(nseg + 1), s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, seg_work.get(), seg_work.get(),
+                                              (int)(nseg + 1), s));
+        count_launch();
+    }
+    // tiles are read from the device prefix; the grid is persistent
+    const long long grid_sc = (long long)g->info.sms * 4;
+    if (insert) {
+        HN_LAUNCH(k_scatter_old<true>, grid_sc, kB, 0, s, seg_work.get(), nseg,
+                  seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
+                  g->vtab, g->pool);
+        HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), totals,
+                  seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool);
+    } else {
+        HN_LAUNCH(k_scatter_old<false>, grid_sc, kB, 0, s, seg_work.get(),
+                  nseg, seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
+                  g->vtab, g->pool);
+    }
+    // 8. commit
+    HN_LAUNCH(k_commit, grid_for(g, nseg, kB), kB, 0, s, seg_u.get(), seg_kstart.get(),
+              seg_ncap.get(), seg_new_off.get(), nseg, insert, plan, (long long* const*)g->d_fl,
+              st, g->vtab);
+    for (int c = 0; c < kNumClasses; c++)
+        g->fl_count[c] = plan.push_base[c] + g->h_alloc->push[c];
+    g->bump_host = bump;
+    g->nE += insert ? kept : -kept;
+    if (applied) *applied = kept;
+    HN_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+}  // namespace hn
+
+using namespace hn;
+
+extern "C" {
+
+int hn_batch_create(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t* dst, int mem,
+                    hn_batch_t** out) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && out, "null argument");
+    *out = nullptr;
+    hn_batch* b = new hn_batch();
+    b->g = g;
+    int rc = hn_batch_reset(b, n, src, dst, mem);
+    if (rc != HN_OK) {
+        delete b;
+        return rc;
+    }
+    *out = b;
+    HN_API_END
+}
+
+int hn_batch_reset(hn_batch_t* b, int64_t n, const int32_t* src, const int32_t* dst, int mem) {
+    HN_API_BEGIN
+    HN_REQUIRE(b != nullptr, "batch is null");
+    HN_REQUIRE(n >= 0 && n <= 0x7FFFFFFF, "batch size must be in [0, 2^31)");
+    HN_REQUIRE(n == 0 || (src && dst), "null batch arrays");
+    HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    hn_graph* g = b->g;
+    HN_CUDA(cudaSetDevice(g->device));
+    if ((size_t)n > b->cap) {
+        if (b->src) HN_CUDA(cudaFree(b->src));
+        if (b->dst) HN_CUDA(cudaFree(b->dst));
+        b->src = b->dst = nullptr;
+        b->cap = 0;
+        HN_CUDA(cudaMalloc((void**)&b->src, sizeof(int32_t) * (size_t)n));
+        HN_CUDA(cudaMalloc((void**)&b->dst, sizeof(int32_t) * (size_t)n));
+        b->cap = (size_t)n;
+    }
+    b->n = n;
+    if (n) {
+        cudaMemcpyKind kind = mem == HN_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+        HN_CUDA(cudaMemcpyAsync(b->src, src, sizeof(int32_t) * (size_t)n, kind, g->stream));
+        HN_CUDA(cudaMemcpyAsync(b->dst, dst, sizeof(int32_t) * (size_t)n, kind, g->stream));
+        HN_CUDA(cudaStreamSynchronize(g->stream));
+    }
+    HN_API_END
+}
+
+int hn_batch_size(const hn_batch_t* b, int64_t* n) {
+    HN_API_BEGIN
+    HN_REQUIRE(b && n, "null argument");
+    *n = b->n;
+    HN_API_END
+}
+
+int hn_batch_destroy(hn_batch_t* b) {
+    HN_API_BEGIN
+    if (!b) return HN_OK;
+    cudaSetDevice(b->g->device);
+    if (b->src) cudaFree(b->src);
+    if (b->dst) cudaFree(b->dst);
+    delete b;
+    HN_API_END
+}
+
+int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && b, "null argument");
+    HN_REQUIRE(b->g == g, "batch belongs to another graph");
+    HN_REQUIRE((flags & ~(HN_DEDUP_BATCH | HN_DEDUP_GRAPH)) == 0, "unknown flags");
+    HN_CUDA(cudaSetDevice(g->device));
+    run_update(g, b, flags, true, applied);
+    HN_API_END
+}
+
+int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && b, "null argument");
+    HN_REQUIRE(b->g == g, "batch belongs to another graph");
+    HN_REQUIRE((flags & ~HN_DEDUP_BATCH) == 0, "unknown flags");
+    HN_CUDA(cudaSetDevice(g->device));
+    run_update(g, b, flags, false, applied);
+    HN_API_END
+}
+
+}  // extern "C"

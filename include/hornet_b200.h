@@ -1,0 +1,232 @@
+/*
+ * hornet_b200 — C ABI of the B200-native Hornet dynamic-graph hot path.
+ *
+ * Every entry point returns an int status (HN_OK or HN_ERR_*), never exits
+ * the process, and records a message readable with hn_last_error_string().
+ * The reference's error path prints, asserts and exits
+ * (xlib/src/Device/Util/SafeCudaAPI.cpp:71-94); this layer reports instead.
+ *
+ * Ids are int32 (VID_T = DEGREE_T = int, hornet/include/Core/Conf/
+ * HornetConf.cuh:41-42).  Unless an entry point says otherwise, pointer
+ * arguments name HOST memory when `mem` is HN_MEM_HOST and DEVICE memory on
+ * the graph's device when it is HN_MEM_DEVICE.  Calls on one handle must be
+ * serialised by the caller; handles on different devices are independent
+ * (the reference's multi-GPU use is one replica per device,
+ * hornet/test/HornetMultiGPUInsertTest.cu:43-81).
+ *
+ * All calls are synchronous with respect to the host, as the reference's
+ * are (every operator ends in CHECK_CUDA_ERROR), except those documented
+ * as asynchronous on the graph's stream.
+ */
+#ifndef HORNET_B200_H
+#define HORNET_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define HN_OK            0
+#define HN_ERR_INVALID   1   /* bad argument (null pointer, id out of range) */
+#define HN_ERR_OOM       2   /* device allocation failed */
+#define HN_ERR_CAPACITY  3   /* a fixed-capacity buffer would overflow */
+#define HN_ERR_TIMEOUT   4   /* a bounded device wait gave up */
+#define HN_ERR_CUDA      5   /* any other CUDA runtime error */
+#define HN_ERR_STATE     6   /* call not valid in the object's state */
+
+/* ---- memory kinds / flags --------------------------------------------- */
+#define HN_MEM_HOST      0
+#define HN_MEM_DEVICE    1
+
+#define HN_CSR_SORTED    1u  /* adjacency lists already sorted ascending */
+
+#define HN_DEDUP_BATCH   1u  /* removeBatchDuplicates (Hornet.cuh:107,109) */
+#define HN_DEDUP_GRAPH   2u  /* removeGraphDuplicates (Hornet.cuh:107)     */
+
+#define HN_CC_MIN_ID     0   /* label = minimum vertex id of the component  */
+#define HN_CC_REFERENCE  1   /* hornetsnest CC colours: giant = 0, others
+                                max(id)+1 (ConnectedComponents/CC.cu:133-156) */
+
+#define HN_LB_BINARY_SEARCH 0 /* load_balancing::BinarySearch              */
+#define HN_LB_VERTEX_BASED  1 /* load_balancing::VertexBased<VW>           */
+
+typedef struct hn_graph hn_graph_t;
+typedef struct hn_batch hn_batch_t;
+
+/* Device view of a graph for user kernels (the C counterpart of
+ * hornet::HornetDevice, hornet/include/Core/HornetDevice/HornetDevice.cuh:52-90).
+ * vertex v: record vtab + 16*v = {int64 off; int32 deg; int32 cap};
+ * its sorted neighbours are pool[off .. off+deg). */
+typedef struct hn_device_view {
+    int32_t nV;
+    int32_t pad;
+    int64_t nE;
+    const void* vtab;
+    const int32_t* pool;
+} hn_device_view_t;
+
+/* Per-call statistics of a traversal. */
+typedef struct hn_bfs_stats {
+    int32_t levels;          /* number of BFS levels (max distance + 1) */
+    int32_t pad;
+    int64_t visited;         /* vertices reached */
+    int64_t edges_scanned;   /* sum of degrees of reached vertices */
+} hn_bfs_stats_t;
+
+/* ---- library ------------------------------------------------------------ */
+const char* hn_last_error_string(void);
+int hn_version(void);
+/* Number of device kernels this library has launched in this process
+ * (instrumentation for the benchmark's launch count). */
+int64_t hn_kernel_launches(void);
+/* Per-kernel timing: when enabled, every library kernel launch is bracketed
+ * by CUDA events on its own stream.  hn_profile_enable also clears the
+ * records.  hn_profile_report writes a JSON object
+ * {"kernel": {"launches": n, "ms": total}, ...} (synchronises). */
+int hn_profile_enable(int on);
+int hn_profile_report(char* buf, int64_t len);
+
+/* ---- graph construction (HornetInit + gpu::Hornet(HornetInit&)) ----------
+ * Replaces hornet::HornetInit(nV, nE, offsets, edges)
+ * (hornet/include/Core/HornetInitialize/HornetInit.cuh:70-73) and
+ * gpu::Hornet::Hornet(HornetInit&) / initialize()
+ * (HornetInitialize/HornetInitialize.i.cuh:88-146).  The CSR is copied;
+ * the caller keeps ownership.  `off` has nV+1 entries, `adj` nE entries.
+ * Adjacency lists are stored sorted (sorted on the device unless
+ * HN_CSR_SORTED says they already are). `device` = CUDA ordinal. */
+int hn_graph_create_csr(int32_t nV, int64_t nE, const int32_t* off,
+                        const int32_t* adj, unsigned flags, int mem,
+                        int device, hn_graph_t** out);
+/* Same with int64 offsets, for graphs with more than 2^31-1 edges. */
+int hn_graph_create_csr64(int32_t nV, int64_t nE, const int64_t* off,
+                          const int32_t* adj, unsigned flags, int mem,
+                          int device, hn_graph_t** out);
+/* gpu::Hornet::reset(HornetInit&) (HornetInitialize.i.cuh:190-204). */
+int hn_graph_reset_csr(hn_graph_t* g, int32_t nV, int64_t nE, const int32_t* off,
+                       const int32_t* adj, unsigned flags, int mem);
+int hn_graph_destroy(hn_graph_t* g);
+/* Use `stream` (a cudaStream_t) for this graph's work; NULL = a private
+ * stream created with the graph. */
+int hn_graph_set_stream(hn_graph_t* g, void* stream);
+
+/* ---- queries (hornet/include/Core/Hornet.cuh:113-127,
+ *               HornetOperations/HornetQuery.i.cuh) ------------------------ */
+int hn_graph_nv(const hn_graph_t* g, int32_t* nV);
+int hn_graph_ne(const hn_graph_t* g, int64_t* nE);
+/* max_degree() and max_degree_id(): lowest id among ties, as
+ * thrust::max_element (HornetQuery.i.cuh:10-21,23-44). */
+int hn_graph_max_degree(hn_graph_t* g, int32_t* max_degree, int32_t* max_id);
+/* getCOO(true): (src,dst) sorted lexicographically, nE entries each
+ * (HornetQuery.i.cuh:67-109).  Adjacency is always sorted here, so
+ * `sorted` only documents intent. */
+int hn_graph_export_coo(hn_graph_t* g, int sorted, int32_t* src, int32_t* dst,
+                        int mem);
+/* getCSR(true) (HornetQuery.i.cuh:111-151): off[nV+1], adj[nE]. */
+int hn_graph_export_csr(hn_graph_t* g, int32_t* off, int32_t* adj, int mem);
+/* Degrees of all vertices (int32[nV]). */
+int hn_graph_degrees(hn_graph_t* g, int32_t* deg, int mem);
+/* hornet.device() (Hornet.cuh:117): raw device view for user kernels. */
+int hn_graph_device_view(hn_graph_t* g, hn_device_view_t* view);
+/* Slots held by the edge pool and by live blocks (for accounting). */
+int hn_graph_memory(hn_graph_t* g, int64_t* pool_slots, int64_t* used_slots,
+                    int64_t* free_list_blocks);
+
+/* ---- batches (BatchUpdatePtr + gpu::BatchUpdate) -----------------------
+ * Replaces BatchUpdatePtr<int, EMPTY, HOST|DEVICE>(n, src, dst)
+ * (hornet/include/Core/BatchUpdate/BatchUpdate.cuh:91-99) and
+ * gpu::BatchUpdate(ptr), which copies into owned device buffers
+ * (BatchUpdate.i.cuh:154-184). */
+int hn_batch_create(hn_graph_t* g, int64_t n, const int32_t* src,
+                    const int32_t* dst, int mem, hn_batch_t** out);
+/* Refill an existing batch (BatchUpdate::reset). */
+int hn_batch_reset(hn_batch_t* b, int64_t n, const int32_t* src,
+                   const int32_t* dst, int mem);
+int hn_batch_size(const hn_batch_t* b, int64_t* n);
+int hn_batch_destroy(hn_batch_t* b);
+
+/* gpu::Hornet::insert(batch, removeBatchDuplicates, removeGraphDuplicates)
+ * (hornet/include/Core/HornetOperations/HornetInsert.i.cuh:12-27).
+ * flags: HN_DEDUP_BATCH | HN_DEDUP_GRAPH.  Multiset semantics: without
+ * flags every batch edge is added; HN_DEDUP_GRAPH drops the first copy of
+ * each batch edge already in the graph.  *applied = edges added.
+ * Ids outside [0,nV) -> HN_ERR_INVALID and the graph is unchanged. */
+int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied);
+/* gpu::Hornet::erase(batch, removeBatchDuplicates)
+ * (HornetInsert.i.cuh:71-89): each distinct (u,v) removes
+ * min(batch multiplicity, graph multiplicity) copies.  *applied = edges
+ * removed. */
+int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied);
+
+/* ---- algorithms (hornetsnest StaticAlgorithm subclasses) -------------- */
+
+/* BfsTopDown: set_parameters(src) + run()
+ * (hornetsnest/src/Static/BreadthFirstSearch/TopDown.cu:80-106).
+ * dist: int32[nV], INT32_MAX when unreachable.  stats may be NULL. */
+int hn_bfs(hn_graph_t* g, int32_t src, int32_t* dist, int mem,
+           hn_bfs_stats_t* stats);
+/* k independent BFS runs (one per source); dist is int32[k][nV]
+ * row-major; stats (may be NULL) has k entries. */
+int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k,
+                 int32_t* dist, int mem, hn_bfs_stats_t* stats);
+
+/* TriangleCounting2::init/run/countTriangles
+ * (hornetsnest/src/Static/TriangleCounting/triangle2.cu:130-171) on the
+ * graph's undirected adjacency, each triangle counted once via the
+ * degree orientation of xlib/src/Graph/GraphStd.cpp:247-268.
+ * per_vertex (may be NULL): uint64[nV], triangles containing each vertex.
+ * per_vertex uses `mem`; *total is always host. */
+int hn_tc(hn_graph_t* g, uint64_t* per_vertex, int mem, uint64_t* total);
+
+/* CC::run (hornetsnest/src/Static/ConnectedComponents/CC.cu:133-156).
+ * mode HN_CC_MIN_ID or HN_CC_REFERENCE.  labels: int32[nV];
+ * *n_components (may be NULL) is host. */
+int hn_cc(hn_graph_t* g, int mode, int32_t* labels, int mem,
+          int32_t* n_components);
+
+/* KTruss::run / getMaxK (hornetsnest/src/Static/KTruss/KTruss.cu:90-174)
+ * on a simple undirected graph.  edge_truss (may be NULL): int32[nE] in
+ * sorted-COO order, the largest k whose k-truss holds the edge (2 if none).
+ * *max_k is host. */
+int hn_ktruss(hn_graph_t* g, int32_t* max_k, int32_t* edge_truss, int mem);
+
+/* ---- operator primitives with built-in operators -----------------------
+ * forAllEdges(hornet, vertex_array, size, op, lb) with the BinarySearch or
+ * VertexBased<vw> load balancer (primitives/Operator++.cuh:143-215,
+ * LoadBalancing/BinarySearch.i.cuh:58-107, VertexBased.i.cuh:43-89) running
+ * the built-in "count" operator: out[dst] += 1 for every edge (src,dst) of
+ * each listed vertex (vertices == NULL: all vertices).  out: int32[nV]
+ * device, accumulated.  User operators use the C++ header
+ * <hornet_b200/Operator++.cuh> instead. */
+int hn_for_all_edges_count(hn_graph_t* g, const int32_t* vertices, int32_t n,
+                           int lb, int vw, int32_t* out);
+/* forAllVertices(hornet, op) with the built-in "degree" operator:
+ * out[v] = degree(v) (Operator++.i.cuh:524-540). out: int32[nV] device. */
+int hn_for_all_vertices_degree(hn_graph_t* g, int32_t* out);
+
+/* ---- synthetic inputs (not part of the reference API) --------------------
+ * R-MAT edge pairs (a,b,c; d = 1-a-b-c) from a counter-based generator:
+ * pair i depends only on (seed, i), so the host and device versions give
+ * identical arrays.  n_vertices may be below 2^scale: endpoints >= n are
+ * redrawn.  src/dst: int32[np]. */
+int hn_gen_rmat_host(int32_t scale, int32_t n_vertices, int64_t np, double a,
+                     double b, double c, uint64_t seed, int32_t* src,
+                     int32_t* dst);
+int hn_gen_rmat_device(int32_t scale, int32_t n_vertices, int64_t np, double a,
+                       double b, double c, uint64_t seed, int32_t* src,
+                       int32_t* dst, int device);
+/* Undirected CSR on the device from an edge-pair list: mirror, drop self
+ * loops, sort, dedup (the GPU counterpart of GraphStd's COOtoCSR,
+ * xlib/src/Graph/GraphStd.cpp:174-206).  src/dst are device arrays of np
+ * pairs.  *off_out / *adj_out receive device buffers allocated with
+ * cudaMalloc (free with hn_free_device); *nE_out is the edge count. */
+int hn_coo_to_csr_device(int32_t nV, int64_t np, const int32_t* src,
+                         const int32_t* dst, int device, int32_t** off_out,
+                         int32_t** adj_out, int64_t* nE_out);
+int hn_free_device(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HORNET_B200_H */

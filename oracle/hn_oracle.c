@@ -1,0 +1,379 @@
+/*
+ * CPU ORACLE — test infrastructure, not product code.  See hn_oracle.h for
+ * what each function restates; the reference line numbers are repeated at
+ * each definition.  Single-threaded on purpose: the reference's host
+ * verifiers are single-threaded, and this file doubles as the "port" CPU
+ * baseline.
+ */
+#include "hn_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+/* ---- small helpers --------------------------------------------------- */
+
+static int cmp_u64(const void* a, const void* b) {
+    uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    return (x > y) - (x < y);
+}
+
+static int cmp_i32(const void* a, const void* b) {
+    int32_t x = *(const int32_t*)a, y = *(const int32_t*)b;
+    return (x > y) - (x < y);
+}
+
+static uint64_t pack(int32_t u, int32_t v) {
+    return ((uint64_t)(uint32_t)u << 32) | (uint32_t)v;
+}
+
+/* Build a CSR (int64 offsets) from sorted packed keys. */
+static void keys_to_csr(int32_t nV, const uint64_t* k, int64_t n, int64_t* off,
+                        int32_t* adj) {
+    memset(off, 0, sizeof(int64_t) * ((size_t)nV + 1));
+    for (int64_t i = 0; i < n; i++) off[(k[i] >> 32) + 1]++;
+    for (int32_t v = 0; v < nV; v++) off[v + 1] += off[v];
+    for (int64_t i = 0; i < n; i++) adj[i] = (int32_t)(uint32_t)k[i];
+}
+
+/* ---- CSR construction ------------------------------------------------ */
+
+/* xlib/src/Graph/GraphStd.cpp:174-206 (mirror, drop self loops, sort+unique)
+ * and :306-310 (sorted adjacency). */
+int64_t hno_build_csr_undirected(int32_t nV, int64_t np, const int32_t* src,
+                                 const int32_t* dst, int64_t* off, int32_t* adj) {
+    uint64_t* k = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(2 * np + 1));
+    int64_t n = 0;
+    for (int64_t i = 0; i < np; i++) {
+        if (src[i] == dst[i]) continue;
+        k[n++] = pack(src[i], dst[i]);
+        k[n++] = pack(dst[i], src[i]);
+    }
+    qsort(k, (size_t)n, sizeof(uint64_t), cmp_u64);
+    int64_t m = 0;
+    for (int64_t i = 0; i < n; i++)
+        if (i == 0 || k[i] != k[i - 1]) k[m++] = k[i];
+    keys_to_csr(nV, k, m, off, adj);
+    free(k);
+    return m;
+}
+
+/* xlib/src/Graph/GraphStd.cpp:247-268: u->v survives iff
+ * (deg_u < deg_v) || (deg_u == deg_v && u < v); degrees are those of the
+ * undirected graph.  Input lists are sorted, so output lists stay sorted. */
+int64_t hno_orient_by_degree(int32_t nV, const int64_t* off, const int32_t* adj,
+                             int64_t* out_off, int32_t* out_adj) {
+    int64_t c = 0;
+    out_off[0] = 0;
+    for (int32_t u = 0; u < nV; u++) {
+        int64_t du = off[u + 1] - off[u];
+        for (int64_t e = off[u]; e < off[u + 1]; e++) {
+            int32_t v = adj[e];
+            int64_t dv = off[v + 1] - off[v];
+            if (du < dv || (du == dv && u < v)) out_adj[c++] = v;
+        }
+        out_off[u + 1] = c;
+    }
+    return c;
+}
+
+/* ---- update model ---------------------------------------------------- */
+
+/* Sorted batch keys, with the BatchUpdate preprocessing applied.
+ * Returns the number of keys or -1 on a bad id. */
+static int64_t sorted_batch(int32_t nV, int64_t b, const int32_t* s,
+                            const int32_t* d, int dedup, uint64_t** out) {
+    uint64_t* k = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)(b + 1));
+    for (int64_t i = 0; i < b; i++) {
+        if (s[i] < 0 || s[i] >= nV || d[i] < 0 || d[i] >= nV) {
+            free(k);
+            return -1;
+        }
+        k[i] = pack(s[i], d[i]);
+    }
+    /* sort_batch: stable sort by dst then by src == lexicographic
+     * (hornet/include/Core/SoA/impl/SoAPtr.i.cuh:560-613) */
+    qsort(k, (size_t)b, sizeof(uint64_t), cmp_u64);
+    int64_t n = b;
+    if (dedup) { /* thrust::unique_copy, BatchUpdate.i.cuh:218-240 */
+        n = 0;
+        for (int64_t i = 0; i < b; i++)
+            if (i == 0 || k[i] != k[i - 1]) k[n++] = k[i];
+    }
+    *out = k;
+    return n;
+}
+
+static int contains(const int32_t* a, int64_t n, int32_t x) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) / 2;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo < n && a[lo] == x;
+}
+
+/* HornetInsert.i.cuh:12-27; BatchUpdate.i.cuh:485-502.
+ * Graph de-duplication (BatchUpdate.i.cuh:353-392, BatchUpdateKernels.cuh:27-58)
+ * walks every graph edge (u,x) of a touched source, finds the FIRST batch
+ * entry equal to (u,x) (xlib lower_bound_left) and clears its flag, so
+ * exactly the first element of each run of equal batch edges is dropped
+ * when (u,x) is already present. */
+int64_t hno_insert(int32_t nV, const int64_t* off, const int32_t* adj,
+                   int64_t b, const int32_t* bsrc, const int32_t* bdst,
+                   unsigned flags, int64_t* out_off, int32_t* out_adj) {
+    uint64_t* k = NULL;
+    int64_t n = sorted_batch(nV, b, bsrc, bdst, (flags & HNO_DEDUP_BATCH) != 0, &k);
+    if (n < 0) return -1;
+    if (flags & HNO_DEDUP_GRAPH) {
+        int64_t w = 0;
+        for (int64_t i = 0; i < n; i++) {
+            int first = (i == 0) || (k[i] != k[i - 1]);
+            int32_t u = (int32_t)(k[i] >> 32), x = (int32_t)(uint32_t)k[i];
+            if (first && contains(adj + off[u], off[u + 1] - off[u], x)) continue;
+            k[w++] = k[i];
+        }
+        n = w;
+    }
+    /* multiset union, lists re-sorted: the reference appends
+     * (BatchUpdateKernels.cuh:243-261) and compares sorted COO
+     * (hornet/test/HornetInsertTest.cu:42-75). */
+    int64_t bi = 0, o = 0;
+    out_off[0] = 0;
+    for (int32_t u = 0; u < nV; u++) {
+        int64_t e = off[u], ee = off[u + 1];
+        while (e < ee || (bi < n && (int32_t)(k[bi] >> 32) == u)) {
+            int take_batch;
+            if (e >= ee) take_batch = 1;
+            else if (bi >= n || (int32_t)(k[bi] >> 32) != u) take_batch = 0;
+            else take_batch = (int32_t)(uint32_t)k[bi] < adj[e];
+            out_adj[o++] = take_batch ? (int32_t)(uint32_t)k[bi++] : adj[e++];
+        }
+        out_off[u + 1] = o;
+    }
+    free(k);
+    return n;
+}
+
+/* HornetInsert.i.cuh:71-89; BatchUpdate.i.cuh:504-524, :638-700;
+ * BatchUpdateKernels.cuh:263-300 (atomicSub on the per-run count, so each
+ * run of c_b equal batch edges removes min(c_b, c_g) graph copies) and
+ * :335-393 (run counts).  Lists stay sorted here; the reference refills
+ * holes from the tail (:395-410) and its tests compare sorted COO
+ * (hornet/test/HornetDeleteTest.cu:87-120). */
+int64_t hno_erase(int32_t nV, const int64_t* off, const int32_t* adj,
+                  int64_t b, const int32_t* bsrc, const int32_t* bdst,
+                  unsigned flags, int64_t* out_off, int32_t* out_adj) {
+    uint64_t* k = NULL;
+    int64_t n = sorted_batch(nV, b, bsrc, bdst, (flags & HNO_DEDUP_BATCH) != 0, &k);
+    if (n < 0) return -1;
+    int64_t bi = 0, o = 0, removed = 0;
+    out_off[0] = 0;
+    for (int32_t u = 0; u < nV; u++) {
+        int64_t e = off[u], ee = off[u + 1];
+        while (e < ee) {
+            int32_t x = adj[e];
+            /* skip batch entries of u smaller than x */
+            while (bi < n && (k[bi] >> 32) == (uint64_t)(uint32_t)u &&
+                   (int32_t)(uint32_t)k[bi] < x) bi++;
+            int64_t cb = 0;
+            while (bi + cb < n && k[bi + cb] == pack(u, x)) cb++;
+            int64_t cg = 0;
+            while (e + cg < ee && adj[e + cg] == x) cg++;
+            int64_t del = cb < cg ? cb : cg;
+            removed += del;
+            for (int64_t j = del; j < cg; j++) out_adj[o++] = x;
+            e += cg;
+            bi += cb;
+        }
+        while (bi < n && (int32_t)(k[bi] >> 32) == u) bi++;
+        out_off[u + 1] = o;
+    }
+    free(k);
+    return removed;
+}
+
+/* ---- traversal ------------------------------------------------------- */
+
+/* xlib/src/Graph/BFS.cpp:54-76: FIFO queue, distances[dest] =
+ * distances[current] + 1 on first discovery; INF = INT32_MAX
+ * (TopDown.cu:42).  The level-synchronous GPU TopDown produces the same
+ * distances. */
+int64_t hno_bfs(int32_t nV, const int64_t* off, const int32_t* adj, int32_t src,
+                int32_t* dist) {
+    for (int32_t v = 0; v < nV; v++) dist[v] = HNO_INF;
+    if (src < 0 || src >= nV) return 0;
+    int32_t* q = (int32_t*)malloc(sizeof(int32_t) * (size_t)nV);
+    int64_t head = 0, tail = 0, scanned = 0;
+    q[tail++] = src;
+    dist[src] = 0;
+    while (head < tail) {
+        int32_t c = q[head++];
+        scanned += off[c + 1] - off[c];
+        for (int64_t e = off[c]; e < off[c + 1]; e++) {
+            int32_t d = adj[e];
+            if (dist[d] == HNO_INF) {
+                dist[d] = dist[c] + 1;
+                q[tail++] = d;
+            }
+        }
+    }
+    free(q);
+    return scanned;
+}
+
+/* ---- triangle counting ----------------------------------------------- */
+
+/* hornetsnest/test/TriangleTest2.cu:22-46 (hostSingleIntersection): a
+ * two-pointer merge counting equal pairs. */
+static int64_t single_intersection(const int32_t* a, int64_t alen,
+                                   const int32_t* b, int64_t blen,
+                                   uint64_t* per_vertex) {
+    if (!alen || !blen || a[alen - 1] < b[0] || b[blen - 1] < a[0]) return 0;
+    int64_t i = 0, j = 0, out = 0;
+    while (i < alen && j < blen) {
+        if (a[i] == b[j]) {
+            if (per_vertex) per_vertex[a[i]]++;
+            i++, j++, out++;
+        } else if (a[i] < b[j]) {
+            i++;
+        } else {
+            j++;
+        }
+    }
+    return out;
+}
+
+/* hornetsnest/test/TriangleTest2.cu:48-69 (hostCountTriangles). */
+uint64_t hno_tc_oriented(int32_t nV, const int64_t* off, const int32_t* adj,
+                         uint64_t* per_vertex) {
+    if (per_vertex) memset(per_vertex, 0, sizeof(uint64_t) * (size_t)nV);
+    uint64_t sum = 0;
+    for (int32_t s = 0; s < nV; s++) {
+        for (int64_t it = off[s]; it < off[s + 1]; it++) {
+            int32_t d = adj[it];
+            int64_t t = single_intersection(adj + off[s], off[s + 1] - off[s],
+                                            adj + off[d], off[d + 1] - off[d],
+                                            per_vertex);
+            if (per_vertex) {
+                per_vertex[s] += (uint64_t)t;
+                per_vertex[d] += (uint64_t)t;
+            }
+            sum += (uint64_t)t;
+        }
+    }
+    return sum;
+}
+
+/* ---- connected components -------------------------------------------- */
+
+/* xlib/src/Graph/WCC.cpp:54-98 (undirected branch): components are found in
+ * order of their smallest vertex id, so relabelling component c to the
+ * source that opened it gives the min-id label directly. */
+int32_t hno_cc_min_label(int32_t nV, const int64_t* off, const int32_t* adj,
+                         int32_t* label) {
+    int32_t* q = (int32_t*)malloc(sizeof(int32_t) * (size_t)(nV + 1));
+    for (int32_t v = 0; v < nV; v++) label[v] = -1;
+    int32_t ncomp = 0;
+    for (int32_t s = 0; s < nV; s++) {
+        if (label[s] != -1) continue;
+        int64_t head = 0, tail = 0;
+        label[s] = s;
+        q[tail++] = s;
+        while (head < tail) {
+            int32_t c = q[head++];
+            for (int64_t e = off[c]; e < off[c + 1]; e++) {
+                int32_t d = adj[e];
+                if (label[d] == -1) {
+                    label[d] = s;
+                    q[tail++] = d;
+                }
+            }
+        }
+        ncomp++;
+    }
+    free(q);
+    return ncomp;
+}
+
+/* hornetsnest/src/Static/ConnectedComponents/CC.cu:133-156: BFS-colour the
+ * component of max_degree_id() with 0; every other vertex starts at id+1
+ * (BuildVertexEnqueue, :65-75) and the pair queue propagates the MAX colour
+ * (ColoringOperator, :86-106) to a fixed point, i.e. max(id)+1 per
+ * component.  max_degree_id is thrust::max_element: lowest id on ties
+ * (hornet/include/Core/HornetOperations/HornetQuery.i.cuh:10-21). */
+void hno_cc_reference_colors(int32_t nV, const int64_t* off, const int32_t* adj,
+                             int32_t* color) {
+    if (nV <= 0) return;
+    int32_t* lab = (int32_t*)malloc(sizeof(int32_t) * (size_t)nV);
+    int32_t* mx = (int32_t*)malloc(sizeof(int32_t) * (size_t)nV);
+    hno_cc_min_label(nV, off, adj, lab);
+    int32_t best = 0;
+    int64_t bestd = -1;
+    for (int32_t v = 0; v < nV; v++) {
+        int64_t d = off[v + 1] - off[v];
+        if (d > bestd) { bestd = d; best = v; }
+        mx[v] = -1;
+    }
+    for (int32_t v = 0; v < nV; v++)
+        if (v > mx[lab[v]]) mx[lab[v]] = v;
+    for (int32_t v = 0; v < nV; v++)
+        color[v] = (lab[v] == lab[best]) ? 0 : mx[lab[v]] + 1;
+    free(lab);
+    free(mx);
+}
+
+/* ---- k-truss ------------------------------------------------------------ */
+
+/* Support of every alive directed edge: |alive N(u) ∩ alive N(v)|
+ * (KTrussSupport.cu:212-294 intersectCount over the current graph). */
+static void supports(int32_t nV, const int64_t* off, const int32_t* adj,
+                     const unsigned char* alive, int32_t* sup) {
+    for (int32_t u = 0; u < nV; u++) {
+        for (int64_t e = off[u]; e < off[u + 1]; e++) {
+            sup[e] = 0;
+            if (!alive[e]) continue;
+            int32_t v = adj[e];
+            int64_t i = off[u], j = off[v];
+            while (i < off[u + 1] && j < off[v + 1]) {
+                if (!alive[i]) { i++; continue; }
+                if (!alive[j]) { j++; continue; }
+                if (adj[i] == adj[j]) { sup[e]++; i++; j++; }
+                else if (adj[i] < adj[j]) i++;
+                else j++;
+            }
+        }
+    }
+}
+
+/* hornetsnest/src/Static/KTruss/KTruss.cu:90-174.  run(): max_K starts at 3;
+ * findTrussOfK repeats {recompute every support; delete every edge whose
+ * support < max_K - 2} until a pass deletes nothing; when no edge is left
+ * max_K-- and stop, otherwise max_K++ on the peeled graph. */
+int32_t hno_ktruss(int32_t nV, const int64_t* off, const int32_t* adj,
+                   int32_t* edge_truss) {
+    int64_t m = off[nV];
+    unsigned char* alive = (unsigned char*)malloc((size_t)m + 1);
+    int32_t* sup = (int32_t*)malloc(sizeof(int32_t) * (size_t)(m + 1));
+    memset(alive, 1, (size_t)m);
+    for (int64_t e = 0; e < m; e++) edge_truss[e] = 2;
+    int64_t remaining = m;
+    int32_t K = 3;
+    for (;;) {
+        for (;;) {
+            if (remaining <= 0) break;
+            supports(nV, off, adj, alive, sup);
+            int64_t del = 0;
+            for (int64_t e = 0; e < m; e++)
+                if (alive[e] && sup[e] < K - 2) { alive[e] = 0; del++; }
+            if (del == 0) break;
+            remaining -= del;
+        }
+        if (remaining <= 0) { K--; break; }
+        for (int64_t e = 0; e < m; e++)
+            if (alive[e]) edge_truss[e] = K;
+        K++;
+    }
+    free(alive);
+    free(sup);
+    return K;
+}

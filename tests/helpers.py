@@ -1,0 +1,51 @@
+"""Shared input synthesis for the tests (seeded, deterministic)."""
+import numpy as np
+
+import hornet_b200 as H
+from oracle import oracle as O
+
+
+def rmat_graph(scale: int, ef: int = 16, seed: int = 1, n_vertices=None) -> O.Csr:
+    """Undirected R-MAT graph (a=.57 b=.19 c=.19), self loops and duplicates
+    removed, sorted adjacency — built by the oracle from the library's
+    host generator."""
+    n = n_vertices if n_vertices is not None else (1 << scale)
+    s, d = H.gen_rmat_host(scale, ef * n, seed, n_vertices=n)
+    return O.build_csr_undirected(n, s, d)
+
+
+def er_graph(n: int, mean_deg: float, seed: int) -> O.Csr:
+    rng = np.random.default_rng(seed)
+    m = int(n * mean_deg / 2)
+    s = rng.integers(0, n, m, dtype=np.int32)
+    d = rng.integers(0, n, m, dtype=np.int32)
+    return O.build_csr_undirected(n, s, d)
+
+
+def uniform_new_edges(g: O.Csr, k: int, seed: int):
+    """k undirected edges (both directions) absent from g and from each other,
+    no self loops."""
+    rng = np.random.default_rng(seed)
+    have = set((g.coo()[0].astype(np.int64) << 32 | g.coo()[1].astype(np.int64)).tolist())
+    out = set()
+    while len(out) < k:
+        u, v = (int(x) for x in rng.integers(0, g.nV, 2))
+        if u == v:
+            continue
+        key = (min(u, v) << 32) | max(u, v)
+        if key in out or ((u << 32) | v) in have:
+            continue
+        out.add(key)
+    a = np.array(sorted(out), np.int64)
+    u, v = (a >> 32).astype(np.int32), (a & 0xFFFFFFFF).astype(np.int32)
+    return np.concatenate([u, v]), np.concatenate([v, u])
+
+
+def sample_existing_edges(g: O.Csr, k: int, seed: int):
+    """k existing undirected edges (both directions), uniform."""
+    rng = np.random.default_rng(seed)
+    s, d = g.coo()
+    mask = s < d
+    s, d = s[mask], d[mask]
+    idx = rng.choice(len(s), size=min(k, len(s)), replace=False)
+    return np.concatenate([s[idx], d[idx]]), np.concatenate([d[idx], s[idx]])

@@ -1,0 +1,307 @@
+"""GPU parity: the sm_100a library through the C ABI against the CPU oracle
+(and the reference's own host BFS/WCC where oracle/_ref was built).
+Every comparison is bit-exact (integer results)."""
+import numpy as np
+import pytest
+
+import hornet_b200 as H
+from oracle import oracle as O
+from tests import helpers as T
+
+pytestmark = pytest.mark.gpu
+
+DEDUP_BOTH = dict(removeBatchDuplicates=True, removeGraphDuplicates=True)
+
+
+def build(g: O.Csr, sorted_adj=True) -> H.Hornet:
+    return H.Hornet(H.HornetInit(g.nV, g.nE, g.off32(), g.adj, sorted_adjacency=sorted_adj))
+
+
+def assert_same_graph(h: H.Hornet, g: O.Csr):
+    assert h.nE() == g.nE
+    s, d = h.getCOO(True)
+    gs, gd = g.coo()
+    np.testing.assert_array_equal(s, gs)
+    np.testing.assert_array_equal(d, gd)
+
+
+GRAPHS = {
+    "rmat10": lambda: T.rmat_graph(10, 16, seed=3),
+    "er2000": lambda: T.er_graph(2000, 8, seed=5),
+    "rmat12_nonpow2": lambda: T.rmat_graph(12, 8, seed=7, n_vertices=3000),
+}
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_construct_export(name):
+    g = GRAPHS[name]()
+    h = build(g)
+    assert h.nV() == g.nV
+    assert_same_graph(h, g)
+    off, adj = h.getCSR()
+    np.testing.assert_array_equal(off, g.off32())
+    np.testing.assert_array_equal(adj, g.adj)
+    deg = np.diff(g.off)
+    np.testing.assert_array_equal(h.degrees(), deg)
+    assert h.max_degree() == deg.max()
+    assert h.max_degree_id() == int(np.argmax(deg))  # lowest id on ties
+
+
+def test_construct_unsorted_input_is_sorted():
+    g = T.rmat_graph(9, 8, seed=11)
+    rng = np.random.default_rng(0)
+    adj = g.adj.copy()
+    for v in range(g.nV):
+        a, b = g.off[v], g.off[v + 1]
+        rng.shuffle(adj[a:b])
+    h = H.Hornet(H.HornetInit(g.nV, g.nE, g.off32(), adj, sorted_adjacency=False))
+    assert_same_graph(h, g)
+
+
+def test_construct_with_isolated_and_empty():
+    # vertices 0, 5, 9 isolated
+    s = np.array([1, 2, 3, 6, 7], np.int32)
+    d = np.array([2, 3, 4, 7, 8], np.int32)
+    g = O.build_csr_undirected(10, s, d)
+    h = build(g)
+    assert_same_graph(h, g)
+    e = O.Csr(np.zeros(5, np.int64), np.zeros(0, np.int32))
+    h0 = build(e)
+    assert h0.nE() == 0 and h0.nV() == 4
+    assert h0.max_degree() == 0 and h0.max_degree_id() == 0
+
+
+def test_invalid_ids_rejected_graph_unchanged():
+    g = T.rmat_graph(8, 8, seed=2)
+    h = build(g)
+    b = H.BatchUpdate(h, np.array([0, g.nV], np.int32), np.array([1, 1], np.int32))
+    with pytest.raises(H.HornetError) as ei:
+        h.insert(b)
+    assert ei.value.code == H.HN_ERR_INVALID
+    assert_same_graph(h, g)
+    with pytest.raises(H.HornetError):
+        H.Hornet(H.HornetInit(3, 1, np.array([0, 1, 1, 1], np.int32), np.array([7], np.int32)))
+
+
+@pytest.mark.parametrize("flags", [(False, False), (True, False), (False, True), (True, True)])
+def test_insert_multiset_semantics(flags):
+    """Batch with in-batch duplicates and edges already present, all four
+    removeBatchDuplicates/removeGraphDuplicates combinations."""
+    g = T.rmat_graph(9, 8, seed=4)
+    rng = np.random.default_rng(1)
+    es, ed = g.coo()
+    pick = rng.choice(len(es), 300, replace=False)
+    bs = np.concatenate([rng.integers(0, g.nV, 700).astype(np.int32), es[pick]])
+    bd = np.concatenate([rng.integers(0, g.nV, 700).astype(np.int32), ed[pick]])
+    dup = rng.choice(len(bs), 150)
+    bs = np.concatenate([bs, bs[dup]])
+    bd = np.concatenate([bd, bd[dup]])
+    h = build(g)
+    b = H.BatchUpdate(h, bs, bd)
+    applied = h.insert(b, removeBatchDuplicates=flags[0], removeGraphDuplicates=flags[1])
+    f = (O_FLAG_BATCH if flags[0] else 0) | (O_FLAG_GRAPH if flags[1] else 0)
+    ref, n = O.insert(g, bs, bd, f)
+    assert applied == n
+    assert_same_graph(h, ref)
+
+
+O_FLAG_BATCH, O_FLAG_GRAPH = 1, 2
+
+
+@pytest.mark.parametrize("dedup", [False, True])
+def test_erase_multiset_semantics(dedup):
+    g0 = T.rmat_graph(9, 8, seed=6)
+    rng = np.random.default_rng(2)
+    # make a multigraph first: insert some existing edges again
+    es, ed = g0.coo()
+    pick = rng.choice(len(es), 400, replace=False)
+    h = build(g0)
+    h.insert(H.BatchUpdate(h, es[pick], ed[pick]))
+    g, _ = O.insert(g0, es[pick], ed[pick], 0)
+    assert_same_graph(h, g)
+    # erase: existing (some duplicated in the batch) + absent edges
+    pick2 = rng.choice(len(es), 500, replace=False)
+    bs = np.concatenate([es[pick2], es[pick2[:100]], rng.integers(0, g.nV, 200).astype(np.int32)])
+    bd = np.concatenate([ed[pick2], ed[pick2[:100]], rng.integers(0, g.nV, 200).astype(np.int32)])
+    removed = h.erase(H.BatchUpdate(h, bs, bd), removeBatchDuplicates=dedup)
+    ref, n = O.erase(g, bs, bd, O_FLAG_BATCH if dedup else 0)
+    assert removed == n
+    assert_same_graph(h, ref)
+
+
+def test_update_sequence_alternating():
+    """Alternately insert and delete batches of several sizes, sorted
+    adjacency re-checked after every batch."""
+    g = T.rmat_graph(11, 16, seed=8)
+    h = build(g)
+    rng = np.random.default_rng(3)
+    for it, k in enumerate([10, 1000, 5000, 1, 20000, 300]):
+        bs = rng.integers(0, g.nV, k).astype(np.int32)
+        bd = rng.integers(0, g.nV, k).astype(np.int32)
+        b = H.BatchUpdate(h, bs, bd)
+        a = h.insert(b, **DEDUP_BOTH)
+        g, n = O.insert(g, bs, bd, 3)
+        assert a == n
+        assert_same_graph(h, g)
+        es, ed = g.coo()
+        sel = rng.choice(len(es), min(k, len(es)), replace=False)
+        b.reset(es[sel], ed[sel])
+        r = h.erase(b, removeBatchDuplicates=True)
+        g, n = O.erase(g, es[sel], ed[sel], 1)
+        assert r == n
+        assert_same_graph(h, g)
+    pool, used, free_blocks = h.memory()
+    assert used <= pool
+
+
+def test_erase_everything_then_reinsert():
+    g = T.rmat_graph(8, 8, seed=9)
+    h = build(g)
+    s, d = g.coo()
+    assert h.erase(H.BatchUpdate(h, s, d)) == g.nE
+    assert h.nE() == 0
+    assert (h.degrees() == 0).all()
+    assert h.insert(H.BatchUpdate(h, s, d)) == g.nE
+    assert_same_graph(h, g)
+
+
+@pytest.mark.parametrize("name", ["rmat10", "er2000"])
+def test_bfs(name):
+    g = GRAPHS[name]()
+    h = build(g)
+    bfs = H.BfsTopDown(h)
+    rng = np.random.default_rng(4)
+    srcs = [0] + list(rng.integers(0, g.nV, 4))
+    for s in srcs:
+        bfs.set_parameters(int(s))
+        dist = bfs.run()
+        ref, scanned = O.bfs(g, int(s))
+        np.testing.assert_array_equal(dist, ref)
+        assert bfs.stats.edges_scanned == scanned
+        assert bfs.stats.visited == int((ref != O.INF).sum())
+    if O.ref_available():
+        out, _ = bfs.run_multi(srcs)
+        np.testing.assert_array_equal(out, O.ref_bfs(g, srcs))
+
+
+def test_bfs_isolated_source():
+    s = np.array([1, 2], np.int32)
+    d = np.array([2, 3], np.int32)
+    g = O.build_csr_undirected(5, s, d)
+    h = build(g)
+    bfs = H.BfsTopDown(h)
+    bfs.set_parameters(0)
+    dist = bfs.run()
+    assert dist[0] == 0 and (dist[1:] == O.INF).all()
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_tc(name):
+    g = GRAPHS[name]()
+    h = build(g)
+    tc = H.TriangleCounting2(h)
+    tc.init()
+    total = tc.run(per_vertex=True)
+    ref, pv = O.tc(g, per_vertex=True)
+    assert total == ref
+    np.testing.assert_array_equal(tc.copyTCToHost(), pv)
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_cc(name):
+    g = GRAPHS[name]()
+    h = build(g)
+    cc = H.CC(h)
+    lab = cc.run()
+    ref, ncomp = O.cc_min_label(g)
+    np.testing.assert_array_equal(lab, ref)
+    assert cc.n_components == ncomp
+    np.testing.assert_array_equal(cc.reference_colors(), O.cc_reference_colors(g))
+    if O.ref_available():
+        np.testing.assert_array_equal(lab, O.canon_labels(O.ref_wcc(g)))
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(7, 8, 1), (8, 16, 2), (9, 8, 3)])
+def test_ktruss(scale, ef, seed):
+    g = T.rmat_graph(scale, ef, seed=seed)
+    h = build(g)
+    kt = H.KTruss(h)
+    kt.init()
+    k = kt.run()
+    rk, ret = O.ktruss(g)
+    assert k == rk
+    np.testing.assert_array_equal(kt.edge_truss, ret)
+
+
+def test_ktruss_no_triangles_and_empty():
+    # a path has no triangles: max_K = 2, every edge truss 2
+    s = np.arange(0, 9, dtype=np.int32)
+    g = O.build_csr_undirected(10, s, s + 1)
+    h = build(g)
+    kt = H.KTruss(h)
+    assert kt.run() == 2
+    assert (kt.edge_truss == 2).all()
+    e = O.Csr(np.zeros(4, np.int64), np.zeros(0, np.int32))
+    assert H.KTruss(build(e)).run() == 2
+
+
+def test_generators_match_host():
+    import torch
+    s_h, d_h = H.gen_rmat_host(12, 50000, 42, n_vertices=3000)
+    s = torch.empty(50000, dtype=torch.int32, device="cuda")
+    d = torch.empty_like(s)
+    H.gen_rmat_device(12, 50000, 42, s, d, n_vertices=3000)
+    np.testing.assert_array_equal(s.cpu().numpy(), s_h)
+    np.testing.assert_array_equal(d.cpu().numpy(), d_h)
+    csr = H.coo_to_csr_device(3000, s, d)
+    h = H.hornet_from_device_csr(csr)
+    ref = O.build_csr_undirected(3000, s_h, d_h)
+    assert_same_graph(h, ref)
+
+
+@pytest.mark.parametrize("lb,vw", [(H.HN_LB_BINARY_SEARCH, 1), (H.HN_LB_VERTEX_BASED, 1),
+                                   (H.HN_LB_VERTEX_BASED, 4), (H.HN_LB_VERTEX_BASED, 32)])
+def test_for_all_edges(lb, vw):
+    import torch
+    g = T.rmat_graph(10, 16, seed=12)
+    h = build(g)
+    out = torch.zeros(g.nV, dtype=torch.int32, device="cuda")
+    H.for_all_edges_count(h, out, lb=lb, vw=vw)
+    ref = np.bincount(g.adj, minlength=g.nV)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+    # a frontier subset with repeats and isolated vertices
+    rng = np.random.default_rng(5)
+    verts = rng.integers(0, g.nV, 500).astype(np.int32)
+    out.zero_()
+    H.for_all_edges_count(h, out, vertices=torch.from_numpy(verts).cuda(), lb=lb, vw=vw)
+    ref = np.zeros(g.nV, np.int64)
+    for v in verts:
+        np.add.at(ref, g.adj[g.off[v]:g.off[v + 1]], 1)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)
+    deg = torch.zeros(g.nV, dtype=torch.int32, device="cuda")
+    H.for_all_vertices_degree(h, deg)
+    np.testing.assert_array_equal(deg.cpu().numpy(), np.diff(g.off))
+
+
+def test_config_plain_small_end_to_end():
+    """The CPU-runnable workload: R-MAT scale 14, ef 16, seed 1; insert 10,000
+    uniform new undirected edges, delete 5,000 existing ones; BFS from 0,
+    TC and CC checked against the oracle (and the reference's host BFS/WCC)."""
+    g = T.rmat_graph(14, 16, seed=1)
+    h = build(g)
+    ins_s, ins_d = T.uniform_new_edges(g, 10000, seed=101)
+    a = h.insert(H.BatchUpdate(h, ins_s, ins_d), **DEDUP_BOTH)
+    g, n = O.insert(g, ins_s, ins_d, 3)
+    assert a == n == 20000
+    del_s, del_d = T.sample_existing_edges(g, 5000, seed=102)
+    r = h.erase(H.BatchUpdate(h, del_s, del_d), removeBatchDuplicates=True)
+    g, n = O.erase(g, del_s, del_d, 1)
+    assert r == n == 10000
+    assert_same_graph(h, g)
+    bfs = H.BfsTopDown(h)
+    bfs.set_parameters(0)
+    np.testing.assert_array_equal(bfs.run(), O.bfs(g, 0)[0])
+    assert H.TriangleCounting2(h).run() == O.tc(g)
+    np.testing.assert_array_equal(H.CC(h).run(), O.cc_min_label(g)[0])
+    if O.ref_available():
+        np.testing.assert_array_equal(bfs.distances, O.ref_bfs(g, [0])[0])
