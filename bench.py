@@ -1,0 +1,533 @@
+"""Benchmark of the Hornet dynamic-graph hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload static|update] [--scale S]
+
+static (default): undirected R-MAT (a=.57 b=.19 c=.19), scale 22, edge
+    factor 16, int32 ids, sorted adjacency; BFS TopDown from 64 seeded random
+    non-isolated sources.  One step = one BFS from the next source.
+    Headline metric: BFS GTEPS (directed edges scanned per second).
+    Also measured on the same graph: TriangleCounting2 (TC edges/s), CC
+    (edges/s) and a 1M-edge insert + erase batch (update edges/s).
+update: R-MAT scale 24; batches of 1K..10M uniform edges alternately
+    inserted and erased.  One step = one batch.  Metric: update edges/s.
+
+The graph is synthetic (seeded) and resident in HBM before timing; graph
+data (>= 0.6 GB) exceeds the 126 MB L2, so no L2 flush is needed between
+steps.  Device time is measured with CUDA events on the stream the library
+launches on, max over ranks.  With N > 1 every rank runs an independent
+replica (the path has no exchange step).
+
+--impl reference times the reference's own CPU implementation on the host
+(graph::BFS from xlib, compiled into oracle/_ref/ref_driver), rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def hbm_peak():
+    try:
+        p = json.load(open(PEAKS_FILE))
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        self.proc.wait()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                try:
+                    rows.append(f)
+                except Exception:
+                    pass
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def load_traffic(name):
+    """Per-launch DRAM bytes of kernel `name` from a committed ncu summary
+    (profiles/*.md line 'traffic_bytes_per_launch <kernel> <workload> <bytes>')."""
+    d = os.path.join(ROOT, "profiles")
+    if not os.path.isdir(d):
+        return None
+    for fn in sorted(os.listdir(d)):
+        if not fn.endswith(".md"):
+            continue
+        for line in open(os.path.join(d, fn)):
+            p = line.strip().strip("`").split()
+            if len(p) == 4 and p[0] == "traffic_bytes_per_launch" and p[1] == name:
+                return p[2], float(p[3])
+    return None
+
+
+# ---------------------------------------------------------------------------
+# graph construction
+# ---------------------------------------------------------------------------
+
+def make_graph_device(H, scale, ef, seed, device):
+    import torch
+    n = 1 << scale
+    np_pairs = ef * n
+    src = torch.empty(np_pairs, dtype=torch.int32, device=f"cuda:{device}")
+    dst = torch.empty_like(src)
+    H.gen_rmat_device(scale, np_pairs, seed, src, dst, device=device)
+    csr = H.coo_to_csr_device(n, src, dst, device=device)
+    del src, dst
+    return H.hornet_from_device_csr(csr, device=device), csr
+
+
+def pick_sources(deg, k, seed):
+    rng = np.random.default_rng(seed)
+    cand = np.nonzero(deg > 0)[0]
+    return rng.choice(cand, size=k, replace=False).astype(np.int32)
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    import hornet_b200 as H
+
+    rank, world, local = dist_env()
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = local
+    peak, peak_kind = hbm_peak()
+    stream = torch.cuda.Stream(device=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    scale = args.scale or (22 if args.workload == "static" else 24)
+    h, csr = make_graph_device(H, scale, 16, 1, dev)
+    H.lib().hn_graph_set_stream(h.handle, __import__("ctypes").c_void_p(stream.cuda_stream))
+    nV, nE = h.nV(), h.nE()
+    deg = h.degrees()
+    result = {}
+    if args.workload == "static":
+        result = bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_kind,
+                              barrier, max_over_ranks, sum_over_ranks, scale)
+    else:
+        result = bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_kind,
+                              barrier, max_over_ranks, sum_over_ranks, scale)
+    if rank == 0:
+        print(json.dumps(result))
+    del h, csr
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def event_time(stream, fn):
+    import torch
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / 1e3
+
+
+def roofline_entry(H, kernel_prefix, algo_bytes_fn, peak, peak_kind, report, workload):
+    """Dominant kernel roofline from the event-profiled pass."""
+    cand = {k: v for k, v in report.items() if k.startswith(kernel_prefix)}
+    if not cand:
+        return None
+    name, rec = max(cand.items(), key=lambda kv: kv[1]["ms"])
+    launches = rec["launches"]
+    sec = rec["ms"] / 1e3
+    algo_total = algo_bytes_fn()
+    per_launch_bytes = algo_total / launches
+    per_launch_s = sec / launches
+    achieved = per_launch_bytes / per_launch_s / 1e9
+    tr = load_traffic(name)
+    return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
+            "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "traffic": tr[1] if tr else None,
+            "algorithmic_bytes_per_launch": round(per_launch_bytes),
+            "avg_launch_us": round(per_launch_s * 1e6, 2), "launches": launches,
+            "peak_kind": peak_kind, "share_of_path": None, "workload": workload}
+
+
+def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_kind, barrier,
+                 max_over_ranks, sum_over_ranks, scale):
+    import torch
+    K, W = args.steps, args.warmup
+    sources = pick_sources(deg, 64, seed=2022 + rank)
+    out = torch.empty(nV, dtype=torch.int32, device=f"cuda:{dev}")
+    bfs = H.BfsTopDown(h)
+
+    def run_bfs(i):
+        bfs.set_parameters(int(sources[i % len(sources)]))
+        bfs.run(out=out)
+        return bfs.stats.edges_scanned, bfs.stats.visited
+
+    for i in range(W):
+        run_bfs(i)
+    # ---- timed region (device) ----
+    clocks = ClockSampler(dev)
+    clocks.start()
+    launches0 = H.kernel_launches()
+    barrier()
+    torch.cuda.synchronize()
+    scanned = [0]
+    visited = [0]
+
+    def timed():
+        for i in range(K):
+            e, v = run_bfs(W + i)
+            scanned[0] += e
+            visited[0] += v
+
+    t = event_time(stream, timed)
+    barrier()
+    launches = H.kernel_launches() - launches0
+    clk = clocks.stop()
+    t_max = max_over_ranks(t)
+    total_edges = sum_over_ranks(scanned[0])
+    value = total_edges / t_max / 1e9
+
+    # ---- e2e: public API, host output buffer, wall clock ----
+    host_out = np.empty(nV, np.int32)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    e2e_edges = 0
+    for i in range(K):
+        bfs.set_parameters(int(sources[(W + i) % len(sources)]))
+        bfs.run(out=host_out)
+        e2e_edges += bfs.stats.edges_scanned
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    e2e_value = sum_over_ranks(e2e_edges) / t_e2e / 1e9
+
+    # ---- profiled pass for the kernel roofline ----
+    H.profile_enable(True)
+    prof_edges = prof_vis = 0
+    for i in range(min(K, 16)):
+        e, v = run_bfs(W + i)
+        prof_edges += e
+        prof_vis += v
+    rep = H.profile_report()
+    H.profile_enable(False)
+    roof = roofline_entry(H, "k_bfs_expand", lambda: 8 * prof_edges + 20 * prof_vis, peak,
+                          peak_kind, rep, f"R-MAT scale {scale} BFS, {min(K, 16)} sources")
+    tot_ms = sum(v["ms"] for v in rep.values())
+    if roof:
+        roof["share_of_path"] = round(rep[roof["kernel"]]["ms"] / tot_ms, 3) if tot_ms else None
+
+    also = {}
+    if not args.no_extras and rank == 0:
+        also = static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale)
+
+    cpu = cpu_baseline_bfs(h, sources, args) if (rank == 0 and world == 1 and not args.no_cpu) else None
+    return {
+        "metric": "BFS GTEPS", "value": round(value, 4), "unit": "GTEPS", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": round(t_max * 1e3 / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic R-MAT (seeded), no dataset",
+        "config": {"workload": f"static analytics: R-MAT scale {scale}, edge factor 16, "
+                               f"a=.57 b=.19 c=.19, BFS TopDown from 64 seeded non-isolated sources",
+                   "nV": nV, "nE": nE, "sources": 64,
+                   "graph500_gteps": round(value / 2, 4),
+                   "parallelism": f"replicas x{world}",
+                   "l2": "graph data > 126 MB L2; no flush"},
+        "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 4,
+                "d2h_bytes_per_step": 4 * nV + 8},
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "also": also,
+    }
+
+
+def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale):
+    import torch
+    also = {}
+    # triangle counting (orientation + intersection per run)
+    tc = H.TriangleCounting2(h)
+    for _ in range(2):
+        tc.run()
+    reps = 3
+    t = event_time(stream, lambda: [tc.run() for _ in range(reps)]) / reps
+    H.profile_enable(True)
+    tc.run()
+    rep = H.profile_report()
+    H.profile_enable(False)
+    m_plus = nE // 2
+    # TC model bytes need sum over oriented edges of d+(u)+d+(v): computed
+    # from the exported oriented degrees on the host
+    off, adj = h.getCSR()
+    d = np.diff(off).astype(np.int64)
+    src = np.repeat(np.arange(nV, dtype=np.int64), d)
+    keep = (d[src] < d[adj]) | ((d[src] == d[adj]) & (src < adj))
+    dplus = np.bincount(src[keep], minlength=nV).astype(np.int64)
+    tc_bytes = 8 * m_plus + 4 * int((dplus[src[keep]] + dplus[adj[keep]]).sum())
+    troof = roofline_entry(H, "k_tc_count", lambda: tc_bytes, peak, peak_kind, rep,
+                           f"R-MAT scale {scale} TC")
+    also["tc"] = {"metric": "TC edges/s", "value": round(m_plus / t, 1), "unit": "edges/s",
+                  "triangles": int(tc.countTriangles()), "ms": round(t * 1e3, 3),
+                  "roofline": troof, "kernels_ms": {k: round(v["ms"], 3) for k, v in rep.items()}}
+    # connected components
+    cc = H.CC(h)
+    lab = torch.empty(nV, dtype=torch.int32, device=f"cuda:{dev}")
+    cc.run(out=lab)
+    t = event_time(stream, lambda: [cc.run(out=lab) for _ in range(reps)]) / reps
+    H.profile_enable(True)
+    cc.run(out=lab)
+    rep = H.profile_report()
+    H.profile_enable(False)
+    croof = roofline_entry(H, "k_cc_hook", lambda: 4 * nE + 8 * (nV + 1) + 8 * nV, peak,
+                           peak_kind, rep, f"R-MAT scale {scale} CC")
+    also["cc"] = {"metric": "CC edges/s", "value": round(nE / t, 1), "unit": "edges/s",
+                  "components": cc.n_components, "ms": round(t * 1e3, 3), "roofline": croof}
+    # one 1M-edge uniform insert + erase on the same graph
+    rng = np.random.default_rng(77)
+    b = 1_000_000
+    bs = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda(dev)
+    bd = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda(dev)
+    batch = H.BatchUpdate(h, bs, bd)
+    ti = event_time(stream, lambda: h.insert(batch, True, True))
+    te = event_time(stream, lambda: h.erase(batch, True))
+    also["update_1M"] = {"metric": "update edges/s", "insert": round(b / ti, 1),
+                         "erase": round(b / te, 1), "unit": "edges/s",
+                         "note": "one 1M uniform batch on the scale-22 graph; see --workload update"}
+    return also
+
+
+def cpu_baseline_bfs(h, sources, args):
+    """Reference graph::BFS (xlib/src/Graph/BFS.cpp) on the host, 1 thread,
+    on a bounded sample of the same sources."""
+    from oracle import oracle as O
+    off, adj = h.getCSR()
+    g = O.Csr(off.astype(np.int64), adj)
+    sample = [int(s) for s in sources[: args.cpu_sources]]
+    if O.ref_available():
+        sec, edges = O.ref_time_bfs(g, sample)
+        kind = "reference"
+    else:
+        t0 = time.perf_counter()
+        edges = 0
+        for s in sample:
+            edges += O.bfs(g, s)[1]
+        sec = time.perf_counter() - t0
+        kind = "port"
+    return {"value": round(edges / sec / 1e9, 5), "unit": "GTEPS", "cores": 1, "kind": kind,
+            "sample": f"graph::BFS from {len(sample)} of the 64 sources on the same graph, "
+                      f"{sec:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+# update workload
+# ---------------------------------------------------------------------------
+
+def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_kind, barrier,
+                 max_over_ranks, sum_over_ranks, scale):
+    import torch
+    K, W = args.steps, args.warmup
+    sizes = [int(x) for x in args.batch_sizes.split(",")]
+    rng = np.random.default_rng(5 + rank)
+    batches = []
+    for b in sizes:
+        bs = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda(dev)
+        bd = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda(dev)
+        batches.append((H.BatchUpdate(h, bs, bd), b, bs, bd))
+
+    def step(i):
+        bt, b, _, _ = batches[(i // 2) % len(batches)]
+        if i % 2 == 0:
+            h.insert(bt, True, True)
+        else:
+            h.erase(bt, True)
+        return b
+
+    for i in range(W + (W % 2)):
+        step(i)
+    start = W + (W % 2)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    l0 = H.kernel_launches()
+    barrier()
+    edges = [0]
+
+    def timed():
+        for i in range(K):
+            edges[0] += step(start + i)
+
+    t = event_time(stream, timed)
+    launches = H.kernel_launches() - l0
+    clk = clocks.stop()
+    t_max = max_over_ranks(t)
+    value = sum_over_ranks(edges[0]) / t_max
+    # e2e: host batch arrays copied in every step
+    host = [(bs.cpu().numpy(), bd.cpu().numpy(), b) for (_, b, bs, bd) in batches]
+    bt = H.BatchUpdate(h, host[0][0][:1], host[0][1][:1])
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e_edges = 0
+    hb = 0
+    for i in range(K):
+        s, d, b = host[((start + i) // 2) % len(host)]
+        bt.reset(s, d)
+        hb += 8 * b
+        if (start + i) % 2 == 0:
+            h.insert(bt, True, True)
+        else:
+            h.erase(bt, True)
+        e_edges += b
+    t_e2e = max_over_ranks(time.perf_counter() - t0)
+    H.profile_enable(True)
+    step(start)
+    step(start + 1)
+    rep = H.profile_report()
+    H.profile_enable(False)
+    return {
+        "metric": "update edges/s", "value": round(value, 1), "unit": "edges/s", "n_gpus": world,
+        "steps": K, "warmup": W, "ms_per_step": round(t_max * 1e3 / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic R-MAT (seeded) + uniform batches",
+        "config": {"workload": f"dynamic batch updates: R-MAT scale {scale}, ef 16; uniform "
+                               f"batches {args.batch_sizes} alternately inserted/erased",
+                   "nV": nV, "nE": nE, "parallelism": f"replicas x{world}"},
+        "e2e": {"value": round(sum_over_ranks(e_edges) / t_e2e, 1), "unit": "edges/s",
+                "h2d_bytes_per_step": hb // K, "d2h_bytes_per_step": 8},
+        "roofline": None, "kernels_ms": {k: round(v["ms"], 4) for k, v in rep.items()},
+        "cpu_baseline": None, "gpu_launches": int(launches), "clocks": clk,
+    }
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    import hornet_b200 as H
+    scale = args.scale or 22
+    n = 1 << scale
+    s, d = H.gen_rmat_host(scale, 16 * n, 1)   # host generator: no device use
+    g = O.build_csr_undirected(n, s, d)
+    del s, d
+    deg = np.diff(g.off)
+    sources = pick_sources(deg, 64, seed=2022)
+    if not O.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/ref_driver (reference graph::BFS) was not built"}))
+        return
+    K, W = args.steps, args.warmup
+    O.ref_time_bfs(g, [int(x) for x in sources[:W]])
+    per_step = 1
+    sec, edges = O.ref_time_bfs(g, [int(sources[i % 64]) for i in range(W, W + K * per_step)])
+    value = edges / sec / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": "BFS GTEPS", "value": round(value, 5), "unit": "GTEPS",
+        "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(sec * 1e3 / K, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic R-MAT (seeded), no dataset",
+        "config": {"workload": f"static analytics: R-MAT scale {scale}, edge factor 16, "
+                               f"a=.57 b=.19 c=.19, BFS TopDown from 64 seeded non-isolated sources",
+                   "nV": g.nV, "nE": g.nE},
+        "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": 1,
+                         "kind": "reference",
+                         "sample": f"graph::BFS (xlib/src/Graph/BFS.cpp), {per_step} source per step"},
+        "e2e": {"value": round(value, 5), "unit": "GTEPS", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="static", choices=["static", "update"])
+    ap.add_argument("--scale", type=int, default=0)
+    ap.add_argument("--batch-sizes", default="1000,10000,100000,1000000,10000000")
+    ap.add_argument("--cpu-sources", type=int, default=8)
+    ap.add_argument("--no-extras", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

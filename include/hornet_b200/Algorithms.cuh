@@ -1,0 +1,139 @@
+// hornetsnest algorithm classes over the C ABI, with the reference's names
+// and methods:
+//   BfsTopDown        (Static/BreadthFirstSearch/TopDown.cuh:52-70)
+//   TriangleCounting2 (Static/TriangleCounting/triangle2.cuh:18-37)
+//   CC                (Static/ConnectedComponents/CC.cuh:53-69)
+//   KTruss            (Static/KTruss/KTruss.cuh:12-92)
+// validate() compares against nothing on the host (the reference's BFS and
+// CC validators are stubs that return true, TopDown.cu:113-128,
+// CC.cu:163-203); the parity suite checks results against the CPU oracle.
+#pragma once
+
+#include <cstdint>
+#include <vector>
+
+#include "Hornet.cuh"
+#include "HornetAlg.cuh"
+
+namespace hornets_nest {
+
+using vid_t = int;
+using dist_t = int;
+using color_t = int;
+using triangle_t = unsigned long long;
+using HornetGraph = ::hornet::gpu::Hornet<int>;
+using HornetInit = ::hornet::HornetInit<int>;
+
+class BfsTopDown : public StaticAlgorithm<HornetGraph> {
+public:
+    explicit BfsTopDown(HornetGraph& h) : StaticAlgorithm(h) {
+        cudaMalloc(&d_distances, sizeof(dist_t) * (size_t)(h.nV() > 0 ? h.nV() : 1));
+    }
+    ~BfsTopDown() override { release(); }
+    void reset() override { _levels = 0; }
+    void set_parameters(vid_t source) { bfs_source = source; }
+    void run() override {
+        hn_bfs_stats_t st;
+        ::hornet::hn_check(hn_bfs(hornet.handle(), bfs_source, d_distances, HN_MEM_DEVICE, &st));
+        _levels = st.levels;
+    }
+    void release() override {
+        if (d_distances) cudaFree(d_distances);
+        d_distances = nullptr;
+    }
+    bool validate() override { return true; }
+    dist_t getLevels() const { return _levels; }
+    const dist_t* distances() const { return d_distances; }  // device
+
+private:
+    dist_t* d_distances = nullptr;
+    vid_t bfs_source = 0;
+    dist_t _levels = 0;
+};
+
+class TriangleCounting2 : public StaticAlgorithm<HornetGraph> {
+public:
+    explicit TriangleCounting2(HornetGraph& h) : StaticAlgorithm(h) {}
+    ~TriangleCounting2() override { release(); }
+    void init() {
+        cudaMalloc(&triPerVertex, sizeof(triangle_t) * (size_t)(hornet.nV() > 0 ? hornet.nV() : 1));
+        reset();
+    }
+    void reset() override { _total = 0; }
+    void run() override { run(1); }
+    void run(const int /*work_factor*/) {
+        uint64_t t = 0;
+        ::hornet::hn_check(hn_tc(hornet.handle(), (uint64_t*)triPerVertex,
+                                 HN_MEM_DEVICE, &t));
+        _total = t;
+    }
+    triangle_t countTriangles() { return _total; }
+    void copyTCToHost(triangle_t* h) {
+        cudaMemcpy(h, triPerVertex, sizeof(triangle_t) * hornet.nV(), cudaMemcpyDeviceToHost);
+    }
+    void release() override {
+        if (triPerVertex) cudaFree(triPerVertex);
+        triPerVertex = nullptr;
+    }
+    bool validate() override { return true; }
+
+private:
+    triangle_t* triPerVertex = nullptr;
+    triangle_t _total = 0;
+};
+
+class CC : public StaticAlgorithm<HornetGraph> {
+public:
+    explicit CC(HornetGraph& h) : StaticAlgorithm(h) {
+        cudaMalloc(&d_colors, sizeof(color_t) * (size_t)(h.nV() > 0 ? h.nV() : 1));
+    }
+    ~CC() override { release(); }
+    void reset() override {}
+    // the reference's colouring (giant component 0, others max(id)+1)
+    void run() override {
+        ::hornet::hn_check(hn_cc(hornet.handle(), HN_CC_REFERENCE, d_colors, HN_MEM_DEVICE,
+                                 &_ncomp));
+    }
+    // canonical labels (minimum vertex id per component)
+    void run_min_label() {
+        ::hornet::hn_check(hn_cc(hornet.handle(), HN_CC_MIN_ID, d_colors, HN_MEM_DEVICE, &_ncomp));
+    }
+    void release() override {
+        if (d_colors) cudaFree(d_colors);
+        d_colors = nullptr;
+    }
+    bool validate() override { return true; }
+    const color_t* colors() const { return d_colors; }  // device
+    int32_t components() const { return _ncomp; }
+
+private:
+    color_t* d_colors = nullptr;
+    int32_t _ncomp = 0;
+};
+
+class KTruss : public StaticAlgorithm<HornetGraph> {
+public:
+    explicit KTruss(HornetGraph& h) : StaticAlgorithm(h) {}
+    ~KTruss() override { release(); }
+    // launch-shape knobs of the reference (KTruss.cu:25-32); the sm_100a
+    // implementation sizes its own launches
+    void setInitParameters(int, int, int, int, int) {}
+    void init() { reset(); }
+    void reset() override { _maxK = 0; }
+    void run() override {
+        _edge_truss.resize((size_t)hornet.nE());
+        ::hornet::hn_check(hn_ktruss(hornet.handle(), &_maxK,
+                                     _edge_truss.empty() ? nullptr : _edge_truss.data(),
+                                     HN_MEM_HOST));
+    }
+    vid_t getMaxK() const { return _maxK; }
+    const std::vector<int32_t>& edgeTruss() const { return _edge_truss; }
+    void release() override {}
+    bool validate() override { return true; }
+
+private:
+    int32_t _maxK = 0;
+    std::vector<int32_t> _edge_truss;
+};
+
+}  // namespace hornets_nest

@@ -1,0 +1,43 @@
+"""GPU: the C++ shim (include/hornet_b200/hornet.cuh) used the way the
+reference's own tests and algorithms use the reference API — compiled for
+sm_100a into hornet_b200/_lib/hn_shim_test — checked against the oracle."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests import helpers as T
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "hornet_b200", "_lib", "hn_shim_test")
+
+
+def test_shim_reference_style_program():
+    assert os.path.exists(EXE), "build the shim test: make -C tests/shim"
+    g = T.rmat_graph(10, 8, seed=31)
+    rng = np.random.default_rng(9)
+    bs = rng.integers(0, g.nV, 2000).astype(np.int32)
+    bd = rng.integers(0, g.nV, 2000).astype(np.int32)
+    with tempfile.TemporaryDirectory() as d:
+        cp, bp, op = (os.path.join(d, x) for x in ("g.csr", "b.bin", "out"))
+        O.write_csr(cp, g)
+        with open(bp, "wb") as f:
+            np.array([len(bs)], np.int64).tofile(f)
+            bs.tofile(f)
+            bd.tofile(f)
+        r = subprocess.run([EXE, cp, bp, op], capture_output=True, text=True, timeout=120)
+        assert r.returncode == 0, r.stdout + r.stderr
+        assert "insert PASSED" in r.stdout
+        assert "erase PASSED" in r.stdout
+        assert "bfs_class PASSED" in r.stdout
+        dist = np.fromfile(op + ".bfs", np.int32)
+        np.testing.assert_array_equal(dist, O.bfs(g, 0)[0])
+        cnt = np.fromfile(op + ".deg", np.int32)
+        np.testing.assert_array_equal(cnt, np.diff(g.off))
+        ncomp = int(r.stdout.split("cc_components")[1].split()[0])
+        assert ncomp == O.cc_min_label(g)[1]
