@@ -412,6 +412,8 @@ void free_graph_object(hn_graph* g) {
     for (int c = 0; c < kNumClasses; c++)
         if (g->fl[c]) cudaFreeAsync(g->fl[c], g->stream);
     for (auto& p : g->scratch) p.release(g->stream);
+    free_bfs_graph(g->bfs);
+    g->bfs = nullptr;
     if (g->vtab) cudaFreeAsync(g->vtab, g->stream);
     if (g->pool) cudaFreeAsync(g->pool, g->stream);
     if (g->stream) cudaStreamSynchronize(g->stream);
@@ -422,6 +424,7 @@ void free_graph_object(hn_graph* g) {
     cudaFree(g->d_scalar);
     if (g->own_stream && g->stream) cudaStreamDestroy(g->stream);
     delete g;
+    (void)cudaGetLastError();
 }
 
 // Copy a CSR into device buffers with int64 offsets.

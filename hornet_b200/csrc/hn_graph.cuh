@@ -4,6 +4,7 @@
 #include <atomic>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 #include "hn_internal.cuh"
 
@@ -85,10 +86,15 @@ struct DeviceInfo {
     int max_threads_per_sm = 2048;
 };
 
+struct BfsGraph;
+void free_bfs_graph(BfsGraph* bg);
+
 }  // namespace hn
 
 // C ABI bodies: exceptions become HN_ERR_* codes, never process exits.
-#define HN_API_BEGIN try {
+// A stale error left by an unchecked call (e.g. a free in a destructor) is
+// cleared on entry so it is never reported against this call.
+#define HN_API_BEGIN try { (void)cudaGetLastError();
 #define HN_API_END                                                   \
     }                                                                \
     catch (const hn::Error& e) {                                     \
@@ -133,10 +139,12 @@ struct hn_graph {
     long long* d_scalar = nullptr;        // device scalars (16)
 
     hn::Persist scratch[8];               // reusable device scratch
+    hn::BfsGraph* bfs = nullptr;          // instantiated BFS CUDA graph
 };
 
 struct hn_batch {
     hn_graph* g = nullptr;
+    int device = 0;          // kept so destroy never touches the graph
     int64_t n = 0;
     int32_t* src = nullptr;  // device copies (owned)
     int32_t* dst = nullptr;

@@ -449,6 +449,7 @@ int hn_batch_create(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t*
     *out = nullptr;
     hn_batch* b = new hn_batch();
     b->g = g;
+    b->device = g->device;
     int rc = hn_batch_reset(b, n, src, dst, mem);
     if (rc != HN_OK) {
         delete b;
@@ -495,10 +496,13 @@ int hn_batch_size(const hn_batch_t* b, int64_t* n) {
 int hn_batch_destroy(hn_batch_t* b) {
     HN_API_BEGIN
     if (!b) return HN_OK;
-    cudaSetDevice(b->g->device);
+    // the batch may outlive its graph (garbage-collection order), so only
+    // its own device id is used here
+    cudaSetDevice(b->device);
     if (b->src) cudaFree(b->src);
     if (b->dst) cudaFree(b->dst);
     delete b;
+    (void)cudaGetLastError();
     HN_API_END
 }
 
