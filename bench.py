@@ -46,6 +46,38 @@ def hbm_peak():
         return FALLBACK_HBM, "fallback"
 
 
+class Dist:
+    """Rank aggregation for the replica benchmark: device time is the MAX
+    over ranks, work is the SUM (works with nccl on cuda tensors and with
+    gloo on cpu tensors)."""
+
+    def __init__(self, world: int, device: str = "cpu"):
+        self.world = world
+        self.device = device
+
+    def barrier(self):
+        if self.world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def _reduce(self, x, op):
+        if self.world == 1:
+            return x
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([float(x)], dtype=torch.float64, device=self.device)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    def max(self, x):
+        import torch.distributed as dist
+        return self._reduce(x, dist.ReduceOp.MAX) if self.world > 1 else x
+
+    def sum(self, x):
+        import torch.distributed as dist
+        return self._reduce(x, dist.ReduceOp.SUM) if self.world > 1 else x
+
+
 def dist_env():
     return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
         int(os.environ.get("LOCAL_RANK", "0"))
@@ -151,23 +183,8 @@ def run_ours(args):
     peak, peak_kind = hbm_peak()
     stream = torch.cuda.Stream(device=dev)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    def sum_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{dev}")
-        dist.all_reduce(t, op=dist.ReduceOp.SUM)
-        return float(t.item())
+    d = Dist(world, f"cuda:{dev}")
+    barrier, max_over_ranks, sum_over_ranks = d.barrier, d.max, d.sum
 
     scale = args.scale or (22 if args.workload == "static" else 24)
     h, csr = make_graph_device(H, scale, 16, 1, dev)
