@@ -8,30 +8,35 @@
 //
 // Here a whole BFS is ONE CUDA-graph launch: an init kernel, then a
 // conditional WHILE node whose body is a single persistent expand kernel.
-//   * The frontier carries, next to each vertex, the exclusive prefix of the
-//     frontier's degrees.  It is produced by the enqueue itself: one 64-bit
-//     atomicAdd of (degree << 32 | 1) per warp hands out the queue slot (low
-//     word) and the edge offset (high word) together, so the offsets are
-//     ordered like the slots and no scan pass is needed.
-//   * The expand kernel walks the frontier's edges with the merge-path load
-//     balancer (tiles over edges + vertex boundaries, segment ends and
-//     adjacency bases staged in shared memory).
-//   * A vertex is claimed with atomicOr on a visited bitmap (nV/8 bytes,
-//     L2-resident), so it is enqueued exactly once and its distance written
-//     once.
-//   * The last CTA to finish a level (ticket counter) seals the next
-//     frontier and sets the WHILE condition with cudaGraphSetConditional, so
-//     the host never waits between levels.  The loop also stops after nV
-//     levels, so it always terminates.
+//   * Frontier entries are (vertex, adjacency base, edge offset).  The edge
+//     offset is the exclusive prefix of the frontier's degrees; it comes out
+//     of the enqueue itself: one 64-bit atomicAdd of (degree << 32 | 1) per
+//     warp hands out the queue slot (low word) and the edge offset (high
+//     word) together, so offsets are ordered like slots and no scan runs.
+//   * The frontier's edge space is cut into chunks of kChunk edges.  The
+//     vertex that covers the first edge of each chunk records itself in
+//     chunk_seg[] when it is enqueued, so the expand kernel finds a chunk's
+//     vertex window with two loads — no search in global memory.  Only
+//     vertices with at least one edge are queued, so a chunk spans at most
+//     kChunk + 1 queue entries.
+//   * A CTA stages the window's (edge offset, adjacency base) pairs in
+//     shared memory; each thread takes kIpt consecutive edges, finds its
+//     first vertex by a shared-memory binary search, then issues all kIpt
+//     neighbour loads and all kIpt visited-bitmap probes back to back (high
+//     memory-level parallelism), and claims new vertices with atomicOr on
+//     the bitmap (nV/8 bytes, L2-resident): each vertex is enqueued and its
+//     distance written exactly once.
+//   * The last CTA of a level (ticket counter) seals the next frontier and
+//     sets the WHILE condition with cudaGraphSetConditional; the loop also
+//     stops after nV levels, so it always terminates.
 // Distances equal the reference's: level-synchronous, INF = INT32_MAX.
-#include <cub/cub.cuh>
-
 #include "hn_graph.cuh"
 
 namespace hn {
 
 constexpr int kBfsBlock = 256;
-constexpr int kBfsItems = 8;
+constexpr int kIpt = 12;                         // edges per thread per chunk
+constexpr int kChunk = kBfsBlock * kIpt;         // edges per chunk
 
 struct BfsState {
     unsigned long long cnt[3];   // frontier counters: (edge total << 32) | size
@@ -45,16 +50,21 @@ struct BfsState {
     const VRec* vtab;
     const int32_t* pool;
     int32_t* q[2];               // frontier vertices
-    unsigned* qoff[2];           // exclusive degree prefix of the frontier
+    long long* qbase[2];         // their adjacency base in the pool
+    unsigned* qoff[2];           // exclusive degree prefix (edge offset)
+    int32_t* chunk[2];           // queue slot covering each chunk's first edge
     unsigned* bitmap;            // visited bits
 };
 
 struct BfsGraph {
     int nV = -1;
+    long long nchunk_cap = 0;
     BfsState* state = nullptr;      // device
     BfsState* h_state = nullptr;    // pinned
     int32_t* qbuf = nullptr;
+    long long* qbasebuf = nullptr;
     unsigned* qoffbuf = nullptr;
+    int32_t* chunkbuf = nullptr;
     unsigned* bitmap = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -62,9 +72,15 @@ struct BfsGraph {
 
 namespace {
 
-using Tile = LbTile<kBfsBlock, kBfsItems>;
+// Record queue slot `pos` as the owner of every chunk whose first edge lies
+// in [off, off + d).
+__device__ __forceinline__ void mark_chunks(int32_t* chunk, unsigned off, unsigned d, int pos) {
+    unsigned c0 = (off + kChunk - 1) / kChunk;
+    unsigned c1 = (off + d - 1) / kChunk;
+    for (unsigned c = c0; c <= c1; c++) chunk[c] = pos;
+}
 
-__global__ void k_bfs2_init(BfsState* st) {
+__global__ void k_bfs3_init(BfsState* st) {
     const int nV = st->nV;
     const int src = st->src;
     int32_t* dist = st->dist;
@@ -75,12 +91,21 @@ __global__ void k_bfs2_init(BfsState* st) {
         dist[i] = i == src ? 0 : kInf;
         if (i < nwords) bm[i] = (i == src / 32) ? (1u << (src & 31)) : 0u;
     }
+    VRec r = st->vtab[src];
+    unsigned d = (unsigned)r.deg;
+    // chunk marks of a high-degree source are spread over the grid
+    if (d > 0) {
+        unsigned nc = (d - 1) / kChunk + 1;
+        for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
+             c += (long long)gridDim.x * blockDim.x)
+            st->chunk[0][c] = 0;
+    }
     if (blockIdx.x == 0 && threadIdx.x == 0) {
-        unsigned d = (unsigned)st->vtab[src].deg;
         st->q[0][0] = src;
+        st->qbase[0][0] = r.off;
         st->qoff[0][0] = 0;
-        st->qoff[0][1] = d;
-        st->cnt[0] = ((unsigned long long)d << 32) | 1ull;
+        st->qoff[0][d > 0 ? 1 : 0] = d;
+        st->cnt[0] = d > 0 ? (((unsigned long long)d << 32) | 1ull) : 0ull;
         st->cnt[1] = 0;
         st->cnt[2] = 0;
         st->level = 1;
@@ -91,72 +116,129 @@ __global__ void k_bfs2_init(BfsState* st) {
 }
 
 __global__ void __launch_bounds__(kBfsBlock)
-k_bfs2_expand(BfsState* st, cudaGraphConditionalHandle cond) {
-    __shared__ Tile t;
-    __shared__ long long s_base[Tile::TILE + 1];
+k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
+    __shared__ unsigned s_start[kChunk + 2];   // window edge offsets (+ end)
+    __shared__ long long s_base[kChunk + 1];   // pool index = s_base + edge
+    __shared__ int s_nw;
     const int level = st->level;
     const int it = level - 1;
     const unsigned long long cin = st->cnt[it % 3];
     unsigned long long* cout = &st->cnt[(it + 1) % 3];
     if (blockIdx.x == 0 && threadIdx.x == 0) st->cnt[(it + 2) % 3] = 0;
-    const long long nq = (long long)(cin & 0xFFFFFFFFull);
-    const long long total = (long long)(cin >> 32);
-    const int32_t* q = st->q[it & 1];
-    const unsigned* prefix = st->qoff[it & 1];
-    int32_t* nqv = st->q[(it + 1) & 1];
-    unsigned* nqoff = st->qoff[(it + 1) & 1];
+    const int nq = (int)(cin & 0xFFFFFFFFull);
+    const unsigned total = (unsigned)(cin >> 32);
+    const int cur = it & 1, nxt = cur ^ 1;
+    const long long* qbase = st->qbase[cur];
+    const unsigned* qoff = st->qoff[cur];
+    const int32_t* chunk = st->chunk[cur];
+    int32_t* nqv = st->q[nxt];
+    long long* nqbase = st->qbase[nxt];
+    unsigned* nqoff = st->qoff[nxt];
+    int32_t* nchunk = st->chunk[nxt];
     const VRec* vtab = st->vtab;
     const int32_t* pool = st->pool;
     unsigned* bm = st->bitmap;
     int32_t* dist = st->dist;
     const int lane = threadIdx.x & 31;
+    int found = 0;
 
-    const long long ntiles = (total + nq + Tile::TILE - 1) / Tile::TILE;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, prefix, nq, total, tile);
-        for (int b = threadIdx.x; b <= t.nends; b += kBfsBlock) {
-            long long s = t.seg0 + b;
-            if (s < nq) s_base[b] = vtab[q[s]].off - t.seg_start(b);
+    const unsigned nchunks = (total + kChunk - 1) / kChunk;
+    for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const unsigned e0 = c * kChunk;
+        const unsigned e1 = e0 + kChunk < total ? e0 + kChunk : total;
+        const int s0 = chunk[c];
+        const int s1 = c + 1 < nchunks ? chunk[c + 1] : nq - 1;   // inclusive
+        const int nw = s1 - s0 + 1;
+        for (int j = threadIdx.x; j <= nw; j += kBfsBlock) {
+            int s = s0 + j;
+            unsigned so = qoff[s];        // qoff[nq] is the sealed total
+            s_start[j] = so;
+            if (j < nw) s_base[j] = qbase[s] - (long long)so;
         }
+        if (threadIdx.x == 0) s_nw = nw;
         __syncthreads();
-        for (int i0 = 0; i0 < n; i0 += kBfsBlock) {
-            int i = i0 + threadIdx.x;
-            bool claim = false;
-            int w = 0;
-            unsigned d = 0;
-            if (i < n) {
-                w = pool[s_base[t.seg[i]] + t.item0 + i];
-                unsigned bit = 1u << (w & 31);
-                unsigned* word = bm + (w >> 5);
-                if (!(__ldcg(word) & bit)) claim = !(atomicOr(word, bit) & bit);
-                if (claim) d = (unsigned)vtab[w].deg;
+        // this thread's edges [a, b)
+        const unsigned a = e0 + threadIdx.x * kIpt;
+        const unsigned b = a + kIpt < e1 ? a + kIpt : e1;
+        int w[kIpt];
+        bool claim[kIpt];
+        if (a < b) {
+            int lo = 0, hi = s_nw;        // last j with s_start[j] <= a
+            while (hi - lo > 1) {
+                int mid = (lo + hi) >> 1;
+                if (s_start[mid] <= a) lo = mid; else hi = mid;
             }
-            // warp-aggregated enqueue: slot and edge offset from one atomic
-            unsigned ballot = __ballot_sync(0xFFFFFFFFu, claim);
-            if (ballot) {
-                unsigned incl = d;
-                for (int o = 1; o < 32; o <<= 1) {
-                    unsigned x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                    if (lane >= o) incl += x;
+            int j = lo;
+#pragma unroll
+            for (int k = 0; k < kIpt; k++) {
+                unsigned e = a + k;
+                if (e < b) {
+                    while (s_start[j + 1] <= e) j++;
+                    w[k] = __ldg(pool + s_base[j] + e);
+                } else {
+                    w[k] = -1;
                 }
-                unsigned wsum = __shfl_sync(0xFFFFFFFFu, incl, 31);
-                int leader = __ffs(ballot) - 1;
-                unsigned long long base = 0;
-                if (lane == leader)
-                    base = atomicAdd(cout, ((unsigned long long)wsum << 32) |
-                                               (unsigned long long)__popc(ballot));
-                base = __shfl_sync(0xFFFFFFFFu, base, leader);
-                if (claim) {
-                    unsigned pos = (unsigned)(base & 0xFFFFFFFFull) +
-                                   __popc(ballot & ((1u << lane) - 1));
-                    nqv[pos] = w;
-                    nqoff[pos] = (unsigned)(base >> 32) + incl - d;
-                    dist[w] = level;
+            }
+            unsigned word[kIpt];
+#pragma unroll
+            for (int k = 0; k < kIpt; k++)
+                word[k] = w[k] >= 0 ? __ldcg(bm + (w[k] >> 5)) : 0xFFFFFFFFu;
+#pragma unroll
+            for (int k = 0; k < kIpt; k++) {
+                claim[k] = false;
+                if (w[k] >= 0 && !(word[k] & (1u << (w[k] & 31)))) {
+                    unsigned bit = 1u << (w[k] & 31);
+                    claim[k] = !(atomicOr(bm + (w[k] >> 5), bit) & bit);
                 }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kIpt; k++) claim[k] = false;
+        }
+        // enqueue: one warp-aggregated 64-bit atomic per round
+#pragma unroll
+        for (int k = 0; k < kIpt; k++) {
+            unsigned ballot = __ballot_sync(0xFFFFFFFFu, claim[k]);
+            if (!ballot) continue;
+            VRec r;
+            r.deg = 0;
+            r.off = 0;
+            if (claim[k]) {
+                r = vtab[w[k]];
+                dist[w[k]] = level;
+                found++;
+            }
+            unsigned d = (unsigned)r.deg;
+            bool q_it = claim[k] && d > 0;          // only vertices with edges
+            unsigned qb = __ballot_sync(0xFFFFFFFFu, q_it);
+            if (!qb) continue;
+            unsigned incl = q_it ? d : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                unsigned x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += x;
+            }
+            unsigned wsum = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            int leader = __ffs(qb) - 1;
+            unsigned long long base = 0;
+            if (lane == leader)
+                base = atomicAdd(cout, ((unsigned long long)wsum << 32) |
+                                           (unsigned long long)__popc(qb));
+            base = __shfl_sync(0xFFFFFFFFu, base, leader);
+            if (q_it) {
+                int pos = (int)(base & 0xFFFFFFFFull) + __popc(qb & ((1u << lane) - 1));
+                unsigned off = (unsigned)(base >> 32) + incl - d;
+                nqv[pos] = w[k];
+                nqbase[pos] = r.off;
+                nqoff[pos] = off;
+                mark_chunks(nchunk, off, d, pos);
             }
         }
         __syncthreads();
     }
+    // visited count: one atomic per warp
+    for (int o = 16; o; o >>= 1) found += __shfl_down_sync(0xFFFFFFFFu, found, o);
+    if (lane == 0 && found) atomicAdd((unsigned long long*)&st->visited, (unsigned long long)found);
     // the last CTA seals the next frontier and decides whether to loop
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -164,11 +246,10 @@ k_bfs2_expand(BfsState* st, cudaGraphConditionalHandle cond) {
         unsigned tk = atomicAdd(&st->ticket, 1u);
         if (tk == gridDim.x - 1) {
             __threadfence();
-            unsigned long long c = atomicAdd(cout, 0ull);
-            unsigned nn = (unsigned)(c & 0xFFFFFFFFull);
-            nqoff[nn] = (unsigned)(c >> 32);
+            unsigned long long cn = atomicAdd(cout, 0ull);
+            unsigned nn = (unsigned)(cn & 0xFFFFFFFFull);
+            nqoff[nn] = (unsigned)(cn >> 32);
             st->ticket = 0;
-            st->visited += nn;
             st->scanned += total;
             st->level = level + 1;
             cudaGraphSetConditional(cond, (nn > 0 && level < st->nV) ? 1u : 0u);
@@ -178,20 +259,23 @@ k_bfs2_expand(BfsState* st, cudaGraphConditionalHandle cond) {
 
 void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
     const int nV = g->nV;
+    const long long nchunk_cap = g->nE / kChunk + 4;
     HN_CUDA(cudaMalloc((void**)&bg.state, sizeof(BfsState)));
     HN_CUDA(cudaMallocHost((void**)&bg.h_state, sizeof(BfsState)));
     HN_CUDA(cudaMalloc((void**)&bg.qbuf, sizeof(int32_t) * 2 * ((size_t)nV + 1)));
+    HN_CUDA(cudaMalloc((void**)&bg.qbasebuf, sizeof(long long) * 2 * ((size_t)nV + 1)));
     HN_CUDA(cudaMalloc((void**)&bg.qoffbuf, sizeof(unsigned) * 2 * ((size_t)nV + 2)));
+    HN_CUDA(cudaMalloc((void**)&bg.chunkbuf, sizeof(int32_t) * 2 * (size_t)nchunk_cap));
     HN_CUDA(cudaMalloc((void**)&bg.bitmap, sizeof(unsigned) * (((size_t)nV + 31) / 32 + 1)));
     bg.nV = nV;
+    bg.nchunk_cap = nchunk_cap;
 
     HN_CUDA(cudaGraphCreate(&bg.graph, 0));
-    // init node
     cudaGraphNode_t init_node, cond_node, body_node;
     {
         void* args[] = {&bg.state};
         cudaKernelNodeParams p = {};
-        p.func = (void*)k_bfs2_init;
+        p.func = (void*)k_bfs3_init;
         p.gridDim = dim3((unsigned)grid_for(g, nV, 256));
         p.blockDim = dim3(256);
         p.kernelParams = args;
@@ -209,8 +293,8 @@ void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
     {
         void* args[] = {&bg.state, &handle};
         cudaKernelNodeParams p = {};
-        p.func = (void*)k_bfs2_expand;
-        p.gridDim = dim3((unsigned)g->info.sms * 4);
+        p.func = (void*)k_bfs3_expand;
+        p.gridDim = dim3((unsigned)g->info.sms * 3);
         p.blockDim = dim3(kBfsBlock);
         p.kernelParams = args;
         HN_CUDA(cudaGraphAddKernelNode(&body_node, body, nullptr, 0, &p));
@@ -227,7 +311,9 @@ void free_bfs_graph(BfsGraph* bg) {
     if (bg->state) cudaFree(bg->state);
     if (bg->h_state) cudaFreeHost(bg->h_state);
     if (bg->qbuf) cudaFree(bg->qbuf);
+    if (bg->qbasebuf) cudaFree(bg->qbasebuf);
     if (bg->qoffbuf) cudaFree(bg->qoffbuf);
+    if (bg->chunkbuf) cudaFree(bg->chunkbuf);
     if (bg->bitmap) cudaFree(bg->bitmap);
     delete bg;
 }
@@ -235,7 +321,9 @@ void free_bfs_graph(BfsGraph* bg) {
 namespace {
 
 BfsGraph& bfs_graph_of(hn_graph* g) {
-    if (g->bfs && g->bfs->nV != g->nV) {
+    // rebuilt when the vertex count changes or the edge count outgrows the
+    // chunk table
+    if (g->bfs && (g->bfs->nV != g->nV || g->nE / kChunk + 4 > g->bfs->nchunk_cap)) {
         HN_CUDA(cudaStreamSynchronize(g->stream));
         free_bfs_graph(g->bfs);
         g->bfs = nullptr;
@@ -277,11 +365,20 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.pool = g->pool;
         h.q[0] = bg.qbuf;
         h.q[1] = bg.qbuf + nV + 1;
+        h.qbase[0] = bg.qbasebuf;
+        h.qbase[1] = bg.qbasebuf + nV + 1;
         h.qoff[0] = bg.qoffbuf;
         h.qoff[1] = bg.qoffbuf + nV + 2;
+        h.chunk[0] = bg.chunkbuf;
+        h.chunk[1] = bg.chunkbuf + bg.nchunk_cap;
         h.bitmap = bg.bitmap;
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
+        // profiling records the whole graph (one init + one expand per
+        // level) under the name of its dominant kernel
+        cudaEvent_t ev0 = nullptr;
+        if (g_profiling) profile_begin(s, &ev0);
         HN_CUDA(cudaGraphLaunch(bg.exec, s));
+        if (ev0) profile_end("k_bfs3_expand", s, ev0);
         count_launch(2);
         HN_CUDA(cudaMemcpyAsync(bg.h_state, bg.state, sizeof(BfsState), cudaMemcpyDeviceToHost, s));
         if (mem == HN_MEM_HOST)
