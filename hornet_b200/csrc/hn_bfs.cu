@@ -115,11 +115,13 @@ __global__ void k_bfs3_init(BfsState* st) {
     }
 }
 
-__global__ void __launch_bounds__(kBfsBlock)
+__global__ void __launch_bounds__(kBfsBlock, 2)
 k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
     __shared__ unsigned s_start[kChunk + 2];   // window edge offsets (+ end)
     __shared__ long long s_base[kChunk + 1];   // pool index = s_base + edge
     __shared__ int s_nw;
+    __shared__ unsigned long long s_wsum[kBfsBlock / 32];
+    __shared__ unsigned long long s_cbase;
     const int level = st->level;
     const int it = level - 1;
     const unsigned long long cin = st->cnt[it % 3];
@@ -195,43 +197,64 @@ k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
 #pragma unroll
             for (int k = 0; k < kIpt; k++) claim[k] = false;
         }
-        // enqueue: one warp-aggregated 64-bit atomic per round
+        // claimed vertices: records loaded together, distances written
+        long long roff[kIpt];
+        unsigned rdeg[kIpt];
+        unsigned long long mine = 0;   // (degree sum << 32) | queued count
 #pragma unroll
         for (int k = 0; k < kIpt; k++) {
-            unsigned ballot = __ballot_sync(0xFFFFFFFFu, claim[k]);
-            if (!ballot) continue;
-            VRec r;
-            r.deg = 0;
-            r.off = 0;
+            rdeg[k] = 0;
+            roff[k] = 0;
             if (claim[k]) {
-                r = vtab[w[k]];
+                VRec r = vtab[w[k]];
+                rdeg[k] = (unsigned)r.deg;
+                roff[k] = r.off;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < kIpt; k++) {
+            if (claim[k]) {
                 dist[w[k]] = level;
                 found++;
+                if (rdeg[k]) mine += ((unsigned long long)rdeg[k] << 32) | 1ull;  // queued
             }
-            unsigned d = (unsigned)r.deg;
-            bool q_it = claim[k] && d > 0;          // only vertices with edges
-            unsigned qb = __ballot_sync(0xFFFFFFFFu, q_it);
-            if (!qb) continue;
-            unsigned incl = q_it ? d : 0;
+        }
+        // CTA-wide exclusive scan of the packed counters; ONE atomic per
+        // chunk reserves both the queue slots and the edge range
+        unsigned long long incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += x;
+        }
+        const int warp = threadIdx.x >> 5;
+        if (lane == 31) s_wsum[warp] = incl;
+        __syncthreads();
+        if (threadIdx.x < 32) {
+            unsigned long long v = threadIdx.x < kBfsBlock / 32 ? s_wsum[threadIdx.x] : 0ull;
+            unsigned long long vi = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                unsigned x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                if (lane >= o) incl += x;
+                unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, vi, o);
+                if (lane >= o) vi += x;
             }
-            unsigned wsum = __shfl_sync(0xFFFFFFFFu, incl, 31);
-            int leader = __ffs(qb) - 1;
-            unsigned long long base = 0;
-            if (lane == leader)
-                base = atomicAdd(cout, ((unsigned long long)wsum << 32) |
-                                           (unsigned long long)__popc(qb));
-            base = __shfl_sync(0xFFFFFFFFu, base, leader);
-            if (q_it) {
-                int pos = (int)(base & 0xFFFFFFFFull) + __popc(qb & ((1u << lane) - 1));
-                unsigned off = (unsigned)(base >> 32) + incl - d;
+            if (threadIdx.x < kBfsBlock / 32) s_wsum[threadIdx.x] = vi - v;   // exclusive
+            unsigned long long tot = __shfl_sync(0xFFFFFFFFu, vi, 31);
+            if (threadIdx.x == 0) s_cbase = tot ? atomicAdd(cout, tot) : 0ull;
+        }
+        __syncthreads();
+        unsigned long long at = s_cbase + s_wsum[warp] + (incl - mine);
+        int pos = (int)(at & 0xFFFFFFFFull);
+        unsigned off = (unsigned)(at >> 32);
+#pragma unroll
+        for (int k = 0; k < kIpt; k++) {
+            if (claim[k] && rdeg[k]) {
                 nqv[pos] = w[k];
-                nqbase[pos] = r.off;
+                nqbase[pos] = roff[k];
                 nqoff[pos] = off;
-                mark_chunks(nchunk, off, d, pos);
+                mark_chunks(nchunk, off, rdeg[k], pos);
+                pos++;
+                off += rdeg[k];
             }
         }
         __syncthreads();
@@ -294,7 +317,7 @@ void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
         void* args[] = {&bg.state, &handle};
         cudaKernelNodeParams p = {};
         p.func = (void*)k_bfs3_expand;
-        p.gridDim = dim3((unsigned)g->info.sms * 3);
+        p.gridDim = dim3((unsigned)g->info.sms * 2);
         p.blockDim = dim3(kBfsBlock);
         p.kernelParams = args;
         HN_CUDA(cudaGraphAddKernelNode(&body_node, body, nullptr, 0, &p));

@@ -7,12 +7,21 @@
 //
 // Here: lock-free union-find in the style of ECL-CC (Jaiganesh & Burtscher,
 // "A High-Performance Connected Components Implementation for GPUs",
-// HPDC 2018): every undirected edge (u > v) hooks the larger root under the
-// smaller one with atomicCAS, finds use intermediate pointer jumping, and
-// a final pass points every vertex at its root.  Parents only ever point to
-// smaller ids, so each root is the minimum id of its component: the labels
-// come out canonical with no relabelling.  One merge-path balanced pass over
-// the edges, two grid-stride passes over the vertices, no host round trips.
+// HPDC 2018) — a link hangs the larger root under the smaller one with
+// atomicCAS, finds use intermediate pointer jumping — driven by the
+// neighbour-sampling schedule of Afforest (Sutton, Ben-Nun & Barak,
+// IPDPS 2018):
+//   1. every vertex links with its first kSample neighbours;
+//   2. compress; the most frequent root among 256 evenly spaced vertices
+//      is taken as the giant component G;
+//   3. only vertices outside G (with more than kSample neighbours) link
+//      with the rest of their neighbours — an edge from G to a vertex
+//      outside G is seen from the outside end, edges inside G are already
+//      implied — so on power-law graphs most edges are never read;
+//   4. compress and count roots.
+// Parents only ever point to smaller ids, so each root is the minimum id of
+// its component: the labels come out canonical with no relabelling, and no
+// step waits on the host.
 // The reference's own colouring is produced from the same roots on request
 // (giant component of max_degree_id -> 0, others max(id)+1).
 #include "hn_graph.cuh"
@@ -21,7 +30,6 @@ namespace hn {
 namespace {
 
 constexpr int kB = 256;
-using Tile = LbTile<kB, 8>;
 
 __device__ __forceinline__ int find_root(int* __restrict__ parent, int v) {
     int cur = parent[v];
@@ -42,37 +50,82 @@ __global__ void k_cc_init(int* __restrict__ parent, int nV) {
         parent[v] = (int)v;
 }
 
-__global__ void __launch_bounds__(kB)
-k_cc_hook(const long long* __restrict__ prefix, int nV, const VRec* __restrict__ vtab,
-          const int32_t* __restrict__ pool, int* __restrict__ parent) {
-    __shared__ Tile t;
-    __shared__ long long s_base[Tile::TILE + 1];
-    const long long total = prefix[nV];
-    const long long ntiles = (total + nV + Tile::TILE - 1) / Tile::TILE;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, prefix, (long long)nV, total, tile);
-        for (int b = threadIdx.x; b <= t.nends; b += kB) {
-            long long u = t.seg0 + b;
-            if (u < nV) s_base[b] = vtab[u].off - t.seg_start(b);
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += kB) {
-            long long e = t.item0 + i;
-            int b = t.seg[i];
-            int u = (int)(t.seg0 + b);
-            int v = pool[s_base[b] + e];
-            if (v >= u) continue;  // each undirected edge once
-            int ru = find_root(parent, u);
-            int rv = find_root(parent, v);
-            while (ru != rv) {
-                if (ru < rv) { int x = ru; ru = rv; rv = x; }
-                // ru > rv: hang ru under rv if ru is still a root
-                int old = atomicCAS(parent + ru, ru, rv);
-                if (old == ru) break;
-                ru = find_root(parent, old);
-            }
-        }
-        __syncthreads();
+constexpr int kSample = 2;
+
+__device__ __forceinline__ void cc_link(int* __restrict__ parent, int u, int v) {
+    int ru = find_root(parent, u);
+    int rv = find_root(parent, v);
+    while (ru != rv) {
+        if (ru < rv) { int x = ru; ru = rv; rv = x; }
+        // ru > rv: hang ru under rv if ru is still a root
+        int old = atomicCAS(parent + ru, ru, rv);
+        if (old == ru) return;
+        ru = find_root(parent, old);
+    }
+}
+
+// 1. link every vertex with its first kSample neighbours
+__global__ void k_cc_sample(const VRec* __restrict__ vtab, const int32_t* __restrict__ pool,
+                            int nV, int* __restrict__ parent) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
+         v += (long long)gridDim.x * blockDim.x) {
+        VRec r = vtab[v];
+        int k = r.deg < kSample ? r.deg : kSample;
+        for (int i = 0; i < k; i++) cc_link(parent, (int)v, pool[r.off + i]);
+    }
+}
+
+__global__ void k_cc_compress(int* __restrict__ parent, int nV) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
+         v += (long long)gridDim.x * blockDim.x)
+        parent[v] = find_root(parent, (int)v);
+}
+
+// 2. most frequent root among 256 evenly spaced vertices (one CTA of 256)
+__global__ void k_cc_giant(const int* __restrict__ parent, int nV, int* __restrict__ giant) {
+    __shared__ int s_r[256];
+    int t = threadIdx.x;
+    long long v = (long long)t * nV / 256;
+    s_r[t] = parent[v < nV ? v : nV - 1];
+    __syncthreads();
+    int mine = s_r[t], c = 0;
+    for (int i = 0; i < 256; i++) c += (s_r[i] == mine);
+    // pack (count, -root) so ties pick the smaller root
+    unsigned long long key = ((unsigned long long)c << 32) | (unsigned)(0x7FFFFFFF - mine);
+    __shared__ unsigned long long s_key;
+    if (t == 0) s_key = 0;
+    __syncthreads();
+    atomicMax(&s_key, key);
+    __syncthreads();
+    if (t == 0) *giant = 0x7FFFFFFF - (int)(s_key & 0xFFFFFFFFull);
+}
+
+// 3a. vertices outside the giant component with unread neighbours
+__global__ void k_cc_worklist(const VRec* __restrict__ vtab, const int* __restrict__ parent,
+                              int nV, const int* __restrict__ giant, int* __restrict__ list,
+                              int* __restrict__ nlist) {
+    const int gr = *giant;
+    for (long long v0 = blockIdx.x * (long long)blockDim.x; v0 < nV;
+         v0 += (long long)gridDim.x * blockDim.x) {
+        long long v = v0 + threadIdx.x;
+        bool take = v < nV && vtab[v].deg > kSample && parent[v] != gr;
+        int p = warp_append(nlist, take);
+        if (take) list[p] = (int)v;
+    }
+}
+
+// 3b. one warp per listed vertex: link with neighbours kSample..deg-1
+__global__ void k_cc_rest(const VRec* __restrict__ vtab, const int32_t* __restrict__ pool,
+                          const int* __restrict__ list, const int* __restrict__ nlist,
+                          int* __restrict__ parent) {
+    const int n = *nlist;
+    const int lane = threadIdx.x & 31;
+    long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long i = wid; i < n; i += nw) {
+        int v = list[i];
+        VRec r = vtab[v];
+        for (int k = kSample + lane; k < r.deg; k += 32) cc_link(parent, v, pool[r.off + k]);
     }
 }
 
@@ -141,12 +194,17 @@ extern "C" int hn_cc(hn_graph_t* g, int mode, int32_t* labels, int mem, int32_t*
         if (n_components) *n_components = 0;
         return HN_OK;
     }
-    DevBuf<int> parent((size_t)nV, s);
-    DevBuf<long long> prefix((size_t)nV + 1, s);
-    degree_prefix(g, nullptr, nV, prefix.get());
+    DevBuf<int> parent((size_t)nV, s), list((size_t)nV, s);
+    int* cnt = (int*)(g->d_scalar + 2);  // [0] giant root, [1] worklist size
+    HN_CUDA(cudaMemsetAsync(cnt, 0, 2 * sizeof(int), s));
     HN_LAUNCH(k_cc_init, grid_for(g, nV, kB), kB, 0, s, parent.get(), nV);
-    HN_LAUNCH(k_cc_hook, (long long)g->info.sms * 8, kB, 0, s, prefix.get(), nV, g->vtab, g->pool,
-              parent.get());
+    HN_LAUNCH(k_cc_sample, grid_for(g, nV, kB), kB, 0, s, g->vtab, g->pool, nV, parent.get());
+    HN_LAUNCH(k_cc_compress, grid_for(g, nV, kB), kB, 0, s, parent.get(), nV);
+    HN_LAUNCH(k_cc_giant, 1, 256, 0, s, parent.get(), nV, cnt);
+    HN_LAUNCH(k_cc_worklist, grid_for(g, nV, kB), kB, 0, s, g->vtab, parent.get(), nV, cnt,
+              list.get(), cnt + 1);
+    HN_LAUNCH(k_cc_rest, (long long)g->info.sms * 8, kB, 0, s, g->vtab, g->pool, list.get(),
+              cnt + 1, parent.get());
     HN_CUDA(cudaMemsetAsync(g->d_scalar, 0, 2 * sizeof(long long), s));
     HN_LAUNCH(k_cc_finish, grid_for(g, nV, kB), kB, 0, s, parent.get(), nV, (int*)g->d_scalar);
     int32_t* out = mem == HN_MEM_DEVICE ? labels : nullptr;

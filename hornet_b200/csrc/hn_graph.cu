@@ -150,12 +150,12 @@ using Tile = LbTile<kLbBlock, kLbItems>;
 __global__ void __launch_bounds__(kLbBlock)
 k_fill_pool(const long long* __restrict__ off, int nV, long long nE,
             const int32_t* __restrict__ adj, const VRec* __restrict__ vtab,
-            int32_t* __restrict__ pool) {
+            int32_t* __restrict__ pool, const long long* __restrict__ splits, long long split_tiles) {
     __shared__ Tile t;
     __shared__ long long dst_base[Tile::TILE + 1];
     long long ntiles = (nE + nV + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, off, (long long)nV, nE, tile);
+        int n = lb_tile_load(t, off, (long long)nV, nE, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kLbBlock) {
             long long v = t.seg0 + b;
             dst_base[b] = v < nV ? vtab[v].off - (b == 0 ? t.start0 : t.ends[b - 1]) : 0;
@@ -183,12 +183,13 @@ __global__ void k_degrees(const VRec* __restrict__ vtab, const int32_t* __restri
 __global__ void __launch_bounds__(kLbBlock)
 k_export(const long long* __restrict__ prefix, int nV, long long nE,
          const VRec* __restrict__ vtab, const int32_t* __restrict__ pool,
-         int32_t* __restrict__ src, int32_t* __restrict__ dst) {
+         int32_t* __restrict__ src, int32_t* __restrict__ dst,
+         const long long* __restrict__ splits, long long split_tiles) {
     __shared__ Tile t;
     __shared__ long long src_base[Tile::TILE + 1];
     long long ntiles = (nE + nV + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, prefix, (long long)nV, nE, tile);
+        int n = lb_tile_load(t, prefix, (long long)nV, nE, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kLbBlock) {
             long long v = t.seg0 + b;
             src_base[b] = v < nV ? vtab[v].off - (b == 0 ? t.start0 : t.ends[b - 1]) : 0;
@@ -311,11 +312,21 @@ void degree_prefix(hn_graph* g, const int32_t* verts, int32_t n, long long* pref
     count_launch();
 }
 
+void lb_splits(hn_graph* g, const long long* prefix, long long nseg, long long max_total,
+               int tile, DevBuf<long long>& splits) {
+    long long max_tiles = (max_total + nseg + tile - 1) / tile + 1;
+    splits.alloc((size_t)max_tiles + 1, g->stream);
+    HN_LAUNCH(lb_partition<long long>, grid_for(g, max_tiles + 1, 256), 256, 0, g->stream, prefix,
+              nseg, tile, max_tiles, splits.get());
+}
+
 void export_csr64(hn_graph* g, long long* off, int32_t* adj) {
     degree_prefix(g, nullptr, g->nV, off);
     long long ntiles = (g->nE + g->nV + Tile::TILE - 1) / Tile::TILE;
+    DevBuf<long long> splits;
+    lb_splits(g, off, g->nV, g->nE, Tile::TILE, splits);
     HN_LAUNCH(k_export, grid_for(g, ntiles, 1, 16), kLbBlock, 0, g->stream, off, g->nV,
-              g->nE, g->vtab, g->pool, (int32_t*)nullptr, adj);
+              g->nE, g->vtab, g->pool, (int32_t*)nullptr, adj, splits.get(), (long long)splits.n - 1);
 }
 
 void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
@@ -374,8 +385,10 @@ void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
         src_adj = sorted_adj.get();
     }
     long long ntiles = ((long long)nE + nV + Tile::TILE - 1) / Tile::TILE;
+    DevBuf<long long> splits;
+    lb_splits(g, d_off, nV, nE, Tile::TILE, splits);
     HN_LAUNCH(k_fill_pool, grid_for(g, ntiles, 1, 16), kLbBlock, 0, s, d_off, nV,
-              (long long)nE, src_adj, g->vtab, g->pool);
+              (long long)nE, src_adj, g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
     HN_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -635,8 +648,10 @@ int hn_graph_export_coo(hn_graph_t* g, int sorted, int32_t* src, int32_t* dst, i
         pd = dd.get();
     }
     long long ntiles = (g->nE + g->nV + Tile::TILE - 1) / Tile::TILE;
+    DevBuf<long long> splits;
+    lb_splits(g, prefix.get(), g->nV, g->nE, Tile::TILE, splits);
     HN_LAUNCH(k_export, grid_for(g, ntiles, 1, 16), kLbBlock, 0, s, prefix.get(), g->nV,
-              g->nE, g->vtab, g->pool, ps, pd);
+              g->nE, g->vtab, g->pool, ps, pd, splits.get(), (long long)splits.n - 1);
     if (mem == HN_MEM_HOST && g->nE) {
         HN_CUDA(cudaMemcpyAsync(src, ps, sizeof(int32_t) * g->nE, cudaMemcpyDeviceToHost, s));
         HN_CUDA(cudaMemcpyAsync(dst, pd, sizeof(int32_t) * g->nE, cudaMemcpyDeviceToHost, s));

@@ -180,6 +180,12 @@ void ensure_pool(hn_graph* g, unsigned long long slots);
 // Ensure free list c can hold `count` entries.
 void ensure_free_list(hn_graph* g, int c, long long count);
 
+// Tile splits for a merge-path LB kernel over `prefix` (nseg segments,
+// at most max_total items, tiles of `tile` merged elements); see
+// lb_partition.  Returns the device array (max_tiles + 1 entries).
+void lb_splits(hn_graph* g, const long long* prefix, long long nseg, long long max_total,
+               int tile, DevBuf<long long>& splits);
+
 // Scratch export of the graph as a contiguous CSR (device, int64 offsets).
 void export_csr64(hn_graph* g, long long* off /*nV+1*/, int32_t* adj /*nE*/);
 

@@ -116,5 +116,6 @@ __device__ __forceinline__ long long upper_bound_dev(const T* a, long long n, T 
 using hornet_b200::detail::LbTile;
 using hornet_b200::detail::lb_tile_load;
 using hornet_b200::detail::merge_path_items;
+using hornet_b200::detail::lb_partition;
 
 }  // namespace hn

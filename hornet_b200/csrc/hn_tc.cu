@@ -13,9 +13,8 @@
 //   pass 1  keep flag of every edge (needs deg(v): one 16-byte record read),
 //   scan    flag positions = the oriented CSR,
 //   pass 2  compact the kept neighbours (lists stay sorted).
-// The intersection then runs one thread per oriented edge (u,v): the
-// shorter of N+(u), N+(v) is walked and each element is found in the
-// longer one by a binary search whose lower bound only moves forward.
+// The intersection is vertex-centric with N+(u) in a shared-memory hash
+// table (see the comment above k_tc_warp).
 #include <cub/cub.cuh>
 
 #include "hn_graph.cuh"
@@ -34,14 +33,15 @@ __device__ __forceinline__ bool oriented_before(int du, int u, int dv, int v) {
 
 __global__ void __launch_bounds__(kB)
 k_orient_flags(const long long* __restrict__ prefix, int nV, const VRec* __restrict__ vtab,
-               const int32_t* __restrict__ pool, int32_t* __restrict__ flag) {
+               const int32_t* __restrict__ pool, int32_t* __restrict__ flag,
+               const long long* __restrict__ splits, long long split_tiles) {
     __shared__ Tile t;
     __shared__ long long s_base[Tile::TILE + 1];
     __shared__ int s_deg[Tile::TILE + 1];
     const long long total = prefix[nV];
     const long long ntiles = (total + nV + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, prefix, (long long)nV, total, tile);
+        int n = lb_tile_load(t, prefix, (long long)nV, total, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kB) {
             long long u = t.seg0 + b;
             if (u < nV) {
@@ -66,13 +66,14 @@ k_orient_flags(const long long* __restrict__ prefix, int nV, const VRec* __restr
 __global__ void __launch_bounds__(kB)
 k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restrict__ vtab,
               const int32_t* __restrict__ pool, const int32_t* __restrict__ pos,
-              int32_t* __restrict__ fwd, long long* __restrict__ offp) {
+              int32_t* __restrict__ fwd, long long* __restrict__ offp,
+              const long long* __restrict__ splits, long long split_tiles) {
     __shared__ Tile t;
     __shared__ long long s_base[Tile::TILE + 1];
     const long long total = prefix[nV];
     const long long ntiles = (total + nV + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, prefix, (long long)nV, total, tile);
+        int n = lb_tile_load(t, prefix, (long long)nV, total, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kB) {
             long long u = t.seg0 + b;
             if (u < nV) s_base[b] = vtab[u].off - t.seg_start(b);
@@ -91,103 +92,58 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
         offp[u] = pos[prefix[u]];
 }
 
-// |A ∩ B| for sorted A (shorter) and B; optional per-match callback.
-template <bool PER_VERTEX>
-__device__ __forceinline__ long long intersect_count(const int32_t* A, long long la,
-                                                     const int32_t* B, long long lb,
-                                                     unsigned long long* per_vertex) {
-    long long cnt = 0, lo = 0;
-    if (la == 0 || lb == 0) return 0;
-    if (A[la - 1] < B[0] || B[lb - 1] < A[0]) return 0;
-    for (long long i = 0; i < la && lo < lb; i++) {
-        int x = A[i];
-        // galloping-free binary search in B[lo, lb)
-        long long l = lo, h = lb;
-        while (l < h) {
-            long long m = (l + h) >> 1;
-            if (B[m] < x) l = m + 1; else h = m;
-        }
-        lo = l;
-        if (l < lb && B[l] == x) {
-            cnt++;
-            lo = l + 1;
-            if (PER_VERTEX) atomicAdd(per_vertex + x, 1ull);
-        }
-    }
-    return cnt;
-}
-
-template <bool PER_VERTEX>
-__global__ void __launch_bounds__(kB)
-k_tc_count(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ fwd,
-           unsigned long long* __restrict__ per_vertex, unsigned long long* __restrict__ total_out) {
-    __shared__ Tile t;
-    __shared__ unsigned long long s_sum[kB / 32];
-    const long long total = offp[nV];
-    const long long ntiles = (total + nV + Tile::TILE - 1) / Tile::TILE;
-    unsigned long long mine = 0;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, offp, (long long)nV, total, tile);
-        for (int i = threadIdx.x; i < n; i += kB) {
-            long long e = t.item0 + i;
-            int b = t.seg[i];
-            int u = (int)(t.seg0 + b);
-            long long ua = t.seg_start(b);
-            long long la = (b < t.nends ? t.ends[b] : offp[u + 1]) - ua;
-            int v = fwd[e];
-            long long vb = offp[v], lbn = offp[v + 1] - vb;
-            const int32_t* A = fwd + ua;
-            const int32_t* B = fwd + vb;
-            long long c = la <= lbn ? intersect_count<PER_VERTEX>(A, la, B, lbn, per_vertex)
-                                    : intersect_count<PER_VERTEX>(B, lbn, A, la, per_vertex);
-            if (PER_VERTEX && c) {
-                atomicAdd(per_vertex + u, (unsigned long long)c);
-                atomicAdd(per_vertex + v, (unsigned long long)c);
-            }
-            mine += (unsigned long long)c;
-        }
-        __syncthreads();
-    }
-    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
-    if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = mine;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        unsigned long long tsum = 0;
-        for (int w = 0; w < kB / 32; w++) tsum += s_sum[w];
-        if (tsum) atomicAdd(total_out, tsum);
-    }
-}
-
 // ---------------------------------------------------------------------------
-// Vertex-centric counting: N+(u) is staged in shared memory once, then all
-// (v, w) pairs with v in N+(u), w in N+(v) are flattened over the lanes
-// (warp prefix of d+(v) over 32 v's at a time) and each w is looked up in
-// the staged list by binary search.  N+(v) lists are read coalesced; N+(u)
-// is read once per u instead of once per edge.
-//   k_tc_warp: one warp per vertex, d+(u) <= kWarpCap, vertices handed out
-//              in chunks by an atomic counter (dynamic balance);
-//   k_tc_cta:  one CTA per vertex with d+(u) > kWarpCap; the list sits in
-//              dynamic shared memory when it fits, else it is searched in
-//              global memory.
+// Vertex-centric counting.  For each vertex u, N+(u) goes into an
+// open-addressing hash table in shared memory (multiplicative hash, linear
+// probing, load factor <= 1/2, so every probe sequence ends at an empty
+// slot).  Then all (v, w) pairs with v in N+(u), w in N+(v) are flattened
+// over the lanes (a warp prefix of d+(v) over 32 v's at a time): N+(v) is
+// read coalesced and each w costs O(1) shared-memory probes instead of a
+// binary search.  w outside [min N+(u), max N+(u)] is skipped.
+//   k_tc_warp: one warp per vertex with d+(u) <= kWarpCap (table of
+//              2*kWarpCap slots per warp); vertices are handed out in chunks
+//              by an atomic counter; larger vertices are pushed on a list;
+//   k_tc_cta:  one CTA per listed vertex, table in dynamic shared memory
+//              (up to kCtaCap entries), or binary search of the sorted list
+//              in global memory beyond that.
 // ---------------------------------------------------------------------------
 constexpr int kTcWarps = 8;
 constexpr int kWarpCap = 512;
+constexpr int kWarpTab = 2 * kWarpCap;
+constexpr int kCtaCap = 16384;
 constexpr int kChunk = 16;
 
-__device__ __forceinline__ int smem_lower_bound(const int32_t* a, int n, int x) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (a[mid] < x) lo = mid + 1; else hi = mid;
-    }
-    return lo;
+__device__ __forceinline__ unsigned tc_hash(int w, int bits) {
+    return ((unsigned)w * 2654435761u) >> (32 - bits);
 }
 
-// One warp: all (v, w) pairs of u against the sorted list L (length du).
+__device__ __forceinline__ void tab_insert(int* tab, int bits, int w) {
+    unsigned mask = (1u << bits) - 1;
+    unsigned h = tc_hash(w, bits);
+    while (true) {
+        int old = atomicCAS(tab + h, -1, w);
+        if (old == -1 || old == w) return;
+        h = (h + 1) & mask;
+    }
+}
+
+__device__ __forceinline__ bool tab_find(const int* tab, int bits, int w) {
+    unsigned mask = (1u << bits) - 1;
+    unsigned h = tc_hash(w, bits);
+    while (true) {
+        int x = tab[h];
+        if (x == w) return true;
+        if (x == -1) return false;
+        h = (h + 1) & mask;
+    }
+}
+
+// One warp: all (v, w) pairs of u.  Membership in N+(u) by hash table (tab
+// != nullptr) or by binary search of the sorted global list L.
 template <bool PER_VERTEX>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
-    int u, const int32_t* __restrict__ L, int du, int v_begin, int v_step,
-    const long long* __restrict__ offp, const int32_t* __restrict__ fwd,
+    int u, const int32_t* __restrict__ L, int du, const int* tab, int bits, int v_begin,
+    int v_step, const long long* __restrict__ offp, const int32_t* __restrict__ fwd,
     long long* s_pref /*33*/, long long* s_vb /*32*/, int* s_v /*32*/,
     unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
@@ -214,16 +170,25 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
         __syncwarp();
         const long long T = s_pref[32];
         for (long long k = lane; k < T; k += 32) {
-            // slot of pair k: last s with s_pref[s] <= k
-            int a = 0, b = 32;
+            int a = 0, b = 32;   // slot of pair k: last s with s_pref[s] <= k
             while (b - a > 1) {
                 int mid = (a + b) >> 1;
                 if (s_pref[mid] <= k) a = mid; else b = mid;
             }
             int w = fwd[s_vb[a] + (k - s_pref[a])];
             if (w < lo_w || w > hi_w) continue;
-            int p = smem_lower_bound(L, du, w);
-            if (p < du && L[p] == w) {
+            bool hit;
+            if (tab) {
+                hit = tab_find(tab, bits, w);
+            } else {
+                int lo = 0, hi = du;
+                while (lo < hi) {
+                    int mid = (lo + hi) >> 1;
+                    if (L[mid] < w) lo = mid + 1; else hi = mid;
+                }
+                hit = lo < du && L[lo] == w;
+            }
+            if (hit) {
                 cnt++;
                 if (PER_VERTEX) {
                     atomicAdd(per_vertex + w, 1ull);
@@ -241,27 +206,37 @@ template <bool PER_VERTEX>
 __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_warp(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ fwd,
           unsigned long long* __restrict__ per_vertex, unsigned long long* __restrict__ total_out,
-          int* __restrict__ next_u) {
-    __shared__ int32_t s_list[kTcWarps][kWarpCap];
+          int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
+          int32_t* __restrict__ big) {
+    __shared__ int s_tab[kTcWarps][kWarpTab];
     __shared__ long long s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
     __shared__ unsigned long long s_sum[kTcWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int* tab = s_tab[warp];
     unsigned long long mine = 0;
     while (true) {
         int u0 = 0;
-        if (lane == 0) u0 = atomicAdd(next_u, kChunk);
+        if (lane == 0) u0 = atomicAdd(counters, kChunk);
         u0 = __shfl_sync(0xFFFFFFFFu, u0, 0);
         if (u0 >= nV) break;
         int u1 = u0 + kChunk < nV ? u0 + kChunk : nV;
         for (int u = u0; u < u1; u++) {
             long long ub = offp[u];
             int du = (int)(offp[u + 1] - ub);
-            if (du == 0 || du > kWarpCap) continue;
-            for (int i = lane; i < du; i += 32) s_list[warp][i] = fwd[ub + i];
+            if (du == 0) continue;
+            if (du > kWarpCap) {
+                if (lane == 0) big[atomicAdd(counters + 1, 1)] = u;
+                continue;
+            }
+            int bits = 32 - __clz(2 * du - 1);   // table of 2^bits >= 2*du slots
+            if (bits < 5) bits = 5;
+            for (int i = lane; i < (1 << bits); i += 32) tab[i] = -1;
             __syncwarp();
-            mine += tc_vertex_warp<PER_VERTEX>(u, s_list[warp], du, 0, 1, offp, fwd,
+            for (int i = lane; i < du; i += 32) tab_insert(tab, bits, fwd[ub + i]);
+            __syncwarp();
+            mine += tc_vertex_warp<PER_VERTEX>(u, fwd + ub, du, tab, bits, 0, 1, offp, fwd,
                                                s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
             __syncwarp();
         }
@@ -276,31 +251,36 @@ k_tc_warp(const long long* __restrict__ offp, int nV, const int32_t* __restrict_
     }
 }
 
-// Vertices with d+(u) > kWarpCap (few): one CTA each.
+// Listed vertices (d+(u) > kWarpCap): one CTA each.
 template <bool PER_VERTEX>
 __global__ void __launch_bounds__(kTcWarps * 32)
-k_tc_cta(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ fwd,
+k_tc_cta(const long long* __restrict__ offp, const int32_t* __restrict__ fwd,
          unsigned long long* __restrict__ per_vertex, unsigned long long* __restrict__ total_out,
-         int smem_cap) {
-    extern __shared__ int32_t s_dyn[];
+         const int* __restrict__ counters, const int32_t* __restrict__ big) {
+    extern __shared__ int s_dyn[];
     __shared__ long long s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
     __shared__ unsigned long long s_sum[kTcWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int nbig = counters[1];
     unsigned long long mine = 0;
-    for (long long u = blockIdx.x; u < nV; u += gridDim.x) {
+    for (int i = blockIdx.x; i < nbig; i += gridDim.x) {
+        int u = big[i];
         long long ub = offp[u];
         int du = (int)(offp[u + 1] - ub);
-        if (du <= kWarpCap) continue;
-        const int32_t* L = fwd + ub;
-        if (du <= smem_cap) {
-            for (int i = threadIdx.x; i < du; i += blockDim.x) s_dyn[i] = fwd[ub + i];
-            L = s_dyn;
+        const int* tab = nullptr;
+        int bits = 0;
+        if (du <= kCtaCap) {
+            bits = 32 - __clz(2 * du - 1);
+            for (int j = threadIdx.x; j < (1 << bits); j += blockDim.x) s_dyn[j] = -1;
+            __syncthreads();
+            for (int j = threadIdx.x; j < du; j += blockDim.x) tab_insert(s_dyn, bits, fwd[ub + j]);
+            tab = s_dyn;
         }
         __syncthreads();
-        mine += tc_vertex_warp<PER_VERTEX>((int)u, L, du, warp, kTcWarps, offp, fwd, s_pref[warp],
-                                           s_vb[warp], s_v[warp], per_vertex);
+        mine += tc_vertex_warp<PER_VERTEX>(u, fwd + ub, du, tab, bits, warp, kTcWarps, offp, fwd,
+                                           s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
         __syncthreads();
     }
     for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
@@ -323,7 +303,10 @@ void build_oriented(hn_graph* g, Oriented& o) {
     degree_prefix(g, nullptr, nV, o.prefix.get());
     DevBuf<int32_t> pos((size_t)m + 1, s);
     const long long grid = (long long)g->info.sms * 8;
-    HN_LAUNCH(k_orient_flags, grid, kB, 0, s, o.prefix.get(), nV, g->vtab, g->pool, pos.get());
+    DevBuf<long long> splits;
+    lb_splits(g, o.prefix.get(), nV, m, Tile::TILE, splits);
+    HN_LAUNCH(k_orient_flags, grid, kB, 0, s, o.prefix.get(), nV, g->vtab, g->pool, pos.get(),
+              splits.get(), (long long)splits.n - 1);
     {
         size_t tb = 0;
         HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, pos.get(), pos.get(), (int)(m + 1), s));
@@ -332,21 +315,20 @@ void build_oriented(hn_graph* g, Oriented& o) {
         count_launch();
     }
     o.offp.alloc((size_t)nV + 1, s);
-    o.fwd.alloc((size_t)(m / 2 + 4), s);
+    o.fwd.alloc((size_t)(m + 4), s);
     HN_LAUNCH(k_orient_fill, grid, kB, 0, s, o.prefix.get(), nV, g->vtab, g->pool, pos.get(),
-              o.fwd.get(), o.offp.get());
+              o.fwd.get(), o.offp.get(), splits.get(), (long long)splits.n - 1);
 }
 
 unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_per_vertex) {
     cudaStream_t s = g->stream;
     unsigned long long* d_total = (unsigned long long*)g->d_scalar;
     HN_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
-    int* next_u = (int*)(g->d_scalar + 1);
-    HN_CUDA(cudaMemsetAsync(next_u, 0, sizeof(int), s));
+    int* counters = (int*)(g->d_scalar + 1);  // next vertex, big-list size
+    HN_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(int), s));
+    DevBuf<int32_t> big((size_t)g->nV + 1, s);
     const long long gw = (long long)g->info.sms * 8;
-    // dynamic shared memory for the CTA path: up to 160 KB of list
-    const int smem_cap = 40 * 1024;
-    const size_t dyn = (size_t)smem_cap * sizeof(int32_t);
+    const size_t dyn = (size_t)2 * kCtaCap * sizeof(int);   // hash table of the CTA path
     static bool attr_set = false;
     if (!attr_set) {
         HN_CUDA(cudaFuncSetAttribute(k_tc_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -355,18 +337,18 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
                                      (int)dyn));
         attr_set = true;
     }
-    const long long gc = (long long)g->info.sms * 2;
+    const long long gc = (long long)g->info.sms;
     if (d_per_vertex) {
         HN_CUDA(cudaMemsetAsync(d_per_vertex, 0, sizeof(unsigned long long) * g->nV, s));
         HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, o.offp.get(), g->nV, o.fwd.get(),
-                  d_per_vertex, d_total, next_u);
-        HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, o.offp.get(), g->nV, o.fwd.get(),
-                  d_per_vertex, d_total, smem_cap);
+                  d_per_vertex, d_total, counters, big.get());
+        HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, o.offp.get(), o.fwd.get(),
+                  d_per_vertex, d_total, counters, big.get());
     } else {
         HN_LAUNCH(k_tc_warp<false>, gw, kTcWarps * 32, 0, s, o.offp.get(), g->nV, o.fwd.get(),
-                  (unsigned long long*)nullptr, d_total, next_u);
-        HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, o.offp.get(), g->nV, o.fwd.get(),
-                  (unsigned long long*)nullptr, d_total, smem_cap);
+                  (unsigned long long*)nullptr, d_total, counters, big.get());
+        HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, o.offp.get(), o.fwd.get(),
+                  (unsigned long long*)nullptr, d_total, counters, big.get());
     }
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];

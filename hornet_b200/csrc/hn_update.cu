@@ -224,7 +224,8 @@ __global__ void __launch_bounds__(kB)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
-              const VRec* __restrict__ vtab, int32_t* __restrict__ pool) {
+              const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
+              const long long* __restrict__ splits, long long split_tiles) {
     __shared__ Tile t;
     __shared__ long long s_old[Tile::TILE + 1];
     __shared__ long long s_new[Tile::TILE + 1];
@@ -233,7 +234,7 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
     const long long total = prefix[nseg];
     long long ntiles = (total + nseg + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int n = lb_tile_load(t, prefix, nseg, total, tile);
+        int n = lb_tile_load(t, prefix, nseg, total, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kB) {
             long long s = t.seg0 + b;
             if (s < nseg) {
@@ -412,16 +413,18 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     }
     // tiles are read from the device prefix; the grid is persistent
     const long long grid_sc = (long long)g->info.sms * 4;
+    DevBuf<long long> splits;
+    lb_splits(g, seg_work.get(), nseg, g->nE, Tile::TILE, splits);
     if (insert) {
         HN_LAUNCH(k_scatter_old<true>, grid_sc, kB, 0, s, seg_work.get(), nseg,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  g->vtab, g->pool);
+                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
         HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), totals,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool);
     } else {
         HN_LAUNCH(k_scatter_old<false>, grid_sc, kB, 0, s, seg_work.get(),
                   nseg, seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  g->vtab, g->pool);
+                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
     }
     // 8. commit
     HN_LAUNCH(k_commit, grid_for(g, nseg, kB), kB, 0, s, seg_u.get(), seg_kstart.get(),

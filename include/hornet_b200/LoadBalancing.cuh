@@ -41,13 +41,14 @@ __global__ void degreesOf(hornet::HornetDevice hd, const int* __restrict__ input
 template <int BLOCK, int ITEMS, typename Operator>
 __global__ void __launch_bounds__(BLOCK)
 binarySearchLB(hornet::HornetDevice hd, const int* __restrict__ input, long long n,
-               const long long* __restrict__ prefix, Operator op) {
+               const long long* __restrict__ prefix, const long long* __restrict__ splits,
+               long long max_tiles, Operator op) {
     using Tile = hornet_b200::detail::LbTile<BLOCK, ITEMS>;
     __shared__ Tile t;
     const long long total = prefix[n];
     const long long ntiles = (total + n + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        int cnt = hornet_b200::detail::lb_tile_load(t, prefix, n, total, tile);
+        int cnt = hornet_b200::detail::lb_tile_load(t, prefix, n, total, tile, splits, max_tiles);
         for (int i = threadIdx.x; i < cnt; i += BLOCK) {
             int b = t.seg[i];
             long long s = t.seg0 + b;
@@ -96,12 +97,20 @@ public:
 
     // Core: every edge of the n vertices in d_input (all vertices when
     // d_input == nullptr), on `stream`.  Asynchronous.
+    // The tile partition is precomputed for a work size of max_total (the
+    // edge count by default, which bounds any list without repeats); tiles
+    // past that bound search for their own split, so any list is correct.
     template <typename Operator>
     static void run(const hornet::HornetDevice& hd, const int* d_input, long long n,
-                    const Operator& op, cudaStream_t stream) {
+                    const Operator& op, cudaStream_t stream, long long max_total = -1) {
         if (n <= 0) return;
+        const int tile = BLOCK_SIZE * ITEMS;
+        if (max_total < 0) max_total = hd.nE();
+        const long long max_tiles = (max_total + n + tile - 1) / tile + 1;
         long long* prefix = nullptr;
+        long long* splits = nullptr;
         cudaMallocAsync((void**)&prefix, sizeof(long long) * (size_t)(n + 1), stream);
+        cudaMallocAsync((void**)&splits, sizeof(long long) * (size_t)(max_tiles + 1), stream);
         const int sms = kernels::num_sms();
         long long g = (n + 256) / 256;
         if (g > sms * 8) g = sms * 8;
@@ -111,9 +120,14 @@ public:
         void* tmp = nullptr;
         cudaMallocAsync(&tmp, tb, stream);
         cub::DeviceScan::ExclusiveSum(tmp, tb, prefix, prefix, n + 1, stream);
+        long long gp = (max_tiles + 256) / 256;
+        if (gp > sms * 8) gp = sms * 8;
+        hornet_b200::detail::lb_partition<long long><<<(unsigned)gp, 256, 0, stream>>>(
+            prefix, n, tile, max_tiles, splits);
         kernels::binarySearchLB<BLOCK_SIZE, ITEMS><<<(unsigned)(sms * 8), BLOCK_SIZE, 0, stream>>>(
-            hd, d_input, n, prefix, op);
+            hd, d_input, n, prefix, splits, max_tiles, op);
         cudaFreeAsync(tmp, stream);
+        cudaFreeAsync(splits, stream);
         cudaFreeAsync(prefix, stream);
     }
 

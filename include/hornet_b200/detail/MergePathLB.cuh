@@ -58,17 +58,40 @@ struct LbTile {
 
 // Fill `t` for tile `tile_id`.  Must be called by all BLOCK threads.
 // Returns the number of items in the tile.
+// Split of every tile boundary (one thread each; all searches run in
+// parallel with independent loads): splits[t] = items among the first
+// t * tile merged elements, t = 0 .. ntiles.  `total` is read from
+// prefix[nseg] so the work size may be known only on the device; at most
+// max_tiles tiles are described.
+template <typename P>
+__global__ void lb_partition(const P* __restrict__ prefix, long long nseg, int tile,
+                             long long max_tiles, long long* __restrict__ splits) {
+    const long long total = (long long)prefix[nseg];
+    long long ntiles = (total + nseg + tile - 1) / tile;
+    if (ntiles > max_tiles) ntiles = max_tiles;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t <= ntiles;
+         t += (long long)gridDim.x * blockDim.x) {
+        long long d = t * tile;
+        if (d > total + nseg) d = total + nseg;
+        splits[t] = merge_path_items(prefix + 1, nseg, total, d);
+    }
+}
+
 template <int BLOCK, int ITEMS, typename P>
 __device__ int lb_tile_load(LbTile<BLOCK, ITEMS>& t, const P* prefix, long long nseg,
-                            long long total, long long tile_id) {
+                            long long total, long long tile_id,
+                            const long long* splits = nullptr, long long split_tiles = 0) {
     constexpr int TILE = BLOCK * ITEMS;
     const P* ends = prefix + 1;
     long long d0 = tile_id * TILE;
     long long d1 = d0 + TILE;
     if (d1 > total + nseg) d1 = total + nseg;
     if (threadIdx.x == 0) {
-        long long a0 = merge_path_items(ends, nseg, total, d0);
-        long long a1 = merge_path_items(ends, nseg, total, d1);
+        // precomputed splits cover tiles [0, split_tiles); beyond them (a
+        // work size above the caller's bound) the tile searches for itself
+        const bool pre = splits && tile_id < split_tiles;
+        long long a0 = pre ? splits[tile_id] : merge_path_items(ends, nseg, total, d0);
+        long long a1 = pre ? splits[tile_id + 1] : merge_path_items(ends, nseg, total, d1);
         t.item0 = a0;
         t.seg0 = d0 - a0;
         t.nitems = (int)(a1 - a0);
