@@ -217,25 +217,30 @@ def event_time(stream, fn):
     return a.elapsed_time(b) / 1e3
 
 
-def roofline_entry(H, kernel_prefix, algo_bytes_fn, peak, peak_kind, report, workload):
-    """Dominant kernel roofline from the event-profiled pass."""
-    cand = {k: v for k, v in report.items() if k.startswith(kernel_prefix)}
+def roofline_entry(H, prefixes, algo_bytes_fn, peak, peak_kind, report, workload):
+    """Roofline of a path from the event-profiled pass: achieved = the
+    path's algorithmic bytes / the summed device time of its kernels
+    (`prefixes`), per launch of the dominant kernel; the dominant kernel and
+    its share of the path time are named."""
+    if isinstance(prefixes, str):
+        prefixes = [prefixes]
+    cand = {k: v for k, v in report.items() if any(k.startswith(p) for p in prefixes)}
     if not cand:
         return None
     name, rec = max(cand.items(), key=lambda kv: kv[1]["ms"])
+    path_s = sum(v["ms"] for v in cand.values()) / 1e3
     launches = rec["launches"]
-    sec = rec["ms"] / 1e3
     algo_total = algo_bytes_fn()
-    per_launch_bytes = algo_total / launches
-    per_launch_s = sec / launches
-    achieved = per_launch_bytes / per_launch_s / 1e9
+    achieved = algo_total / path_s / 1e9
     tr = load_traffic(name)
     return {"kernel": name, "bound": "hbm", "achieved": round(achieved, 1), "peak": peak,
             "unit": "GB/s", "frac": round(achieved / peak, 4),
             "traffic": tr[1] if tr else None,
-            "algorithmic_bytes_per_launch": round(per_launch_bytes),
-            "avg_launch_us": round(per_launch_s * 1e6, 2), "launches": launches,
-            "peak_kind": peak_kind, "share_of_path": None, "workload": workload}
+            "algorithmic_bytes_per_launch": round(algo_total / launches),
+            "avg_launch_us": round(rec["ms"] * 1e3 / launches, 2), "launches": launches,
+            "path_kernels": sorted(cand), "path_us": round(path_s * 1e6, 2),
+            "share_of_path": round(rec["ms"] / 1e3 / path_s, 3) if path_s else None,
+            "peak_kind": peak_kind, "workload": workload}
 
 
 def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_kind, barrier,
@@ -300,9 +305,6 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     H.profile_enable(False)
     roof = roofline_entry(H, "k_bfs3_expand", lambda: 8 * prof_edges + 20 * prof_vis, peak,
                           peak_kind, rep, f"R-MAT scale {scale} BFS, {min(K, 16)} sources")
-    tot_ms = sum(v["ms"] for v in rep.values())
-    if roof:
-        roof["share_of_path"] = round(rep[roof["kernel"]]["ms"] / tot_ms, 3) if tot_ms else None
 
     also = {}
     if not args.no_extras and rank == 0:
@@ -352,7 +354,7 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale):
     keep = (d[src] < d[adj]) | ((d[src] == d[adj]) & (src < adj))
     dplus = np.bincount(src[keep], minlength=nV).astype(np.int64)
     tc_bytes = 8 * m_plus + 4 * int((dplus[src[keep]] + dplus[adj[keep]]).sum())
-    troof = roofline_entry(H, "k_tc_count", lambda: tc_bytes, peak, peak_kind, rep,
+    troof = roofline_entry(H, ["k_orient", "k_tc_", "k_degrees"], lambda: tc_bytes, peak, peak_kind, rep,
                            f"R-MAT scale {scale} TC")
     also["tc"] = {"metric": "TC edges/s", "value": round(m_plus / t, 1), "unit": "edges/s",
                   "triangles": int(tc.countTriangles()), "ms": round(t * 1e3, 3),
@@ -366,7 +368,7 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale):
     cc.run(out=lab)
     rep = H.profile_report()
     H.profile_enable(False)
-    croof = roofline_entry(H, "k_cc_hook", lambda: 4 * nE + 8 * (nV + 1) + 8 * nV, peak,
+    croof = roofline_entry(H, ["k_cc_"], lambda: 4 * nE + 8 * (nV + 1) + 8 * nV, peak,
                            peak_kind, rep, f"R-MAT scale {scale} CC")
     also["cc"] = {"metric": "CC edges/s", "value": round(nE / t, 1), "unit": "edges/s",
                   "components": cc.n_components, "ms": round(t * 1e3, 3), "roofline": croof}
