@@ -110,6 +110,7 @@ _SIGNATURES = {
     "hn_gen_rmat_device": [_I32, _I32, _I64, _D, _D, _D, _U64, _P, _P, _INT],
     "hn_coo_to_csr_device": [_I32, _I64, _P, _P, _INT, _P, _P, _P],
     "hn_free_device": [_P],
+    "hn_cc_csr_noalloc": [_I32, _P, _P, _P, _P, _P],
 }
 _RESTYPES = {"hn_last_error_string": ctypes.c_char_p, "hn_kernel_launches": _I64}
 

@@ -205,6 +205,23 @@ int hn_for_all_edges_count(hn_graph_t* g, const int32_t* vertices, int32_t n,
  * out[v] = degree(v) (Operator++.i.cuh:524-540). out: int32[nV] device. */
 int hn_for_all_vertices_degree(hn_graph_t* g, int32_t* out);
 
+/* ---- connected components without device allocation ---------------------
+ * No counterpart in the reference.  For callers that cannot allocate device
+ * memory (a host framework that owns all device memory, a service whose
+ * memory budget is fixed up front, a loop that cannot afford the implicit
+ * synchronisation of cudaMalloc/cudaFree): the same labels as
+ * hn_cc(HN_CC_MIN_ID) computed over a caller-owned device CSR
+ * (off[nV+1], adj[off[nV]]) into a caller-owned device array labels[nV],
+ * with no cudaMalloc/cudaFree and no allocating library call.  Its only
+ * working memory is a 16 MiB static device array inside the library, so
+ * nV is limited to 4,194,304 (HN_ERR_CAPACITY above that).  The first call
+ * on a device resolves that array's address: make it before any stream
+ * capture.  All calls share the array; calls that overlap on the GPU race.
+ * `stream` is a cudaStream_t (NULL = legacy default stream); the call
+ * returns when the labels are ready.  *n_components (may be NULL) is host. */
+int hn_cc_csr_noalloc(int32_t nV, const int32_t* off, const int32_t* adj,
+                      int32_t* labels, int32_t* n_components, void* stream);
+
 /* ---- synthetic inputs (not part of the reference API) --------------------
  * R-MAT edge pairs (a,b,c; d = 1-a-b-c) from a counter-based generator:
  * pair i depends only on (seed, i), so the host and device versions give
