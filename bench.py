@@ -268,10 +268,13 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     visited = [0]
 
     def timed():
+        # NVTX range "hn_bfs" lets a profiler select exactly these launches
+        torch.cuda.nvtx.range_push("hn_bfs")
         for i in range(K):
             e, v = run_bfs(W + i)
             scanned[0] += e
             visited[0] += v
+        torch.cuda.nvtx.range_pop()
 
     t = event_time(stream, timed)
     barrier()
@@ -442,8 +445,10 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     edges = [0]
 
     def timed():
+        torch.cuda.nvtx.range_push("hn_update")
         for i in range(K):
             edges[0] += step(start + i)
+        torch.cuda.nvtx.range_pop()
 
     t = event_time(stream, timed)
     launches = H.kernel_launches() - l0

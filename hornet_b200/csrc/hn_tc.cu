@@ -93,25 +93,32 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
 }
 
 // ---------------------------------------------------------------------------
-// Vertex-centric counting.  For each vertex u, N+(u) goes into an
-// open-addressing hash table in shared memory (multiplicative hash, linear
-// probing, load factor <= 1/2, so every probe sequence ends at an empty
-// slot).  Then all (v, w) pairs with v in N+(u), w in N+(v) are flattened
-// over the lanes (a warp prefix of d+(v) over 32 v's at a time): N+(v) is
-// read coalesced and each w costs O(1) shared-memory probes instead of a
-// binary search.  w outside [min N+(u), max N+(u)] is skipped.
-//   k_tc_warp: one warp per vertex with d+(u) <= kWarpCap (table of
-//              2*kWarpCap slots per warp); vertices are handed out in chunks
-//              by an atomic counter; larger vertices are pushed on a list;
+// Vertex-centric counting, each edge probed from its smaller side.
+// For each vertex u, N+(u) goes into an open-addressing hash table in shared
+// memory (multiplicative hash, linear probing, load factor <= 1/2, so every
+// probe sequence ends at an empty slot).  Every oriented edge (u,v) needs
+// |N+(u) ∩ N+(v)|; it is counted by whichever endpoint has the LONGER list,
+// walking the shorter list against that endpoint's table:
+//   out-phase: v in N+(u) with d+(v) <= d+(u): walk N+(v), probe table(u);
+//   in-phase:  x in N-(u) (undirected neighbours that precede u in the
+//              (degree, id) order) with d+(x) < d+(u): walk N+(x), probe
+//              table(u).
+// So each edge costs min(d+(u), d+(v)) probes.  The (candidate, element)
+// pairs of 32 candidates at a time are flattened over the lanes (warp
+// prefix of the list lengths), each lane keeps 4 element loads in flight,
+// and elements outside [min N+(u), max N+(u)] are skipped before probing.
+//   k_tc_warp: one warp per vertex with d+(u) <= kWarpCap; vertices handed
+//              out in chunks by an atomic counter; larger ones are listed;
 //   k_tc_cta:  one CTA per listed vertex, table in dynamic shared memory
-//              (up to kCtaCap entries), or binary search of the sorted list
-//              in global memory beyond that.
+//              (up to kCtaCap entries), binary search of the sorted list in
+//              global memory beyond that.
 // ---------------------------------------------------------------------------
 constexpr int kTcWarps = 8;
 constexpr int kWarpCap = 512;
 constexpr int kWarpTab = 2 * kWarpCap;
 constexpr int kCtaCap = 16384;
 constexpr int kChunk = 16;
+constexpr int kUnroll = 4;
 
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
@@ -138,74 +145,109 @@ __device__ __forceinline__ bool tab_find(const int* tab, int bits, int w) {
     }
 }
 
-// One warp: all (v, w) pairs of u.  Membership in N+(u) by hash table (tab
-// != nullptr) or by binary search of the sorted global list L.
+struct TcView {
+    const long long* offp;   // oriented offsets
+    const int32_t* fwd;      // oriented lists
+    const VRec* vtab;        // undirected graph (for in-neighbours)
+    const int32_t* pool;
+};
+
+// One warp: the probes u is responsible for.  Membership in N+(u) by hash
+// table (tab != nullptr) or binary search of the sorted global list L.
 template <bool PER_VERTEX>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
-    int u, const int32_t* __restrict__ L, int du, const int* tab, int bits, int v_begin,
-    int v_step, const long long* __restrict__ offp, const int32_t* __restrict__ fwd,
-    long long* s_pref /*33*/, long long* s_vb /*32*/, int* s_v /*32*/,
-    unsigned long long* __restrict__ per_vertex) {
+    int u, const int32_t* __restrict__ L, int du, const int* tab, int bits, int cand_begin,
+    int cand_step, const TcView& g, long long* s_pref /*33*/, long long* s_vb /*32*/,
+    int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
     const int lo_w = L[0], hi_w = L[du - 1];
+    const VRec ru = g.vtab[u];
     unsigned long long cnt = 0;
-    for (int c0 = v_begin * 32; c0 < du; c0 += v_step * 32) {
-        int idx = c0 + lane;
-        long long dv = 0, vb = 0;
-        int v = 0;
-        if (idx < du) {
-            v = L[idx];
-            vb = offp[v];
-            dv = offp[v + 1] - vb;
-        }
-        long long incl = dv;
-        for (int o = 1; o < 32; o <<= 1) {
-            long long x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += x;
-        }
-        s_pref[lane + 1] = incl;
-        if (lane == 0) s_pref[0] = 0;
-        s_vb[lane] = vb;
-        s_v[lane] = v;
-        __syncwarp();
-        const long long T = s_pref[32];
-        for (long long k = lane; k < T; k += 32) {
-            int a = 0, b = 32;   // slot of pair k: last s with s_pref[s] <= k
-            while (b - a > 1) {
-                int mid = (a + b) >> 1;
-                if (s_pref[mid] <= k) a = mid; else b = mid;
-            }
-            int w = fwd[s_vb[a] + (k - s_pref[a])];
-            if (w < lo_w || w > hi_w) continue;
-            bool hit;
-            if (tab) {
-                hit = tab_find(tab, bits, w);
-            } else {
-                int lo = 0, hi = du;
-                while (lo < hi) {
-                    int mid = (lo + hi) >> 1;
-                    if (L[mid] < w) lo = mid + 1; else hi = mid;
+#pragma unroll 1
+    for (int phase = 0; phase < 2; phase++) {
+        const int32_t* cand = phase == 0 ? L : g.pool + ru.off;
+        const int ncand = phase == 0 ? du : ru.deg;
+        for (int c0 = cand_begin * 32; c0 < ncand; c0 += cand_step * 32) {
+            int idx = c0 + lane;
+            long long dx = 0, xb = 0;
+            int x = 0;
+            if (idx < ncand) {
+                x = cand[idx];
+                bool take = true;
+                if (phase == 1) {
+                    VRec rx = g.vtab[x];
+                    take = rx.deg < ru.deg || (rx.deg == ru.deg && x < u);   // x precedes u
                 }
-                hit = lo < du && L[lo] == w;
-            }
-            if (hit) {
-                cnt++;
-                if (PER_VERTEX) {
-                    atomicAdd(per_vertex + w, 1ull);
-                    atomicAdd(per_vertex + u, 1ull);
-                    atomicAdd(per_vertex + s_v[a], 1ull);
+                if (take) {
+                    xb = g.offp[x];
+                    dx = g.offp[x + 1] - xb;
+                    if (phase == 0 ? dx > du : dx >= du) dx = 0;   // other side walks
                 }
             }
+            long long incl = dx;
+            for (int o = 1; o < 32; o <<= 1) {
+                long long y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            s_pref[lane + 1] = incl;
+            if (lane == 0) s_pref[0] = 0;
+            s_vb[lane] = xb;
+            s_v[lane] = x;
+            __syncwarp();
+            const long long T = s_pref[32];
+            for (long long k0 = lane; k0 < T; k0 += 32 * kUnroll) {
+                int wv[kUnroll];
+                int sl[kUnroll];
+#pragma unroll
+                for (int j = 0; j < kUnroll; j++) {
+                    long long k = k0 + 32 * j;
+                    wv[j] = -1;
+                    sl[j] = 0;
+                    if (k < T) {
+                        int a = 0, b = 32;   // slot of pair k: last s with s_pref[s] <= k
+                        while (b - a > 1) {
+                            int mid = (a + b) >> 1;
+                            if (s_pref[mid] <= k) a = mid; else b = mid;
+                        }
+                        sl[j] = a;
+                        wv[j] = g.fwd[s_vb[a] + (k - s_pref[a])];
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kUnroll; j++) {
+                    int w = wv[j];
+                    if (w < lo_w || w > hi_w) continue;   // also drops the -1 fillers
+                    bool hit;
+                    if (tab) {
+                        hit = tab_find(tab, bits, w);
+                    } else {
+                        int lo = 0, hi = du;
+                        while (lo < hi) {
+                            int mid = (lo + hi) >> 1;
+                            if (L[mid] < w) lo = mid + 1; else hi = mid;
+                        }
+                        hit = lo < du && L[lo] == w;
+                    }
+                    if (hit) {
+                        cnt++;
+                        if (PER_VERTEX) {
+                            atomicAdd(per_vertex + w, 1ull);
+                            atomicAdd(per_vertex + u, 1ull);
+                            atomicAdd(per_vertex + s_v[sl[j]], 1ull);
+                        }
+                    }
+                }
+            }
+            __syncwarp();
         }
-        __syncwarp();
     }
     return cnt;
 }
 
 template <bool PER_VERTEX>
 __global__ void __launch_bounds__(kTcWarps * 32)
-k_tc_warp(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ fwd,
-          unsigned long long* __restrict__ per_vertex, unsigned long long* __restrict__ total_out,
+k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
+          unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
           int32_t* __restrict__ big) {
     __shared__ int s_tab[kTcWarps][kWarpTab];
@@ -223,8 +265,8 @@ k_tc_warp(const long long* __restrict__ offp, int nV, const int32_t* __restrict_
         if (u0 >= nV) break;
         int u1 = u0 + kChunk < nV ? u0 + kChunk : nV;
         for (int u = u0; u < u1; u++) {
-            long long ub = offp[u];
-            int du = (int)(offp[u + 1] - ub);
+            long long ub = g.offp[u];
+            int du = (int)(g.offp[u + 1] - ub);
             if (du == 0) continue;
             if (du > kWarpCap) {
                 if (lane == 0) big[atomicAdd(counters + 1, 1)] = u;
@@ -234,10 +276,10 @@ k_tc_warp(const long long* __restrict__ offp, int nV, const int32_t* __restrict_
             if (bits < 5) bits = 5;
             for (int i = lane; i < (1 << bits); i += 32) tab[i] = -1;
             __syncwarp();
-            for (int i = lane; i < du; i += 32) tab_insert(tab, bits, fwd[ub + i]);
+            for (int i = lane; i < du; i += 32) tab_insert(tab, bits, g.fwd[ub + i]);
             __syncwarp();
-            mine += tc_vertex_warp<PER_VERTEX>(u, fwd + ub, du, tab, bits, 0, 1, offp, fwd,
-                                               s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
+            mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, bits, 0, 1, g, s_pref[warp],
+                                               s_vb[warp], s_v[warp], per_vertex);
             __syncwarp();
         }
     }
@@ -254,9 +296,9 @@ k_tc_warp(const long long* __restrict__ offp, int nV, const int32_t* __restrict_
 // Listed vertices (d+(u) > kWarpCap): one CTA each.
 template <bool PER_VERTEX>
 __global__ void __launch_bounds__(kTcWarps * 32)
-k_tc_cta(const long long* __restrict__ offp, const int32_t* __restrict__ fwd,
-         unsigned long long* __restrict__ per_vertex, unsigned long long* __restrict__ total_out,
-         const int* __restrict__ counters, const int32_t* __restrict__ big) {
+k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
+         unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
+         const int32_t* __restrict__ big) {
     extern __shared__ int s_dyn[];
     __shared__ long long s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
@@ -267,19 +309,19 @@ k_tc_cta(const long long* __restrict__ offp, const int32_t* __restrict__ fwd,
     unsigned long long mine = 0;
     for (int i = blockIdx.x; i < nbig; i += gridDim.x) {
         int u = big[i];
-        long long ub = offp[u];
-        int du = (int)(offp[u + 1] - ub);
+        long long ub = g.offp[u];
+        int du = (int)(g.offp[u + 1] - ub);
         const int* tab = nullptr;
         int bits = 0;
         if (du <= kCtaCap) {
             bits = 32 - __clz(2 * du - 1);
             for (int j = threadIdx.x; j < (1 << bits); j += blockDim.x) s_dyn[j] = -1;
             __syncthreads();
-            for (int j = threadIdx.x; j < du; j += blockDim.x) tab_insert(s_dyn, bits, fwd[ub + j]);
+            for (int j = threadIdx.x; j < du; j += blockDim.x) tab_insert(s_dyn, bits, g.fwd[ub + j]);
             tab = s_dyn;
         }
         __syncthreads();
-        mine += tc_vertex_warp<PER_VERTEX>(u, fwd + ub, du, tab, bits, warp, kTcWarps, offp, fwd,
+        mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, bits, warp, kTcWarps, g,
                                            s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
         __syncthreads();
     }
@@ -338,16 +380,17 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
         attr_set = true;
     }
     const long long gc = (long long)g->info.sms;
+    TcView view{o.offp.get(), o.fwd.get(), g->vtab, g->pool};
     if (d_per_vertex) {
         HN_CUDA(cudaMemsetAsync(d_per_vertex, 0, sizeof(unsigned long long) * g->nV, s));
-        HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, o.offp.get(), g->nV, o.fwd.get(),
-                  d_per_vertex, d_total, counters, big.get());
-        HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, o.offp.get(), o.fwd.get(),
-                  d_per_vertex, d_total, counters, big.get());
+        HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, view, g->nV, d_per_vertex, d_total,
+                  counters, big.get());
+        HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, view, d_per_vertex, d_total,
+                  counters, big.get());
     } else {
-        HN_LAUNCH(k_tc_warp<false>, gw, kTcWarps * 32, 0, s, o.offp.get(), g->nV, o.fwd.get(),
+        HN_LAUNCH(k_tc_warp<false>, gw, kTcWarps * 32, 0, s, view, g->nV,
                   (unsigned long long*)nullptr, d_total, counters, big.get());
-        HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, o.offp.get(), o.fwd.get(),
+        HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, view,
                   (unsigned long long*)nullptr, d_total, counters, big.get());
     }
     read_scalars(g, 1);
