@@ -111,6 +111,11 @@ _SIGNATURES = {
     "hn_coo_to_csr_device": [_I32, _I64, _P, _P, _INT, _P, _P, _P],
     "hn_free_device": [_P],
     "hn_cc_csr_noalloc": [_I32, _P, _P, _P, _P, _P],
+    "hn_csr_write_bin": [ctypes.c_char_p, _I32, _I32, _P, _P],
+    "hn_csr_read_bin": [ctypes.c_char_p, _P, _P, _P, _P],
+    "hn_csr_write_mtx": [ctypes.c_char_p, _I32, _I64, _P, _P],
+    "hn_graph_write_bin": [_P, ctypes.c_char_p],
+    "hn_graph_read_bin": [ctypes.c_char_p, _INT, _P],
 }
 _RESTYPES = {"hn_last_error_string": ctypes.c_char_p, "hn_kernel_launches": _I64}
 
@@ -590,6 +595,33 @@ def coo_to_csr_device(nV: int, src, dst, device: int = 0) -> DeviceCSR:
                                       ctypes.c_void_p(dst.data_ptr()), device, ctypes.byref(po),
                                       ctypes.byref(pa), ctypes.byref(ne)))
     return DeviceCSR(nV, po.value or 0, pa.value or 0, ne.value)
+
+
+def write_bin(path: str, off, adj) -> None:
+    """GraphStd binary (.bin) from a host CSR (int32 offsets)."""
+    off = np.ascontiguousarray(off, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32)
+    _check(lib().hn_csr_write_bin(path.encode(), len(off) - 1, len(adj),
+                                  off.ctypes.data_as(_P), adj.ctypes.data_as(_P)))
+
+
+def read_bin(path: str):
+    """(off, adj) host CSR from a GraphStd binary (.bin) file."""
+    nv, ne = ctypes.c_int32(), ctypes.c_int32()
+    _check(lib().hn_csr_read_bin(path.encode(), ctypes.byref(nv), ctypes.byref(ne), None, None))
+    off = np.empty(nv.value + 1, np.int32)
+    adj = np.empty(max(1, ne.value), np.int32)
+    _check(lib().hn_csr_read_bin(path.encode(), ctypes.byref(nv), ctypes.byref(ne),
+                                 off.ctypes.data_as(_P), adj.ctypes.data_as(_P)))
+    return off, adj[:ne.value]
+
+
+def write_mtx(path: str, off, adj) -> None:
+    """Matrix Market (coordinate pattern general, 1-based) from a host CSR."""
+    off = np.ascontiguousarray(off, np.int32)
+    adj = np.ascontiguousarray(adj, np.int32)
+    _check(lib().hn_csr_write_mtx(path.encode(), len(off) - 1, len(adj),
+                                  off.ctypes.data_as(_P), adj.ctypes.data_as(_P)))
 
 
 def hornet_from_device_csr(csr: DeviceCSR, device: int = 0) -> Hornet:

@@ -205,6 +205,25 @@ int hn_for_all_edges_count(hn_graph_t* g, const int32_t* vertices, int32_t n,
  * out[v] = degree(v) (Operator++.i.cuh:524-540). out: int32[nV] device. */
 int hn_for_all_vertices_degree(hn_graph_t* g, int32_t* out);
 
+/* ---- on-disk formats ------------------------------------------------------
+ * GraphStd binary (.bin): the reference's fast-reload format
+ * (xlib/src/Graph/GraphStd.cpp:389-420 writeBinary,
+ * xlib/src/Graph/GraphStdRead.cpp:212-245 readBinary) for int ids and
+ * offsets.  hn_csr_read_bin with off == NULL only reports nV and nE; call
+ * again with off[nV+1] and adj[nE] host buffers.  Files written with
+ * in-edges (DIRECTED | ENABLE_INGOING) are read for their out-edges. */
+int hn_csr_write_bin(const char* path, int32_t nV, int32_t nE, const int32_t* off,
+                     const int32_t* adj);
+int hn_csr_read_bin(const char* path, int32_t* nV, int32_t* nE, int32_t* off,
+                    int32_t* adj);
+/* Matrix Market coordinate pattern general, 1-based (the format GraphStd's
+ * Market reader takes, GraphStdRead.cpp:46-61).  Host CSR. */
+int hn_csr_write_mtx(const char* path, int32_t nV, int64_t nE, const int32_t* off,
+                     const int32_t* adj);
+/* getCSR + writeBinary / readBinary + HornetInit for a device graph. */
+int hn_graph_write_bin(hn_graph_t* g, const char* path);
+int hn_graph_read_bin(const char* path, int device, hn_graph_t** out);
+
 /* ---- connected components without device allocation ---------------------
  * No counterpart in the reference.  For callers that cannot allocate device
  * memory (a host framework that owns all device memory, a service whose
