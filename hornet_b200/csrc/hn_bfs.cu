@@ -30,12 +30,17 @@
 //     sets the WHILE condition with cudaGraphSetConditional; the loop also
 //     stops after nV levels, so it always terminates.
 // Distances equal the reference's: level-synchronous, INF = INT32_MAX.
+//
+// hn_bfs_do runs the same graph with a level kernel that may switch to
+// bottom-up steps (Beamer's direction-optimising BFS, the counterpart of
+// hornetsnest's BottomUpBFS, src/Static/BottomUpBreadthFirstSearch/
+// BottomUpBFS.cu); distances are identical, fewer edges are read.
 #include "hn_graph.cuh"
 
 namespace hn {
 
 constexpr int kBfsBlock = 256;
-constexpr int kIpt = 12;                         // edges per thread per chunk
+constexpr int kIpt = 8;                          // edges per thread per chunk
 constexpr int kChunk = kBfsBlock * kIpt;         // edges per chunk
 
 struct BfsState {
@@ -54,6 +59,10 @@ struct BfsState {
     unsigned* qoff[2];           // exclusive degree prefix (edge offset)
     int32_t* chunk[2];           // queue slot covering each chunk's first edge
     unsigned* bitmap;            // visited bits
+    int mode;                    // direction-optimising: 0 top-down, 1 bottom-up
+    int pad;
+    long long m_total;           // edges of the graph
+    long long edges_visited;     // sum of degrees of vertices reached so far
 };
 
 struct BfsGraph {
@@ -66,8 +75,8 @@ struct BfsGraph {
     unsigned* qoffbuf = nullptr;
     int32_t* chunkbuf = nullptr;
     unsigned* bitmap = nullptr;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraph_t graph[2] = {nullptr, nullptr};      // [0] top-down, [1] direction-optimising
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -112,16 +121,101 @@ __global__ void k_bfs3_init(BfsState* st) {
         st->ticket = 0;
         st->visited = 1;
         st->scanned = 0;
+        st->mode = 0;
+        st->edges_visited = d;
     }
 }
 
-__global__ void __launch_bounds__(kBfsBlock, 2)
-k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
-    __shared__ unsigned s_start[kChunk + 2];   // window edge offsets (+ end)
-    __shared__ long long s_base[kChunk + 1];   // pool index = s_base + edge
-    __shared__ int s_nw;
-    __shared__ unsigned long long s_wsum[kBfsBlock / 32];
-    __shared__ unsigned long long s_cbase;
+// Per-level shared memory of the level kernel.
+struct BfsSmem {
+    unsigned start[kChunk + 2];   // window edge offsets (+ end)
+    long long base[kChunk + 1];   // pool index = base + edge
+    int nw;
+    unsigned long long wsum[kBfsBlock / 32];
+    unsigned long long cbase;
+};
+
+// CTA-wide enqueue of this thread's claimed vertices w[k] (claim[k]):
+// distances written, vertices with edges appended to the next frontier with
+// their adjacency base and edge offset; ONE atomic per call reserves both
+// the queue slots and the edge range.  Must be called by all threads.
+__device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
+                                            const bool (&claim)[kIpt], int level,
+                                            const VRec* __restrict__ vtab, int32_t* dist,
+                                            unsigned long long* cout, int32_t* nqv,
+                                            long long* nqbase, unsigned* nqoff, int32_t* nchunk,
+                                            int& found) {
+    const int lane = threadIdx.x & 31;
+    long long roff[kIpt];
+    unsigned rdeg[kIpt];
+    unsigned long long mine = 0;   // (degree sum << 32) | queued count
+#pragma unroll
+    for (int k = 0; k < kIpt; k++) {
+        rdeg[k] = 0;
+        roff[k] = 0;
+        if (claim[k]) {
+            VRec r = vtab[w[k]];
+            rdeg[k] = (unsigned)r.deg;
+            roff[k] = r.off;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kIpt; k++) {
+        if (claim[k]) {
+            dist[w[k]] = level;
+            found++;
+            if (rdeg[k]) mine += ((unsigned long long)rdeg[k] << 32) | 1ull;
+        }
+    }
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += x;
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane == 31) sm.wsum[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        unsigned long long v = threadIdx.x < kBfsBlock / 32 ? sm.wsum[threadIdx.x] : 0ull;
+        unsigned long long vi = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, vi, o);
+            if (lane >= o) vi += x;
+        }
+        if (threadIdx.x < kBfsBlock / 32) sm.wsum[threadIdx.x] = vi - v;   // exclusive
+        unsigned long long tot = __shfl_sync(0xFFFFFFFFu, vi, 31);
+        if (threadIdx.x == 0) sm.cbase = tot ? atomicAdd(cout, tot) : 0ull;
+    }
+    __syncthreads();
+    unsigned long long at = sm.cbase + sm.wsum[warp] + (incl - mine);
+    int pos = (int)(at & 0xFFFFFFFFull);
+    unsigned off = (unsigned)(at >> 32);
+#pragma unroll
+    for (int k = 0; k < kIpt; k++) {
+        if (claim[k] && rdeg[k]) {
+            nqv[pos] = w[k];
+            nqbase[pos] = roff[k];
+            nqoff[pos] = off;
+            mark_chunks(nchunk, off, rdeg[k], pos);
+            pos++;
+            off += rdeg[k];
+        }
+    }
+    __syncthreads();
+}
+
+// One BFS level.  TopDown (always, or while st->mode == 0 when DO): the
+// frontier's edges in chunks.  BottomUp (DO and st->mode == 1): every
+// unvisited vertex scans its sorted neighbours for one at distance level-1
+// and stops at the first (Beamer, Asanovic & Patterson, "Direction-Optimizing
+// Breadth-First Search", SC 2012).  Both produce the next frontier queue, so
+// the direction may change at any level; distances are the same either way.
+template <bool DO>
+__global__ void __launch_bounds__(kBfsBlock, 4)
+k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
+    __shared__ BfsSmem sm;
     const int level = st->level;
     const int it = level - 1;
     const unsigned long long cin = st->cnt[it % 3];
@@ -130,9 +224,6 @@ k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
     const int nq = (int)(cin & 0xFFFFFFFFull);
     const unsigned total = (unsigned)(cin >> 32);
     const int cur = it & 1, nxt = cur ^ 1;
-    const long long* qbase = st->qbase[cur];
-    const unsigned* qoff = st->qoff[cur];
-    const int32_t* chunk = st->chunk[cur];
     int32_t* nqv = st->q[nxt];
     long long* nqbase = st->qbase[nxt];
     unsigned* nqoff = st->qoff[nxt];
@@ -142,127 +233,99 @@ k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
     unsigned* bm = st->bitmap;
     int32_t* dist = st->dist;
     const int lane = threadIdx.x & 31;
+    const int mode = DO ? st->mode : 0;
     int found = 0;
 
-    const unsigned nchunks = (total + kChunk - 1) / kChunk;
-    for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
-        const unsigned e0 = c * kChunk;
-        const unsigned e1 = e0 + kChunk < total ? e0 + kChunk : total;
-        const int s0 = chunk[c];
-        const int s1 = c + 1 < nchunks ? chunk[c + 1] : nq - 1;   // inclusive
-        const int nw = s1 - s0 + 1;
-        for (int j = threadIdx.x; j <= nw; j += kBfsBlock) {
-            int s = s0 + j;
-            unsigned so = qoff[s];        // qoff[nq] is the sealed total
-            s_start[j] = so;
-            if (j < nw) s_base[j] = qbase[s] - (long long)so;
-        }
-        if (threadIdx.x == 0) s_nw = nw;
-        __syncthreads();
-        // this thread's edges [a, b)
-        const unsigned a = e0 + threadIdx.x * kIpt;
-        const unsigned b = a + kIpt < e1 ? a + kIpt : e1;
-        int w[kIpt];
-        bool claim[kIpt];
-        if (a < b) {
-            int lo = 0, hi = s_nw;        // last j with s_start[j] <= a
-            while (hi - lo > 1) {
-                int mid = (lo + hi) >> 1;
-                if (s_start[mid] <= a) lo = mid; else hi = mid;
+    if (mode == 0) {
+        const long long* qbase = st->qbase[cur];
+        const unsigned* qoff = st->qoff[cur];
+        const int32_t* chunk = st->chunk[cur];
+        const unsigned nchunks = (total + kChunk - 1) / kChunk;
+        for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
+            const unsigned e0 = c * kChunk;
+            const unsigned e1 = e0 + kChunk < total ? e0 + kChunk : total;
+            const int s0 = chunk[c];
+            const int s1 = c + 1 < nchunks ? chunk[c + 1] : nq - 1;   // inclusive
+            const int nw = s1 - s0 + 1;
+            for (int j = threadIdx.x; j <= nw; j += kBfsBlock) {
+                int s = s0 + j;
+                unsigned so = qoff[s];        // qoff[nq] is the sealed total
+                sm.start[j] = so;
+                if (j < nw) sm.base[j] = qbase[s] - (long long)so;
             }
-            int j = lo;
+            if (threadIdx.x == 0) sm.nw = nw;
+            __syncthreads();
+            // this thread's edges [a, b)
+            const unsigned a = e0 + threadIdx.x * kIpt;
+            const unsigned b = a + kIpt < e1 ? a + kIpt : e1;
+            int w[kIpt];
+            bool claim[kIpt];
 #pragma unroll
-            for (int k = 0; k < kIpt; k++) {
-                unsigned e = a + k;
-                if (e < b) {
-                    while (s_start[j + 1] <= e) j++;
-                    w[k] = __ldg(pool + s_base[j] + e);
-                } else {
-                    w[k] = -1;
+            for (int k = 0; k < kIpt; k++) { w[k] = -1; claim[k] = false; }
+            if (a < b) {
+                int lo = 0, hi = sm.nw;        // last j with start[j] <= a
+                while (hi - lo > 1) {
+                    int mid = (lo + hi) >> 1;
+                    if (sm.start[mid] <= a) lo = mid; else hi = mid;
+                }
+                int j = lo;
+#pragma unroll
+                for (int k = 0; k < kIpt; k++) {
+                    unsigned e = a + k;
+                    if (e < b) {
+                        while (sm.start[j + 1] <= e) j++;
+                        w[k] = __ldg(pool + sm.base[j] + e);
+                    }
+                }
+                unsigned word[kIpt];
+#pragma unroll
+                for (int k = 0; k < kIpt; k++)
+                    word[k] = w[k] >= 0 ? __ldcg(bm + (w[k] >> 5)) : 0xFFFFFFFFu;
+#pragma unroll
+                for (int k = 0; k < kIpt; k++) {
+                    if (w[k] >= 0 && !(word[k] & (1u << (w[k] & 31)))) {
+                        unsigned bit = 1u << (w[k] & 31);
+                        claim[k] = !(atomicOr(bm + (w[k] >> 5), bit) & bit);
+                    }
                 }
             }
-            unsigned word[kIpt];
-#pragma unroll
-            for (int k = 0; k < kIpt; k++)
-                word[k] = w[k] >= 0 ? __ldcg(bm + (w[k] >> 5)) : 0xFFFFFFFFu;
+            bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk, found);
+        }
+    } else {
+        // bottom-up over all vertices, kIpt per thread, striped
+        const int nV = st->nV;
+        const int per = kBfsBlock * kIpt;
+        const int nvc = (nV + per - 1) / per;
+        for (int c = blockIdx.x; c < nvc; c += gridDim.x) {
+            int w[kIpt];
+            bool claim[kIpt];
+            int dv[kIpt];
 #pragma unroll
             for (int k = 0; k < kIpt; k++) {
+                int v = c * per + k * kBfsBlock + threadIdx.x;
+                w[k] = v < nV ? v : -1;
                 claim[k] = false;
-                if (w[k] >= 0 && !(word[k] & (1u << (w[k] & 31)))) {
-                    unsigned bit = 1u << (w[k] & 31);
-                    claim[k] = !(atomicOr(bm + (w[k] >> 5), bit) & bit);
+                dv[k] = w[k] >= 0 ? __ldcg(dist + v) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < kIpt; k++) {
+                if (w[k] >= 0 && dv[k] == kInf) {
+                    VRec r = vtab[w[k]];
+                    const int32_t* nb = pool + r.off;
+                    for (int i = 0; i < r.deg; i++) {
+                        if (__ldcg(dist + nb[i]) == level - 1) { claim[k] = true; break; }
+                    }
+                    if (claim[k]) atomicOr(bm + (w[k] >> 5), 1u << (w[k] & 31));
                 }
             }
-        } else {
-#pragma unroll
-            for (int k = 0; k < kIpt; k++) claim[k] = false;
+            bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk, found);
         }
-        // claimed vertices: records loaded together, distances written
-        long long roff[kIpt];
-        unsigned rdeg[kIpt];
-        unsigned long long mine = 0;   // (degree sum << 32) | queued count
-#pragma unroll
-        for (int k = 0; k < kIpt; k++) {
-            rdeg[k] = 0;
-            roff[k] = 0;
-            if (claim[k]) {
-                VRec r = vtab[w[k]];
-                rdeg[k] = (unsigned)r.deg;
-                roff[k] = r.off;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < kIpt; k++) {
-            if (claim[k]) {
-                dist[w[k]] = level;
-                found++;
-                if (rdeg[k]) mine += ((unsigned long long)rdeg[k] << 32) | 1ull;  // queued
-            }
-        }
-        // CTA-wide exclusive scan of the packed counters; ONE atomic per
-        // chunk reserves both the queue slots and the edge range
-        unsigned long long incl = mine;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += x;
-        }
-        const int warp = threadIdx.x >> 5;
-        if (lane == 31) s_wsum[warp] = incl;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            unsigned long long v = threadIdx.x < kBfsBlock / 32 ? s_wsum[threadIdx.x] : 0ull;
-            unsigned long long vi = v;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, vi, o);
-                if (lane >= o) vi += x;
-            }
-            if (threadIdx.x < kBfsBlock / 32) s_wsum[threadIdx.x] = vi - v;   // exclusive
-            unsigned long long tot = __shfl_sync(0xFFFFFFFFu, vi, 31);
-            if (threadIdx.x == 0) s_cbase = tot ? atomicAdd(cout, tot) : 0ull;
-        }
-        __syncthreads();
-        unsigned long long at = s_cbase + s_wsum[warp] + (incl - mine);
-        int pos = (int)(at & 0xFFFFFFFFull);
-        unsigned off = (unsigned)(at >> 32);
-#pragma unroll
-        for (int k = 0; k < kIpt; k++) {
-            if (claim[k] && rdeg[k]) {
-                nqv[pos] = w[k];
-                nqbase[pos] = roff[k];
-                nqoff[pos] = off;
-                mark_chunks(nchunk, off, rdeg[k], pos);
-                pos++;
-                off += rdeg[k];
-            }
-        }
-        __syncthreads();
     }
     // visited count: one atomic per warp
     for (int o = 16; o; o >>= 1) found += __shfl_down_sync(0xFFFFFFFFu, found, o);
     if (lane == 0 && found) atomicAdd((unsigned long long*)&st->visited, (unsigned long long)found);
-    // the last CTA seals the next frontier and decides whether to loop
+    // the last CTA seals the next frontier, picks the next direction and
+    // decides whether to loop
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -271,10 +334,23 @@ k_bfs3_expand(BfsState* st, cudaGraphConditionalHandle cond) {
             __threadfence();
             unsigned long long cn = atomicAdd(cout, 0ull);
             unsigned nn = (unsigned)(cn & 0xFFFFFFFFull);
-            nqoff[nn] = (unsigned)(cn >> 32);
+            unsigned long long mf = cn >> 32;
+            nqoff[nn] = (unsigned)mf;
             st->ticket = 0;
             st->scanned += total;
             st->level = level + 1;
+            if (DO) {
+                // Beamer's switch: to bottom-up when the next frontier's edges
+                // exceed 1/14 of the unexplored edges, back to top-down when
+                // the frontier falls below nV/24 vertices and is shrinking
+                st->edges_visited += (long long)mf;
+                long long mu = st->m_total - st->edges_visited;
+                if (st->mode == 0) {
+                    if ((long long)mf * 14 > mu) st->mode = 1;
+                } else {
+                    if ((long long)nn * 24 < st->nV && nn < (unsigned)nq) st->mode = 0;
+                }
+            }
             cudaGraphSetConditional(cond, (nn > 0 && level < st->nV) ? 1u : 0u);
         }
     }
@@ -293,44 +369,49 @@ void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
     bg.nV = nV;
     bg.nchunk_cap = nchunk_cap;
 
-    HN_CUDA(cudaGraphCreate(&bg.graph, 0));
-    cudaGraphNode_t init_node, cond_node, body_node;
-    {
-        void* args[] = {&bg.state};
-        cudaKernelNodeParams p = {};
-        p.func = (void*)k_bfs3_init;
-        p.gridDim = dim3((unsigned)grid_for(g, nV, 256));
-        p.blockDim = dim3(256);
-        p.kernelParams = args;
-        HN_CUDA(cudaGraphAddKernelNode(&init_node, bg.graph, nullptr, 0, &p));
+    for (int variant = 0; variant < 2; variant++) {
+        cudaGraph_t& graph = bg.graph[variant];
+        HN_CUDA(cudaGraphCreate(&graph, 0));
+        cudaGraphNode_t init_node, cond_node, body_node;
+        {
+            void* args[] = {&bg.state};
+            cudaKernelNodeParams p = {};
+            p.func = (void*)k_bfs3_init;
+            p.gridDim = dim3((unsigned)grid_for(g, nV, 256));
+            p.blockDim = dim3(256);
+            p.kernelParams = args;
+            HN_CUDA(cudaGraphAddKernelNode(&init_node, graph, nullptr, 0, &p));
+        }
+        cudaGraphConditionalHandle handle;
+        HN_CUDA(cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        HN_CUDA(cudaGraphAddNode(&cond_node, graph, &init_node, 1, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        {
+            void* args[] = {&bg.state, &handle};
+            cudaKernelNodeParams p = {};
+            p.func = variant ? (void*)k_bfs_level<true> : (void*)k_bfs_level<false>;
+            p.gridDim = dim3((unsigned)g->info.sms * 4);
+            p.blockDim = dim3(kBfsBlock);
+            p.kernelParams = args;
+            HN_CUDA(cudaGraphAddKernelNode(&body_node, body, nullptr, 0, &p));
+        }
+        HN_CUDA(cudaGraphInstantiate(&bg.exec[variant], graph, 0));
     }
-    cudaGraphConditionalHandle handle;
-    HN_CUDA(cudaGraphConditionalHandleCreate(&handle, bg.graph, 1, cudaGraphCondAssignDefault));
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = handle;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    HN_CUDA(cudaGraphAddNode(&cond_node, bg.graph, &init_node, 1, &cp));
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    {
-        void* args[] = {&bg.state, &handle};
-        cudaKernelNodeParams p = {};
-        p.func = (void*)k_bfs3_expand;
-        p.gridDim = dim3((unsigned)g->info.sms * 2);
-        p.blockDim = dim3(kBfsBlock);
-        p.kernelParams = args;
-        HN_CUDA(cudaGraphAddKernelNode(&body_node, body, nullptr, 0, &p));
-    }
-    HN_CUDA(cudaGraphInstantiate(&bg.exec, bg.graph, 0));
 }
 
 }  // namespace
 
 void free_bfs_graph(BfsGraph* bg) {
     if (!bg) return;
-    if (bg->exec) cudaGraphExecDestroy(bg->exec);
-    if (bg->graph) cudaGraphDestroy(bg->graph);
+    for (int i = 0; i < 2; i++) {
+        if (bg->exec[i]) cudaGraphExecDestroy(bg->exec[i]);
+        if (bg->graph[i]) cudaGraphDestroy(bg->graph[i]);
+    }
     if (bg->state) cudaFree(bg->state);
     if (bg->h_state) cudaFreeHost(bg->h_state);
     if (bg->qbuf) cudaFree(bg->qbuf);
@@ -365,7 +446,7 @@ BfsGraph& bfs_graph_of(hn_graph* g) {
 }
 
 void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
-             hn_bfs_stats_t* stats) {
+             hn_bfs_stats_t* stats, bool direction_optimizing) {
     cudaStream_t s = g->stream;
     const int nV = g->nV;
     for (int i = 0; i < k; i++)
@@ -395,13 +476,15 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.chunk[0] = bg.chunkbuf;
         h.chunk[1] = bg.chunkbuf + bg.nchunk_cap;
         h.bitmap = bg.bitmap;
+        h.m_total = g->nE;
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
         // profiling records the whole graph (one init + one expand per
         // level) under the name of its dominant kernel
         cudaEvent_t ev0 = nullptr;
         if (g_profiling) profile_begin(s, &ev0);
-        HN_CUDA(cudaGraphLaunch(bg.exec, s));
-        if (ev0) profile_end("k_bfs3_expand", s, ev0);
+        HN_CUDA(cudaGraphLaunch(bg.exec[direction_optimizing ? 1 : 0], s));
+        if (ev0)
+            profile_end(direction_optimizing ? "k_bfs_level<true>" : "k_bfs_level<false>", s, ev0);
         count_launch(2);
         HN_CUDA(cudaMemcpyAsync(bg.h_state, bg.state, sizeof(BfsState), cudaMemcpyDeviceToHost, s));
         if (mem == HN_MEM_HOST)
@@ -432,7 +515,7 @@ int hn_bfs(hn_graph_t* g, int32_t src, int32_t* dist, int mem, hn_bfs_stats_t* s
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_REQUIRE(g->nV > 0, "empty graph");
     HN_CUDA(cudaSetDevice(g->device));
-    bfs_run(g, &src, 1, dist, mem, stats);
+    bfs_run(g, &src, 1, dist, mem, stats, false);
     HN_API_END
 }
 
@@ -444,7 +527,19 @@ int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_REQUIRE(g->nV > 0 || k == 0, "empty graph");
     HN_CUDA(cudaSetDevice(g->device));
-    bfs_run(g, sources, k, dist, mem, stats);
+    bfs_run(g, sources, k, dist, mem, stats, false);
+    HN_API_END
+}
+
+int hn_bfs_do(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist, int mem,
+              hn_bfs_stats_t* stats) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && sources && dist, "null argument");
+    HN_REQUIRE(k >= 0, "negative source count");
+    HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    HN_REQUIRE(g->nV > 0 || k == 0, "empty graph");
+    HN_CUDA(cudaSetDevice(g->device));
+    bfs_run(g, sources, k, dist, mem, stats, true);
     HN_API_END
 }
 

@@ -119,6 +119,10 @@ constexpr int kWarpTab = 2 * kWarpCap;
 constexpr int kCtaCap = 16384;
 constexpr int kChunk = 16;
 constexpr int kUnroll = 4;
+// 1: every oriented edge (u,v) is counted by u, walking N+(v) against
+//    table(u); 2: counted by the endpoint with the longer list (fewer probes,
+//    but in-neighbour work concentrates on high-in-degree vertices).
+constexpr int kPhases = 1;
 
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
@@ -164,7 +168,7 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
     const VRec ru = g.vtab[u];
     unsigned long long cnt = 0;
 #pragma unroll 1
-    for (int phase = 0; phase < 2; phase++) {
+    for (int phase = 0; phase < kPhases; phase++) {
         const int32_t* cand = phase == 0 ? L : g.pool + ru.off;
         const int ncand = phase == 0 ? du : ru.deg;
         for (int c0 = cand_begin * 32; c0 < ncand; c0 += cand_step * 32) {
@@ -181,7 +185,7 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                 if (take) {
                     xb = g.offp[x];
                     dx = g.offp[x + 1] - xb;
-                    if (phase == 0 ? dx > du : dx >= du) dx = 0;   // other side walks
+                    if (kPhases == 2 && (phase == 0 ? dx > du : dx >= du)) dx = 0;
                 }
             }
             long long incl = dx;

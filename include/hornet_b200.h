@@ -171,6 +171,14 @@ int hn_bfs(hn_graph_t* g, int32_t src, int32_t* dist, int mem,
 int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k,
                  int32_t* dist, int mem, hn_bfs_stats_t* stats);
 
+/* Direction-optimising BFS (top-down levels switch to bottom-up ones while
+ * the frontier is large; the counterpart of hornetsnest's BottomUpBFS,
+ * src/Static/BottomUpBreadthFirstSearch/BottomUpBFS.cu).  Same arguments
+ * and the same distances as hn_bfs_multi; stats count the same edges
+ * (sum of degrees of reached vertices), although fewer are read. */
+int hn_bfs_do(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist,
+              int mem, hn_bfs_stats_t* stats);
+
 /* TriangleCounting2::init/run/countTriangles
  * (hornetsnest/src/Static/TriangleCounting/triangle2.cu:130-171) on the
  * graph's undirected adjacency, each triangle counted once via the

@@ -184,6 +184,24 @@ def test_bfs(name):
         np.testing.assert_array_equal(out, O.ref_bfs(g, srcs))
 
 
+@pytest.mark.parametrize("name", ["rmat10", "er2000", "rmat12_nonpow2"])
+def test_bfs_direction_optimizing(name):
+    """Direction-optimising BFS (bottom-up levels on large frontiers) gives
+    exactly the top-down distances and counts the same scanned edges."""
+    g = GRAPHS[name]()
+    h = build(g)
+    rng = np.random.default_rng(6)
+    srcs = [0] + [int(x) for x in rng.integers(0, g.nV, 5)]
+    td, td_stats = H.BfsTopDown(h).run_multi(srcs)
+    do, do_stats = H.BfsTopDown(h).run_multi(srcs, direction_optimizing=True)
+    np.testing.assert_array_equal(do, td)
+    for i, s in enumerate(srcs):
+        np.testing.assert_array_equal(do[i], O.bfs(g, s)[0])
+        assert do_stats[i].edges_scanned == td_stats[i].edges_scanned
+        assert do_stats[i].visited == td_stats[i].visited
+        assert do_stats[i].levels == td_stats[i].levels
+
+
 def test_bfs_isolated_source():
     s = np.array([1, 2], np.int32)
     d = np.array([2, 3], np.int32)
