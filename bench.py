@@ -440,17 +440,29 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     sizes = [int(x) for x in args.batch_sizes.split(",")]
     rng = np.random.default_rng(5 + rank)
     batches = []
+    deg0 = np.asarray(deg, np.int64)
+    model = []   # algorithmic bytes of (insert, erase) per batch
     for b in sizes:
-        bs = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda(dev)
-        bd = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda(dev)
+        bs_h = rng.integers(0, nV, b).astype(np.int32)
+        bd_h = rng.integers(0, nV, b).astype(np.int32)
+        bs = torch.from_numpy(bs_h).cuda(dev)
+        bd = torch.from_numpy(bd_h).cuda(dev)
         batches.append((H.BatchUpdate(h, bs, bd), b, bs, bd))
+        # insert: 8b + 4*applied + 4*sum deg_old(u) over distinct sources;
+        # the erase that follows sees deg_old + the inserted edges
+        keys = np.unique((bs_h.astype(np.int64) << 32) | bd_h.astype(np.int64))
+        u = (keys >> 32).astype(np.int64)
+        uu, cnt = np.unique(u, return_counts=True)
+        model.append((8 * b + 4 * len(keys) + 4 * int(deg0[uu].sum()),
+                      8 * b + 4 * len(keys) + 4 * int((deg0[uu] + cnt).sum())))
+    applied = [0]
 
     def step(i):
         bt, b, _, _ = batches[(i // 2) % len(batches)]
         if i % 2 == 0:
-            h.insert(bt, True, True)
+            applied[0] += h.insert(bt, True, True)
         else:
-            h.erase(bt, True)
+            applied[0] += h.erase(bt, True)
         return b
 
     for i in range(W + (W % 2)):
@@ -473,6 +485,26 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     clk = clocks.stop()
     t_max = max_over_ranks(t)
     value = sum_over_ranks(edges[0]) / t_max
+    # path roofline: model bytes of the timed steps over their device time
+    # (graph de-duplication makes insert then erase of a batch a round trip,
+    # so every step sees the initial degrees, plus the batch for erases)
+    model_bytes = sum(model[((start + i) // 2) % len(model)][(start + i) % 2] for i in range(K))
+    achieved = model_bytes / t / 1e9
+    per_size = []
+    for j, b in enumerate(sizes):
+        ti = event_time(stream, lambda: step(2 * j))
+        te = event_time(stream, lambda: step(2 * j + 1))
+        per_size.append({"batch": b, "insert_edges_per_s": round(b / ti, 1),
+                         "erase_edges_per_s": round(b / te, 1),
+                         "insert_frac": round(model[j][0] / ti / 1e9 / peak, 4),
+                         "erase_frac": round(model[j][1] / te / 1e9 / peak, 4)})
+    roof = {"kernel": "update path (sort, mark, scan, plan, assign, scatter, commit)",
+            "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": None,
+            "algorithmic_bytes_per_launch": round(model_bytes / K),
+            "peak_kind": peak_kind, "per_batch_size": per_size,
+            "note": "device time of whole insert/erase calls (includes the one host "
+                    "synchronisation per batch)"}
     # e2e: host batch arrays copied in every step
     host = [(bs.cpu().numpy(), bd.cpu().numpy(), b) for (_, b, bs, bd) in batches]
     bt = H.BatchUpdate(h, host[0][0][:1], host[0][1][:1])
@@ -505,7 +537,7 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
                    "nV": nV, "nE": nE, "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(sum_over_ranks(e_edges) / t_e2e, 1), "unit": "edges/s",
                 "h2d_bytes_per_step": hb // K, "d2h_bytes_per_step": 8},
-        "roofline": None, "kernels_ms": {k: round(v["ms"], 4) for k, v in rep.items()},
+        "roofline": roof, "kernels_ms": {k: round(v["ms"], 4) for k, v in rep.items()},
         "cpu_baseline": None, "gpu_launches": int(launches), "clocks": clk,
     }
 

@@ -93,20 +93,15 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
 }
 
 // ---------------------------------------------------------------------------
-// Vertex-centric counting, each edge probed from its smaller side.
-// For each vertex u, N+(u) goes into an open-addressing hash table in shared
-// memory (multiplicative hash, linear probing, load factor <= 1/2, so every
-// probe sequence ends at an empty slot).  Every oriented edge (u,v) needs
-// |N+(u) ∩ N+(v)|; it is counted by whichever endpoint has the LONGER list,
-// walking the shorter list against that endpoint's table:
-//   out-phase: v in N+(u) with d+(v) <= d+(u): walk N+(v), probe table(u);
-//   in-phase:  x in N-(u) (undirected neighbours that precede u in the
-//              (degree, id) order) with d+(x) < d+(u): walk N+(x), probe
-//              table(u).
-// So each edge costs min(d+(u), d+(v)) probes.  The (candidate, element)
-// pairs of 32 candidates at a time are flattened over the lanes (warp
-// prefix of the list lengths), each lane keeps 4 element loads in flight,
-// and elements outside [min N+(u), max N+(u)] are skipped before probing.
+// Vertex-centric counting.  For each vertex u, N+(u) goes into an
+// open-addressing hash table in shared memory (multiplicative hash, linear
+// probing, load factor <= 1/2, so every probe sequence ends at an empty
+// slot).  Every oriented edge (u,v) is counted by its tail u: the elements
+// of N+(v) are probed against table(u), after N+(v) is narrowed to
+// [min N+(u), max N+(u)] by two binary searches.  The (v, w) pairs of 32
+// candidates v at a time are split into 32 equal contiguous shares, so each
+// lane walks its share sequentially (coalescing-friendly, no per-pair
+// search).
 //   k_tc_warp: one warp per vertex with d+(u) <= kWarpCap; vertices handed
 //              out in chunks by an atomic counter; larger ones are listed;
 //   k_tc_cta:  one CTA per listed vertex, table in dynamic shared memory
@@ -118,11 +113,6 @@ constexpr int kWarpCap = 512;
 constexpr int kWarpTab = 2 * kWarpCap;
 constexpr int kCtaCap = 16384;
 constexpr int kChunk = 16;
-constexpr int kUnroll = 4;
-// 1: every oriented edge (u,v) is counted by u, walking N+(v) against
-//    table(u); 2: counted by the endpoint with the longer list (fewer probes,
-//    but in-neighbour work concentrates on high-in-degree vertices).
-constexpr int kPhases = 1;
 
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
@@ -152,98 +142,92 @@ __device__ __forceinline__ bool tab_find(const int* tab, int bits, int w) {
 struct TcView {
     const long long* offp;   // oriented offsets
     const int32_t* fwd;      // oriented lists
-    const VRec* vtab;        // undirected graph (for in-neighbours)
-    const int32_t* pool;
 };
 
-// One warp: the probes u is responsible for.  Membership in N+(u) by hash
-// table (tab != nullptr) or binary search of the sorted global list L.
+// One warp: every (v, w) pair of u, w in N+(v) for v in N+(u), probed
+// against N+(u) (hash table `tab`, or binary search of the sorted global
+// list L when tab == nullptr).  Candidates v are taken 32 at a time; each
+// lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
+// searches, then the warp's pairs are split into 32 equal contiguous
+// shares, so each lane walks its share sequentially with no per-pair search
+// (one search over the 33-entry prefix per lane per group).
 template <bool PER_VERTEX>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int* tab, int bits, int cand_begin,
-    int cand_step, const TcView& g, long long* s_pref /*33*/, long long* s_vb /*32*/,
+    int cand_step, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
     int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
     const int lo_w = L[0], hi_w = L[du - 1];
-    const VRec ru = g.vtab[u];
     unsigned long long cnt = 0;
-#pragma unroll 1
-    for (int phase = 0; phase < kPhases; phase++) {
-        const int32_t* cand = phase == 0 ? L : g.pool + ru.off;
-        const int ncand = phase == 0 ? du : ru.deg;
-        for (int c0 = cand_begin * 32; c0 < ncand; c0 += cand_step * 32) {
-            int idx = c0 + lane;
-            long long dx = 0, xb = 0;
-            int x = 0;
-            if (idx < ncand) {
-                x = cand[idx];
-                bool take = true;
-                if (phase == 1) {
-                    VRec rx = g.vtab[x];
-                    take = rx.deg < ru.deg || (rx.deg == ru.deg && x < u);   // x precedes u
-                }
-                if (take) {
-                    xb = g.offp[x];
-                    dx = g.offp[x + 1] - xb;
-                    if (kPhases == 2 && (phase == 0 ? dx > du : dx >= du)) dx = 0;
-                }
-            }
-            long long incl = dx;
-            for (int o = 1; o < 32; o <<= 1) {
-                long long y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            s_pref[lane + 1] = incl;
-            if (lane == 0) s_pref[0] = 0;
-            s_vb[lane] = xb;
-            s_v[lane] = x;
-            __syncwarp();
-            const long long T = s_pref[32];
-            for (long long k0 = lane; k0 < T; k0 += 32 * kUnroll) {
-                int wv[kUnroll];
-                int sl[kUnroll];
-#pragma unroll
-                for (int j = 0; j < kUnroll; j++) {
-                    long long k = k0 + 32 * j;
-                    wv[j] = -1;
-                    sl[j] = 0;
-                    if (k < T) {
-                        int a = 0, b = 32;   // slot of pair k: last s with s_pref[s] <= k
-                        while (b - a > 1) {
-                            int mid = (a + b) >> 1;
-                            if (s_pref[mid] <= k) a = mid; else b = mid;
-                        }
-                        sl[j] = a;
-                        wv[j] = g.fwd[s_vb[a] + (k - s_pref[a])];
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < kUnroll; j++) {
-                    int w = wv[j];
-                    if (w < lo_w || w > hi_w) continue;   // also drops the -1 fillers
-                    bool hit;
-                    if (tab) {
-                        hit = tab_find(tab, bits, w);
-                    } else {
-                        int lo = 0, hi = du;
-                        while (lo < hi) {
-                            int mid = (lo + hi) >> 1;
-                            if (L[mid] < w) lo = mid + 1; else hi = mid;
-                        }
-                        hit = lo < du && L[lo] == w;
-                    }
-                    if (hit) {
-                        cnt++;
-                        if (PER_VERTEX) {
-                            atomicAdd(per_vertex + w, 1ull);
-                            atomicAdd(per_vertex + u, 1ull);
-                            atomicAdd(per_vertex + s_v[sl[j]], 1ull);
-                        }
-                    }
-                }
-            }
-            __syncwarp();
+    for (int c0 = cand_begin * 32; c0 < du; c0 += cand_step * 32) {
+        int idx = c0 + lane;
+        int dx = 0, v = 0;
+        long long xb = 0;
+        if (idx < du) {
+            v = L[idx];
+            long long b0 = g.offp[v], b1 = g.offp[v + 1];
+            const int32_t* lst = g.fwd + b0;
+            int n = (int)(b1 - b0);
+            // [first element >= lo_w, first element > hi_w)
+            int lo = 0, hi = n;
+            while (lo < hi) { int m = (lo + hi) >> 1; if (lst[m] < lo_w) lo = m + 1; else hi = m; }
+            int s0 = lo;
+            hi = n;
+            while (lo < hi) { int m = (lo + hi) >> 1; if (lst[m] <= hi_w) lo = m + 1; else hi = m; }
+            xb = b0 + s0;
+            dx = lo - s0;
         }
+        int incl = dx;
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        s_pref[lane + 1] = incl;
+        if (lane == 0) s_pref[0] = 0;
+        s_vb[lane] = xb;
+        s_v[lane] = v;
+        __syncwarp();
+        const int T = s_pref[32];
+        // this lane's share of the pairs: [k0, k1)
+        const int k0 = (int)((long long)T * lane / 32);
+        const int k1 = (int)((long long)T * (lane + 1) / 32);
+        if (k0 < k1) {
+            int a = 0, b = 32;   // candidate slot of pair k0
+            while (b - a > 1) {
+                int mid = (a + b) >> 1;
+                if (s_pref[mid] <= k0) a = mid; else b = mid;
+            }
+            int end = s_pref[a + 1];
+            const int32_t* p = g.fwd + s_vb[a] + (k0 - s_pref[a]);
+            for (int k = k0; k < k1; k++) {
+                while (k >= end) {   // next non-empty candidate
+                    a++;
+                    end = s_pref[a + 1];
+                    p = g.fwd + s_vb[a];
+                }
+                int w = *p++;
+                bool hit;
+                if (tab) {
+                    hit = tab_find(tab, bits, w);
+                } else {
+                    int lo = 0, hi = du;
+                    while (lo < hi) {
+                        int mid = (lo + hi) >> 1;
+                        if (L[mid] < w) lo = mid + 1; else hi = mid;
+                    }
+                    hit = lo < du && L[lo] == w;
+                }
+                if (hit) {
+                    cnt++;
+                    if (PER_VERTEX) {
+                        atomicAdd(per_vertex + w, 1ull);
+                        atomicAdd(per_vertex + u, 1ull);
+                        atomicAdd(per_vertex + s_v[a], 1ull);
+                    }
+                }
+            }
+        }
+        __syncwarp();
     }
     return cnt;
 }
@@ -255,7 +239,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
           int32_t* __restrict__ big) {
     __shared__ int s_tab[kTcWarps][kWarpTab];
-    __shared__ long long s_pref[kTcWarps][33];
+    __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
     __shared__ unsigned long long s_sum[kTcWarps];
@@ -304,7 +288,7 @@ k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
          const int32_t* __restrict__ big) {
     extern __shared__ int s_dyn[];
-    __shared__ long long s_pref[kTcWarps][33];
+    __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
     __shared__ unsigned long long s_sum[kTcWarps];
@@ -384,7 +368,7 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
         attr_set = true;
     }
     const long long gc = (long long)g->info.sms;
-    TcView view{o.offp.get(), o.fwd.get(), g->vtab, g->pool};
+    TcView view{o.offp.get(), o.fwd.get()};
     if (d_per_vertex) {
         HN_CUDA(cudaMemsetAsync(d_per_vertex, 0, sizeof(unsigned long long) * g->nV, s));
         HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, view, g->nV, d_per_vertex, d_total,
