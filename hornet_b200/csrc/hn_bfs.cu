@@ -19,6 +19,11 @@
 //     vertex window with two loads — no search in global memory.  Only
 //     vertices with at least one edge are queued, so a chunk spans at most
 //     kChunk + 1 queue entries.
+//   * Visited-bitmap probes go through L1 (ld.ca): on power-law graphs most
+//     edges point at a few hubs, and L2-only probes of their bitmap words
+//     turn into a hot spot on a few L2 slices.  A stale L1 copy can only
+//     miss bits set during this level (bits never clear), which costs an
+//     extra atomicOr and never a wrong claim.
 //   * A CTA stages the window's (edge offset, adjacency base) pairs in
 //     shared memory; each thread takes kIpt consecutive edges, finds its
 //     first vertex by a shared-memory binary search, then issues all kIpt
@@ -280,7 +285,7 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
                 unsigned word[kIpt];
 #pragma unroll
                 for (int k = 0; k < kIpt; k++)
-                    word[k] = w[k] >= 0 ? __ldcg(bm + (w[k] >> 5)) : 0xFFFFFFFFu;
+                    word[k] = w[k] >= 0 ? __ldca(bm + (w[k] >> 5)) : 0xFFFFFFFFu;
 #pragma unroll
                 for (int k = 0; k < kIpt; k++) {
                     if (w[k] >= 0 && !(word[k] & (1u << (w[k] & 31)))) {
@@ -313,7 +318,7 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
                     VRec r = vtab[w[k]];
                     const int32_t* nb = pool + r.off;
                     for (int i = 0; i < r.deg; i++) {
-                        if (__ldcg(dist + nb[i]) == level - 1) { claim[k] = true; break; }
+                        if (__ldca(dist + nb[i]) == level - 1) { claim[k] = true; break; }
                     }
                     if (claim[k]) atomicOr(bm + (w[k] >> 5), 1u << (w[k] & 31));
                 }
