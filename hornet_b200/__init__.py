@@ -102,6 +102,7 @@ _SIGNATURES = {
     "hn_bfs": [_P, _I32, _P, _INT, _P],
     "hn_bfs_multi": [_P, _P, _I32, _P, _INT, _P],
     "hn_bfs_do": [_P, _P, _I32, _P, _INT, _P],
+    "hn_bfs_batch": [_P, _P, _P, _I32, _I32, _P, _INT, _P],
     "hn_tc": [_P, _P, _INT, _P],
     "hn_cc": [_P, _INT, _P, _INT, _P],
     "hn_ktruss": [_P, _P, _P, _INT],
@@ -433,6 +434,24 @@ class BfsTopDown(StaticAlgorithm):
         return out, [stats[i] for i in range(len(srcs))]
 
 
+    def run_batch(self, sources, slots=None, nslots=None, out=None):
+        """Batched BFS (hn_bfs_batch): up to 64 slots in one traversal.
+        Returns (dist[nslots][nV], per-slot stats)."""
+        srcs = np.ascontiguousarray(sources, np.int32)
+        sl = None if slots is None else np.ascontiguousarray(slots, np.int32)
+        if nslots is None:
+            nslots = len(srcs) if sl is None else int(sl.max()) + 1
+        n = self.hornet.nV()
+        if out is None:
+            out = np.empty((nslots, n), np.int32)
+        p, mem = _out_ptr(out)
+        stats = (BfsStats * nslots)()
+        _check(lib().hn_bfs_batch(self.hornet.handle, srcs.ctypes.data_as(_P),
+                                  None if sl is None else sl.ctypes.data_as(_P),
+                                  len(srcs), nslots, p, mem, stats))
+        return out, [stats[i] for i in range(nslots)]
+
+
 class BfsDirectionOptimizing(BfsTopDown):
     """Direction-optimising BFS (hornetsnest BottomUpBFS counterpart): same
     distances as BfsTopDown, fewer edges read on large frontiers."""
@@ -649,4 +668,16 @@ def hornet_from_device_csr(csr: DeviceCSR, device: int = 0) -> Hornet:
     _check(lib().hn_graph_create_csr(csr.nV, csr.nE, ctypes.c_void_p(csr.off_ptr),
                                      ctypes.c_void_p(csr.adj_ptr), HN_CSR_SORTED, HN_MEM_DEVICE,
                                      device, ctypes.byref(h._h)))
+    return h
+
+
+def hornet_from_device_arrays(nV: int, nE: int, off, adj, device: int = 0) -> Hornet:
+    """Build a Hornet from caller-owned device arrays (torch int32 tensors:
+    sorted CSR offsets[nV+1] and edges[nE]); the arrays are copied."""
+    h = Hornet.__new__(Hornet)
+    h._h = ctypes.c_void_p()
+    h._device = device
+    _check(lib().hn_graph_create_csr(nV, nE, ctypes.c_void_p(off.data_ptr()),
+                                     ctypes.c_void_p(adj.data_ptr()), HN_CSR_SORTED,
+                                     HN_MEM_DEVICE, device, ctypes.byref(h._h)))
     return h

@@ -1,0 +1,72 @@
+"""Many graphs, one launch: a batch of independent graphs of uneven size held
+as one Hornet (their disjoint union, vertex ids shifted by each graph's
+base), traversed together by the batched BFS and counted together by
+triangle counting.
+
+The reference runs one StaticAlgorithm per graph and per source
+(hornetsnest/src/Static/BreadthFirstSearch/TopDown.cu:88-106,
+hornetsnest/src/Static/TriangleCounting/triangle2.cu:158-171); a batch gives
+the same per-graph results:
+
+* BFS: source j of every graph goes to slot j, so one hn_bfs_batch call
+  with `sources_per_graph` slots computes every (graph, source) pair; the
+  graphs are disjoint, so a slot's distances inside graph i are graph i's
+  own BFS from its source j.
+* Triangles: the union's per-vertex counts summed over each graph's
+  vertex range (every triangle lies inside one graph and is credited to
+  each of its three vertices, hence the division by 3).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import HN_MEM_DEVICE, Hornet, _check, _P, lib
+
+
+class GraphBatch:
+    """A batch of graphs as one Hornet.  `bases[i]` is the first vertex id of
+    graph i in the union; `sizes[i]` its vertex count."""
+
+    def __init__(self, hornet: Hornet, bases, sizes):
+        self.hornet = hornet
+        self.bases = np.ascontiguousarray(bases, np.int64)
+        self.sizes = np.ascontiguousarray(sizes, np.int64)
+        assert len(self.bases) == len(self.sizes)
+        assert int(self.bases[-1] + self.sizes[-1]) == hornet.nV()
+
+    @property
+    def n_graphs(self) -> int:
+        return len(self.sizes)
+
+    def bfs(self, local_sources, out):
+        """local_sources: int[n_graphs][k] vertex ids local to each graph
+        (k <= 64).  out: device int32 tensor [k][nV] (the union's ids);
+        graph i's distances from its source j are out[j, bases[i]:bases[i]+sizes[i]].
+        Returns the per-slot statistics."""
+        from . import BfsStats
+        ls = np.ascontiguousarray(local_sources, np.int64)
+        k = ls.shape[1]
+        if (ls < 0).any() or (ls >= self.sizes[:, None]).any():
+            raise ValueError("source outside its graph")
+        srcs = (ls + self.bases[:, None]).astype(np.int32).ravel()
+        slots = np.tile(np.arange(k, dtype=np.int32), self.n_graphs)
+        stats = (BfsStats * k)()
+        _check(lib().hn_bfs_batch(self.hornet.handle, srcs.ctypes.data_as(_P),
+                                  slots.ctypes.data_as(_P), len(srcs), k,
+                                  ctypes.c_void_p(out.data_ptr()), HN_MEM_DEVICE, stats))
+        return [stats[i] for i in range(k)]
+
+    def triangles(self, per_vertex):
+        """Per-graph triangle counts (device int64 tensor [n_graphs]);
+        per_vertex is a device int64 scratch tensor [nV]."""
+        import torch
+        total = ctypes.c_uint64()
+        _check(lib().hn_tc(self.hornet.handle, ctypes.c_void_p(per_vertex.data_ptr()),
+                           HN_MEM_DEVICE, ctypes.byref(total)))
+        csum = torch.cumsum(per_vertex, 0)
+        ends = torch.as_tensor(self.bases + self.sizes - 1, device=per_vertex.device)
+        at_end = csum[ends]
+        prev = torch.cat([at_end.new_zeros(1), at_end[:-1]])
+        return (at_end - prev) // 3, total.value

@@ -427,6 +427,8 @@ void free_graph_object(hn_graph* g) {
     for (auto& p : g->scratch) p.release(g->stream);
     free_bfs_graph(g->bfs);
     g->bfs = nullptr;
+    free_ms_graph(g->ms);
+    g->ms = nullptr;
     if (g->vtab) cudaFreeAsync(g->vtab, g->stream);
     if (g->pool) cudaFreeAsync(g->pool, g->stream);
     if (g->stream) cudaStreamSynchronize(g->stream);

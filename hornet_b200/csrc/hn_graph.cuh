@@ -88,6 +88,8 @@ struct DeviceInfo {
 
 struct BfsGraph;
 void free_bfs_graph(BfsGraph* bg);
+struct MsGraph;
+void free_ms_graph(MsGraph* mg);
 
 }  // namespace hn
 
@@ -140,6 +142,7 @@ struct hn_graph {
 
     hn::Persist scratch[8];               // reusable device scratch
     hn::BfsGraph* bfs = nullptr;          // instantiated BFS CUDA graph
+    hn::MsGraph* ms = nullptr;            // instantiated batched-BFS CUDA graph
 };
 
 struct hn_batch {

@@ -179,6 +179,20 @@ int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k,
 int hn_bfs_do(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist,
               int mem, hn_bfs_stats_t* stats);
 
+/* Batched BFS: up to 64 BFS "slots" traversed together, one 64-bit mask
+ * per vertex, each edge read once per level for all slots on it.  Source j
+ * seeds slot slots[j] (slots NULL: slot j, k <= nslots); a slot seeded by
+ * several sources gets the distance to the nearest of them, which on a
+ * disjoint union of graphs with one source per graph per slot is each
+ * graph's own BFS.  dist is int32[nslots][nV] row-major (INT32_MAX when
+ * unreachable); slot_stats (may be NULL) has nslots entries.  With one
+ * source per slot the result equals hn_bfs_multi on the same sources.
+ * Batches the reference's per-source BfsTopDown::run
+ * (hornetsnest/src/Static/BreadthFirstSearch/TopDown.cu:88-106). */
+int hn_bfs_batch(hn_graph_t* g, const int32_t* sources, const int32_t* slots,
+                 int32_t k, int32_t nslots, int32_t* dist, int mem,
+                 hn_bfs_stats_t* slot_stats);
+
 /* TriangleCounting2::init/run/countTriangles
  * (hornetsnest/src/Static/TriangleCounting/triangle2.cu:130-171) on the
  * graph's undirected adjacency, each triangle counted once via the

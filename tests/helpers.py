@@ -49,3 +49,18 @@ def sample_existing_edges(g: O.Csr, k: int, seed: int):
     s, d = s[mask], d[mask]
     idx = rng.choice(len(s), size=min(k, len(s)), replace=False)
     return np.concatenate([s[idx], d[idx]]), np.concatenate([d[idx], s[idx]])
+
+
+def disjoint_union(graphs):
+    """One CSR holding `graphs` side by side (vertex ids shifted by the
+    running vertex count).  Returns (union, first vertex id of each graph)."""
+    offs, adjs, base = [np.zeros(1, np.int64)], [], []
+    nv = 0
+    ne = 0
+    for g in graphs:
+        base.append(nv)
+        offs.append(g.off[1:] + ne)
+        adjs.append(g.adj + nv)
+        nv += g.nV
+        ne += g.nE
+    return O.Csr(np.concatenate(offs), np.concatenate(adjs).astype(np.int32)), np.array(base)
