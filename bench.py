@@ -369,7 +369,11 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale):
     for _ in range(2):
         tc.run()
     reps = 3
-    t = event_time(stream, lambda: [tc.run() for _ in range(reps)]) / reps
+    clk = ClockSampler(dev)
+    clk.start()
+    tc_reps = [event_time(stream, tc.run) for _ in range(reps)]
+    tc_clocks = clk.stop()
+    t = statistics.median(tc_reps)
     H.profile_enable(True)
     tc.run()
     rep = H.profile_report()
@@ -387,7 +391,8 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale):
                            f"R-MAT scale {scale} TC")
     also["tc"] = {"metric": "TC edges/s", "value": round(m_plus / t, 1), "unit": "edges/s",
                   "triangles": int(tc.countTriangles()), "ms": round(t * 1e3, 3),
-                  "roofline": troof, "kernels_ms": {k: round(v["ms"], 3) for k, v in rep.items()}}
+                  "roofline": troof, "kernels_ms": {k: round(v["ms"], 3) for k, v in rep.items()},
+                  "rep_ms": [round(x * 1e3, 2) for x in tc_reps], "clocks": tc_clocks}
     # connected components
     cc = H.CC(h)
     lab = torch.empty(nV, dtype=torch.int32, device=f"cuda:{dev}")

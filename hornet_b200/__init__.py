@@ -104,6 +104,8 @@ _SIGNATURES = {
     "hn_bfs_do": [_P, _P, _I32, _P, _INT, _P],
     "hn_bfs_batch": [_P, _P, _P, _I32, _I32, _P, _INT, _P],
     "hn_tc": [_P, _P, _INT, _P],
+    "hn_tc_local": [_P, _P, _I32, _P, _INT],
+    "hn_update_coalesced": [_P, _I64, _P, _P, _P, _INT, _P, _P],
     "hn_cc": [_P, _INT, _P, _INT, _P],
     "hn_ktruss": [_P, _P, _P, _INT],
     "hn_for_all_edges_count": [_P, _P, _I32, _INT, _INT, _P],
@@ -303,6 +305,27 @@ class Hornet:
 
     get_csr = getCSR
 
+    def update_coalesced(self, src, dst, ops) -> Tuple[int, int]:
+        """A run of insert/erase batches applied as one (hn_update_coalesced):
+        ops[i] != 0 inserts edge i, 0 erases it; the last entry of an edge
+        decides.  Host numpy arrays or device tensors (all three alike).
+        Returns (inserted, erased)."""
+        ins, era = ctypes.c_int64(), ctypes.c_int64()
+        if _is_device(src):
+            _check(lib().hn_update_coalesced(self._h, int(src.numel()),
+                                             ctypes.c_void_p(src.data_ptr()),
+                                             ctypes.c_void_p(dst.data_ptr()),
+                                             ctypes.c_void_p(ops.data_ptr()), HN_MEM_DEVICE,
+                                             ctypes.byref(ins), ctypes.byref(era)))
+        else:
+            s_ = np.ascontiguousarray(src, np.int32)
+            d_ = np.ascontiguousarray(dst, np.int32)
+            o_ = np.ascontiguousarray(ops, np.uint8)
+            _check(lib().hn_update_coalesced(self._h, len(s_), s_.ctypes.data_as(_P),
+                                             d_.ctypes.data_as(_P), o_.ctypes.data_as(_P),
+                                             HN_MEM_HOST, ctypes.byref(ins), ctypes.byref(era)))
+        return ins.value, era.value
+
     def degrees(self):
         d = np.empty(self.nV(), np.int32)
         _check(lib().hn_graph_degrees(self._h, d.ctypes.data_as(_P), HN_MEM_HOST))
@@ -501,6 +524,21 @@ class TriangleCounting2(StaticAlgorithm):
 
     def countTriangles(self) -> int:
         return self._total
+
+    def local(self, seeds, out=None):
+        """Triangles containing each seed vertex (hn_tc_local).  seeds: host
+        int array, or a device int32 tensor (then `out`, a device int64
+        tensor, receives the counts)."""
+        if _is_device(seeds):
+            _check(lib().hn_tc_local(self.hornet.handle, ctypes.c_void_p(seeds.data_ptr()),
+                                     int(seeds.numel()), ctypes.c_void_p(out.data_ptr()),
+                                     HN_MEM_DEVICE))
+            return out
+        sd = np.ascontiguousarray(seeds, np.int32)
+        res = np.empty(len(sd), np.uint64)
+        _check(lib().hn_tc_local(self.hornet.handle, sd.ctypes.data_as(_P), len(sd),
+                                 res.ctypes.data_as(_P), HN_MEM_HOST))
+        return res
 
     def copyTCToHost(self):
         if self._per_vertex is None:

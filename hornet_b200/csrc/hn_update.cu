@@ -438,6 +438,46 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     HN_CUDA(cudaStreamSynchronize(s));
 }
 
+// Net effect of a mixed run of update batches: after a stable sort of
+// the packed keys (ops carried as values), the last entry of each key's run
+// holds the op that decides the edge's final presence.  Packed scan value:
+// (erase << 32) | insert.
+__global__ void k_net_mark(const unsigned long long* __restrict__ keys,
+                           const unsigned char* __restrict__ ops, long long n,
+                           unsigned long long* __restrict__ val) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const bool last = i == n - 1 || keys[i + 1] != keys[i];
+        const unsigned long long ins = last && ops[i] != 0;
+        const unsigned long long del = last && ops[i] == 0;
+        val[i] = (del << 32) | ins;
+    }
+}
+
+__global__ void k_net_split(const unsigned long long* __restrict__ keys,
+                            const unsigned long long* __restrict__ val,
+                            const unsigned long long* __restrict__ scan, long long n, int L,
+                            int32_t* ins_src, int32_t* ins_dst, int32_t* del_src,
+                            int32_t* del_dst, long long* totals) {
+    const unsigned long long mask = (1ull << L) - 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long v = val[i], at = scan[i];
+        const int32_t u = (int32_t)(keys[i] >> L), w = (int32_t)(keys[i] & mask);
+        if (v & 0xFFFFFFFFull) {
+            ins_src[at & 0xFFFFFFFFull] = u;
+            ins_dst[at & 0xFFFFFFFFull] = w;
+        } else if (v >> 32) {
+            del_src[at >> 32] = u;
+            del_dst[at >> 32] = w;
+        }
+        if (i == n - 1) {
+            totals[0] = (long long)((at + v) & 0xFFFFFFFFull);
+            totals[1] = (long long)((at + v) >> 32);
+        }
+    }
+}
+
 }  // namespace
 }  // namespace hn
 
@@ -526,6 +566,92 @@ int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
     HN_REQUIRE((flags & ~HN_DEDUP_BATCH) == 0, "unknown flags");
     HN_CUDA(cudaSetDevice(g->device));
     run_update(g, b, flags, false, applied);
+    HN_API_END
+}
+
+int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t* dst,
+                        const uint8_t* ops, int mem, int64_t* inserted, int64_t* erased) {
+    HN_API_BEGIN
+    HN_REQUIRE(g, "graph is null");
+    HN_REQUIRE(n >= 0 && n <= 0x7FFFFFFF, "batch size must be in [0, 2^31)");
+    HN_REQUIRE(n == 0 || (src && dst && ops), "null batch arrays");
+    HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    if (inserted) *inserted = 0;
+    if (erased) *erased = 0;
+    if (n == 0) return HN_OK;
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    const int L = g->key_bits;
+    DevBuf<int32_t> hs, hd;
+    DevBuf<unsigned char> hops;
+    const int32_t* d_src = src;
+    const int32_t* d_dst = dst;
+    const unsigned char* d_ops = ops;
+    if (mem == HN_MEM_HOST) {
+        hs.alloc((size_t)n, s);
+        hd.alloc((size_t)n, s);
+        hops.alloc((size_t)n, s);
+        HN_CUDA(cudaMemcpyAsync(hs.get(), src, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+        HN_CUDA(cudaMemcpyAsync(hd.get(), dst, sizeof(int32_t) * n, cudaMemcpyHostToDevice, s));
+        HN_CUDA(cudaMemcpyAsync(hops.get(), ops, (size_t)n, cudaMemcpyHostToDevice, s));
+        d_src = hs.get();
+        d_dst = hd.get();
+        d_ops = hops.get();
+    }
+    AllocState* st = g->alloc;
+    DevBuf<unsigned long long> keys((size_t)n, s), keys2((size_t)n, s);
+    DevBuf<unsigned char> ops2((size_t)n, s), ops1((size_t)n, s);
+    HN_CUDA(cudaMemsetAsync(st, 0, sizeof(AllocState), s));
+    HN_LAUNCH(k_pack, grid_for(g, n, kB), kB, 0, s, d_src, d_dst, n, g->nV, L, keys.get(), st);
+    HN_CUDA(cudaMemcpyAsync(ops1.get(), d_ops, (size_t)n, cudaMemcpyDeviceToDevice, s));
+    {
+        // LSD radix sort is stable: equal keys keep their batch order
+        cub::DoubleBuffer<unsigned long long> dk(keys.get(), keys2.get());
+        cub::DoubleBuffer<unsigned char> dv(ops1.get(), ops2.get());
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, (int)n, 0, 2 * L, s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, dk, dv, (int)n, 0, 2 * L, s));
+        count_launch();
+        if (dk.Current() != keys.get()) std::swap(keys.p, keys2.p);
+        if (dv.Current() != ops1.get()) std::swap(ops1.p, ops2.p);
+    }
+    unsigned long long* val = keys2.get();
+    HN_LAUNCH(k_net_mark, grid_for(g, n, kB), kB, 0, s, keys.get(), ops1.get(), n, val);
+    DevBuf<unsigned long long> scan((size_t)n, s);
+    {
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, val, scan.get(), (int)n, s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, val, scan.get(), (int)n, s));
+        count_launch();
+    }
+    hn_batch bi, bd;
+    bi.g = bd.g = g;
+    bi.device = bd.device = g->device;
+    DevBuf<int32_t> is((size_t)n, s), id((size_t)n, s), ds((size_t)n, s), dd((size_t)n, s);
+    HN_LAUNCH(k_net_split, grid_for(g, n, kB), kB, 0, s, keys.get(), val, scan.get(), n, L,
+              is.get(), id.get(), ds.get(), dd.get(), g->d_scalar);
+    HN_CUDA(cudaMemcpyAsync(g->h_scalar, g->d_scalar, 2 * sizeof(long long),
+                            cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaMemcpyAsync(g->h_alloc, st, sizeof(AllocState), cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
+    if (g->h_alloc->error) {
+        HN_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(int), s));
+        throw Error(HN_ERR_INVALID, "batch vertex id outside [0, nV)");
+    }
+    bi.n = g->h_scalar[0];
+    bd.n = g->h_scalar[1];
+    keys.release();
+    keys2.release();
+    scan.release();
+    bd.src = ds.get();
+    bd.dst = dd.get();
+    bi.src = is.get();
+    bi.dst = id.get();
+    // the two sets are disjoint, so their order does not matter
+    run_update(g, &bd, HN_DEDUP_BATCH, false, erased);
+    run_update(g, &bi, HN_DEDUP_BATCH | HN_DEDUP_GRAPH, true, inserted);
     HN_API_END
 }
 

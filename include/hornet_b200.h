@@ -159,6 +159,18 @@ int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied);
  * removed. */
 int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied);
 
+/* A run of update batches applied as one: entry i inserts (ops[i] != 0) or
+ * erases (ops[i] == 0) edge (src[i], dst[i]), the entries in the order the
+ * batches arrived.  On a simple graph the result equals applying the
+ * entries in order with insert(removeBatchDuplicates,
+ * removeGraphDuplicates) and erase(removeBatchDuplicates)
+ * (HornetInsert.i.cuh:12-27, HornetDelete.i.cuh:12-37): the last entry of
+ * each edge decides its presence.  The net erase set is applied, then the
+ * net insert set.  src/dst/ops are all in `mem`.  *inserted / *erased
+ * (may be NULL) receive the edges actually added and removed. */
+int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t* dst,
+                        const uint8_t* ops, int mem, int64_t* inserted, int64_t* erased);
+
 /* ---- algorithms (hornetsnest StaticAlgorithm subclasses) -------------- */
 
 /* BfsTopDown: set_parameters(src) + run()
@@ -200,6 +212,14 @@ int hn_bfs_batch(hn_graph_t* g, const int32_t* sources, const int32_t* slots,
  * per_vertex (may be NULL): uint64[nV], triangles containing each vertex.
  * per_vertex uses `mem`; *total is always host. */
 int hn_tc(hn_graph_t* g, uint64_t* per_vertex, int mem, uint64_t* total);
+
+/* Local triangle counts: counts[i] = number of triangles containing
+ * seeds[i] — TriangleCounting2's per-vertex count
+ * (hornetsnest/src/Static/TriangleCounting/triangle2.cu:30-59) for the
+ * seeds only, without counting the rest of the graph.  The graph must be
+ * simple (no self loops or repeated edges).  seeds and counts are both in
+ * `mem`; counts is uint64[k]. */
+int hn_tc_local(hn_graph_t* g, const int32_t* seeds, int32_t k, uint64_t* counts, int mem);
 
 /* CC::run (hornetsnest/src/Static/ConnectedComponents/CC.cu:133-156).
  * mode HN_CC_MIN_ID or HN_CC_REFERENCE.  labels: int32[nV];

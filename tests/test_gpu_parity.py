@@ -323,3 +323,25 @@ def test_config_plain_small_end_to_end():
     np.testing.assert_array_equal(H.CC(h).run(), O.cc_min_label(g)[0])
     if O.ref_available():
         np.testing.assert_array_equal(bfs.distances, O.ref_bfs(g, [0])[0])
+
+
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_tc_local(name):
+    """Triangles containing each seed == TriangleCounting2's per-vertex
+    counts (oracle) at those seeds; repeated seeds, isolated seeds, hubs."""
+    g = GRAPHS[name]()
+    h = build(g)
+    _, pv = O.tc(g, per_vertex=True)
+    deg = np.diff(g.off)
+    rng = np.random.default_rng(8)
+    seeds = np.concatenate([rng.integers(0, g.nV, 1000), [int(np.argmax(deg))] * 3,
+                            np.nonzero(deg == 0)[0][:5]]).astype(np.int32)
+    tc = H.TriangleCounting2(h)
+    np.testing.assert_array_equal(tc.local(seeds), pv[seeds])
+    import torch
+    sd = torch.from_numpy(seeds).cuda()
+    out = torch.empty(len(seeds), dtype=torch.int64, device="cuda")
+    tc.local(sd, out)
+    np.testing.assert_array_equal(out.cpu().numpy().astype(np.uint64), pv[seeds])
+    with pytest.raises(H.HornetError):
+        tc.local(np.array([g.nV], np.int32))
