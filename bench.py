@@ -752,24 +752,28 @@ def bench_serve(args, H, dev, rank, world):
                 if r.kind in S.QUERY_KINDS]
         row = {"rate_rps": rate if rate > 0 else "saturation"}
         res = {}
-        for batched in (False, True):
+        for mode in ("per_request", "per_request_do", "batched"):
             h = H.hornet_from_device_arrays(nV, nE, off_d, adj_d, device=dev)
-            srv = S.Server(h, batched=batched)
+            srv = S.Server(h, batched=mode == "batched",
+                           single_bfs="do" if mode != "per_request" else "td")
             srv.run(warm)                       # CUDA graphs built, read-only
             srv.calls, srv.split_for_memory = 0, 0
             srv.groups = {k: 0 for k in srv.groups}
+            srv.service_s = {k: 0.0 for k in srv.service_s}
             rep = srv.run(reqs)
-            res[batched] = rep.results
-            row["batched" if batched else "per_request"] = rep.summary()
+            res[mode] = rep.results
+            row[mode] = rep.summary()
             del srv, h
             gc.collect()
-        same = S.same_results(res[False], res[True])
+        same = S.same_results(res["per_request"], res["batched"]) and \
+            S.same_results(res["per_request"], res["per_request_do"])
         identical &= same
         row["results_identical"] = same
-        pr, bt = row["per_request"], row["batched"]
+        pr, pd, bt = row["per_request"], row["per_request_do"], row["batched"]
         row["throughput_x"] = round(bt["throughput_rps"] / pr["throughput_rps"], 2)
-        row["p99_ms"] = {"per_request": pr["latency_ms"]["all"]["p99"],
-                         "batched": bt["latency_ms"]["all"]["p99"]}
+        row["throughput_x_vs_per_request_do"] = round(bt["throughput_rps"] / pd["throughput_rps"], 2)
+        row["p99_ms"] = {m: row[m]["latency_ms"]["all"]["p99"]
+                         for m in ("per_request", "per_request_do", "batched")}
         table.append(row)
     sat = [r for r in table if r["rate_rps"] == "saturation"]
     head = sat[0] if sat else table[-1]

@@ -106,6 +106,10 @@ _SIGNATURES = {
     "hn_tc": [_P, _P, _INT, _P],
     "hn_tc_local": [_P, _P, _I32, _P, _INT],
     "hn_update_coalesced": [_P, _I64, _P, _P, _P, _INT, _P, _P],
+    "hn_tune_set": [ctypes.c_char_p, _I64],
+    "hn_tune_get": [ctypes.c_char_p, _P],
+    "hn_tune_reset": [],
+    "hn_tune_name": [_I32],
     "hn_cc": [_P, _INT, _P, _INT, _P],
     "hn_ktruss": [_P, _P, _P, _INT],
     "hn_for_all_edges_count": [_P, _P, _I32, _INT, _INT, _P],
@@ -121,7 +125,8 @@ _SIGNATURES = {
     "hn_graph_write_bin": [_P, ctypes.c_char_p],
     "hn_graph_read_bin": [ctypes.c_char_p, _INT, _P],
 }
-_RESTYPES = {"hn_last_error_string": ctypes.c_char_p, "hn_kernel_launches": _I64}
+_RESTYPES = {"hn_last_error_string": ctypes.c_char_p, "hn_kernel_launches": _I64,
+             "hn_tune_name": ctypes.c_char_p}
 
 _lib = None
 
@@ -719,3 +724,28 @@ def hornet_from_device_arrays(nV: int, nE: int, off, adj, device: int = 0) -> Ho
                                      ctypes.c_void_p(adj.data_ptr()), HN_CSR_SORTED,
                                      HN_MEM_DEVICE, device, ctypes.byref(h._h)))
     return h
+
+
+def tune_names():
+    """Names of the tuning knobs (hn_tune_name)."""
+    out, i = [], 0
+    while True:
+        n = lib().hn_tune_name(i)
+        if not n:
+            return out
+        out.append(n.decode())
+        i += 1
+
+
+def tune_get(name: str) -> int:
+    v = ctypes.c_int64()
+    _check(lib().hn_tune_get(name.encode(), ctypes.byref(v)))
+    return v.value
+
+
+def tune_set(name: str, value: int) -> None:
+    _check(lib().hn_tune_set(name.encode(), int(value)))
+
+
+def tune_reset() -> None:
+    _check(lib().hn_tune_reset())

@@ -68,6 +68,8 @@ struct BfsState {
     int pad;
     long long m_total;           // edges of the graph
     long long edges_visited;     // sum of degrees of vertices reached so far
+    int alpha;                   // direction-optimising switch thresholds
+    int beta;
 };
 
 struct BfsGraph {
@@ -82,6 +84,7 @@ struct BfsGraph {
     unsigned* bitmap = nullptr;
     cudaGraph_t graph[2] = {nullptr, nullptr};      // [0] top-down, [1] direction-optimising
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    unsigned grid = 0;                              // level-kernel CTAs baked in
 };
 
 namespace {
@@ -346,14 +349,15 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
             st->level = level + 1;
             if (DO) {
                 // Beamer's switch: to bottom-up when the next frontier's edges
-                // exceed 1/14 of the unexplored edges, back to top-down when
-                // the frontier falls below nV/24 vertices and is shrinking
+                // exceed 1/alpha of the unexplored edges (alpha = 14 by
+                // default), back to top-down when the frontier falls below
+                // nV/beta vertices (beta = 24) and is shrinking
                 st->edges_visited += (long long)mf;
                 long long mu = st->m_total - st->edges_visited;
                 if (st->mode == 0) {
-                    if ((long long)mf * 14 > mu) st->mode = 1;
+                    if ((long long)mf * st->alpha > mu) st->mode = 1;
                 } else {
-                    if ((long long)nn * 24 < st->nV && nn < (unsigned)nq) st->mode = 0;
+                    if ((long long)nn * st->beta < st->nV && nn < (unsigned)nq) st->mode = 0;
                 }
             }
             cudaGraphSetConditional(cond, (nn > 0 && level < st->nV) ? 1u : 0u);
@@ -400,7 +404,7 @@ void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
             void* args[] = {&bg.state, &handle};
             cudaKernelNodeParams p = {};
             p.func = variant ? (void*)k_bfs_level<true> : (void*)k_bfs_level<false>;
-            p.gridDim = dim3((unsigned)g->info.sms * 4);
+            p.gridDim = dim3(bg.grid);
             p.blockDim = dim3(kBfsBlock);
             p.kernelParams = args;
             HN_CUDA(cudaGraphAddKernelNode(&body_node, body, nullptr, 0, &p));
@@ -430,15 +434,18 @@ void free_bfs_graph(BfsGraph* bg) {
 namespace {
 
 BfsGraph& bfs_graph_of(hn_graph* g) {
-    // rebuilt when the vertex count changes or the edge count outgrows the
-    // chunk table
-    if (g->bfs && (g->bfs->nV != g->nV || g->nE / kChunk + 4 > g->bfs->nchunk_cap)) {
+    // rebuilt when the vertex count changes, the edge count outgrows the
+    // chunk table or the bfs.ctas_per_sm knob changes the level grid
+    const unsigned grid = (unsigned)(g->info.sms * knob(kKnobBfsCtasPerSm));
+    if (g->bfs && (g->bfs->nV != g->nV || g->nE / kChunk + 4 > g->bfs->nchunk_cap ||
+                   g->bfs->grid != grid)) {
         HN_CUDA(cudaStreamSynchronize(g->stream));
         free_bfs_graph(g->bfs);
         g->bfs = nullptr;
     }
     if (!g->bfs) {
         g->bfs = new BfsGraph();
+        g->bfs->grid = grid;
         try {
             build_bfs_graph(g, *g->bfs);
         } catch (...) {
@@ -482,6 +489,8 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.chunk[1] = bg.chunkbuf + bg.nchunk_cap;
         h.bitmap = bg.bitmap;
         h.m_total = g->nE;
+        h.alpha = (int)knob(kKnobBfsDoAlpha);
+        h.beta = (int)knob(kKnobBfsDoBeta);
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
         // profiling records the whole graph (one init + one expand per
         // level) under the name of its dominant kernel

@@ -31,6 +31,35 @@ static thread_local std::string g_last_error;
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 bool g_profiling = false;
+
+namespace {
+struct KnobDef {
+    const char* name;
+    long long def, lo, hi;
+    bool pow2;   // value must be a power of two
+};
+const KnobDef kKnobs[kNumKnobs] = {
+    {"bfs.ctas_per_sm", 4, 1, 8, false},
+    {"bfs.do_alpha", 14, 1, 1 << 20, false},
+    {"bfs.do_beta", 24, 1, 1 << 20, false},
+    {"msbfs.block", 256, 128, 512, true},
+    {"msbfs.ctas_per_sm", 4, 1, 8, false},
+    {"tc.warp_cap", 512, 32, 512, false},
+    {"tc.chunk", 16, 1, 256, false},
+    {"tc.warp_ctas_per_sm", 8, 1, 16, false},
+};
+std::atomic<long long> g_knob[kNumKnobs] = {
+    {4}, {14}, {24}, {256}, {4}, {512}, {16}, {8}};
+
+int knob_index(const char* name) {
+    if (!name) return -1;
+    for (int i = 0; i < kNumKnobs; i++)
+        if (std::strcmp(name, kKnobs[i].name) == 0) return i;
+    return -1;
+}
+}  // namespace
+
+long long knob(Knob k) { return g_knob[k].load(std::memory_order_relaxed); }
 struct ProfRec {
     std::string name;
     cudaEvent_t a, b;
@@ -511,6 +540,32 @@ extern "C" {
 const char* hn_last_error_string(void) { return g_last_error.c_str(); }
 
 int hn_version(void) { return 10000; }
+
+int hn_tune_set(const char* name, int64_t value) {
+    HN_API_BEGIN
+    int i = knob_index(name);
+    HN_REQUIRE(i >= 0, "unknown tuning knob");
+    const KnobDef& d = kKnobs[i];
+    if (value < d.lo || value > d.hi || (d.pow2 && (value & (value - 1))))
+        throw Error(HN_ERR_INVALID, std::string("value out of range for ") + d.name);
+    g_knob[i].store(value, std::memory_order_relaxed);
+    HN_API_END
+}
+
+int hn_tune_get(const char* name, int64_t* value) {
+    HN_API_BEGIN
+    int i = knob_index(name);
+    HN_REQUIRE(i >= 0 && value, "unknown tuning knob");
+    *value = g_knob[i].load(std::memory_order_relaxed);
+    HN_API_END
+}
+
+int hn_tune_reset(void) {
+    for (int i = 0; i < kNumKnobs; i++) g_knob[i].store(kKnobs[i].def, std::memory_order_relaxed);
+    return HN_OK;
+}
+
+const char* hn_tune_name(int32_t i) { return i >= 0 && i < kNumKnobs ? kKnobs[i].name : nullptr; }
 
 int64_t hn_kernel_launches(void) { return g_launches.load(); }
 

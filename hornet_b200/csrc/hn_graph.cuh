@@ -86,6 +86,20 @@ struct DeviceInfo {
     int max_threads_per_sm = 2048;
 };
 
+// Tuning knobs (hn_tune_set / hn_tune_get); read on the host at launch.
+enum Knob {
+    kKnobBfsCtasPerSm,
+    kKnobBfsDoAlpha,
+    kKnobBfsDoBeta,
+    kKnobMsBlock,
+    kKnobMsCtasPerSm,
+    kKnobTcWarpCap,
+    kKnobTcChunk,
+    kKnobTcWarpCtasPerSm,
+    kNumKnobs
+};
+long long knob(Knob k);
+
 struct BfsGraph;
 void free_bfs_graph(BfsGraph* bg);
 struct MsGraph;

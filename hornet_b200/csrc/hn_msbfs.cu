@@ -26,9 +26,8 @@
 
 namespace hn {
 
-constexpr int kMsBlock = 256;
-constexpr int kMsIpt = 8;
-constexpr int kMsChunk = kMsBlock * kMsIpt;
+constexpr int kSeedBlock = 256;       // the single seeding CTA
+constexpr int kMsChunk = 2048;        // edges per chunk (block x items per thread)
 constexpr int kMaxSlots = 64;
 
 struct MsState {
@@ -71,6 +70,8 @@ struct MsGraph {
     unsigned long long* h_stat = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    int block = 256;      // msbfs.block knob baked into the graph
+    unsigned grid = 0;    // msbfs.ctas_per_sm x SMs
 };
 
 namespace {
@@ -83,7 +84,8 @@ __device__ __forceinline__ void ms_mark_chunks(int32_t* chunk, unsigned off, uns
 
 // CTA-wide exclusive scan of a packed (degree << 32 | count) value and one
 // atomic on `counter`; returns this thread's (slot, edge offset) base.
-// Must be called by all threads of a kMsBlock CTA.
+// Must be called by all threads of a BLOCK-thread CTA.
+template <int BLOCK>
 __device__ __forceinline__ unsigned long long ms_cta_reserve(unsigned long long mine,
                                                              unsigned long long* counter,
                                                              unsigned long long* s_wsum,
@@ -98,14 +100,14 @@ __device__ __forceinline__ unsigned long long ms_cta_reserve(unsigned long long 
     if (lane == 31) s_wsum[warp] = incl;
     __syncthreads();
     if (threadIdx.x < 32) {
-        unsigned long long v = threadIdx.x < kMsBlock / 32 ? s_wsum[threadIdx.x] : 0ull;
+        unsigned long long v = threadIdx.x < BLOCK / 32 ? s_wsum[threadIdx.x] : 0ull;
         unsigned long long vi = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             unsigned long long x = __shfl_up_sync(0xFFFFFFFFu, vi, o);
             if (lane >= o) vi += x;
         }
-        if (threadIdx.x < kMsBlock / 32) s_wsum[threadIdx.x] = vi - v;
+        if (threadIdx.x < BLOCK / 32) s_wsum[threadIdx.x] = vi - v;
         unsigned long long tot = __shfl_sync(0xFFFFFFFFu, vi, 31);
         if (threadIdx.x == 0) *s_base = tot ? atomicAdd(counter, tot) : 0ull;
     }
@@ -132,11 +134,11 @@ __global__ void k_ms_fill(MsState* st) {
 }
 
 // one CTA: seed every source, build the first frontier
-__global__ void __launch_bounds__(kMsBlock) k_ms_seed(MsState* st) {
-    __shared__ unsigned long long s_wsum[kMsBlock / 32];
+__global__ void __launch_bounds__(kSeedBlock) k_ms_seed(MsState* st) {
+    __shared__ unsigned long long s_wsum[kSeedBlock / 32];
     __shared__ unsigned long long s_base;
     __shared__ unsigned long long s_stat[2 * kMaxSlots];
-    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += kMsBlock) s_stat[i] = 0;
+    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += kSeedBlock) s_stat[i] = 0;
     if (threadIdx.x == 0) {
         st->cnt[0] = 0;
         st->cnt[1] = 0;
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_seed(MsState* st) {
     }
     __syncthreads();
     const int nV = st->nV;
-    for (int j0 = 0; j0 < st->nsrc; j0 += kMsBlock) {
+    for (int j0 = 0; j0 < st->nsrc; j0 += kSeedBlock) {
         int j = j0 + threadIdx.x;
         bool first = false;
         int v = 0;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_seed(MsState* st) {
         }
         bool q = first && r.deg > 0;
         unsigned long long mine = q ? (((unsigned long long)r.deg << 32) | 1ull) : 0ull;
-        unsigned long long at = ms_cta_reserve(mine, &st->cnt[0], s_wsum, &s_base);
+        unsigned long long at = ms_cta_reserve<kSeedBlock>(mine, &st->cnt[0], s_wsum, &s_base);
         if (q) {
             int pos = (int)(at & 0xFFFFFFFFull);
             unsigned off = (unsigned)(at >> 32);
@@ -185,17 +187,19 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_seed(MsState* st) {
         unsigned long long c = st->cnt[0];
         st->qoff[0][c & 0xFFFFFFFFull] = (unsigned)(c >> 32);
     }
-    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += kMsBlock)
+    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += kSeedBlock)
         if (s_stat[i]) atomicAdd(st->stat + i, s_stat[i]);
 }
 
 // push: OR frontier masks along the frontier's edges
-__global__ void __launch_bounds__(kMsBlock, 4) k_ms_push(MsState* st) {
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_ms_push(MsState* st) {
+    constexpr int IPT = kMsChunk / BLOCK;
     __shared__ unsigned s_start[kMsChunk + 2];
     __shared__ long long s_base[kMsChunk + 1];
     __shared__ unsigned long long s_front[kMsChunk + 1];
     __shared__ int s_nw;
-    __shared__ unsigned long long s_wsum[kMsBlock / 32];
+    __shared__ unsigned long long s_wsum[BLOCK / 32];
     __shared__ unsigned long long s_cb;
     const int it = st->level - 1;
     const unsigned long long cin = st->cnt[it % 3];
@@ -218,7 +222,7 @@ __global__ void __launch_bounds__(kMsBlock, 4) k_ms_push(MsState* st) {
         const int s0 = chunk[c];
         const int s1 = c + 1 < nchunks ? chunk[c + 1] : nq - 1;
         const int nw = s1 - s0 + 1;
-        for (int j = threadIdx.x; j <= nw; j += kMsBlock) {
+        for (int j = threadIdx.x; j <= nw; j += BLOCK) {
             int s = s0 + j;
             unsigned so = qoff[s];
             s_start[j] = so;
@@ -229,9 +233,9 @@ __global__ void __launch_bounds__(kMsBlock, 4) k_ms_push(MsState* st) {
         }
         if (threadIdx.x == 0) s_nw = nw;
         __syncthreads();
-        const unsigned a = e0 + threadIdx.x * kMsIpt;
-        const unsigned b = a + kMsIpt < e1 ? a + kMsIpt : e1;
-        int touched_here[kMsIpt];
+        const unsigned a = e0 + threadIdx.x * IPT;
+        const unsigned b = a + IPT < e1 ? a + IPT : e1;
+        int touched_here[IPT];
         int nt = 0;
         if (a < b) {
             int lo = 0, hi = s_nw;
@@ -240,10 +244,10 @@ __global__ void __launch_bounds__(kMsBlock, 4) k_ms_push(MsState* st) {
                 if (s_start[mid] <= a) lo = mid; else hi = mid;
             }
             int j = lo;
-            int w[kMsIpt];
-            unsigned long long fm[kMsIpt];
+            int w[IPT];
+            unsigned long long fm[IPT];
 #pragma unroll
-            for (int k = 0; k < kMsIpt; k++) {
+            for (int k = 0; k < IPT; k++) {
                 unsigned e = a + k;
                 w[k] = -1;
                 fm[k] = 0;
@@ -253,11 +257,11 @@ __global__ void __launch_bounds__(kMsBlock, 4) k_ms_push(MsState* st) {
                     fm[k] = s_front[j];
                 }
             }
-            unsigned long long sv[kMsIpt];
+            unsigned long long sv[IPT];
 #pragma unroll
-            for (int k = 0; k < kMsIpt; k++) sv[k] = w[k] >= 0 ? __ldca(seen + w[k]) : ~0ull;
+            for (int k = 0; k < IPT; k++) sv[k] = w[k] >= 0 ? __ldca(seen + w[k]) : ~0ull;
 #pragma unroll
-            for (int k = 0; k < kMsIpt; k++) {
+            for (int k = 0; k < IPT; k++) {
                 unsigned long long m = fm[k] & ~sv[k];
                 if (m) {
                     unsigned long long old = atomicOr(nxt + w[k], m);
@@ -265,20 +269,21 @@ __global__ void __launch_bounds__(kMsBlock, 4) k_ms_push(MsState* st) {
                 }
             }
         }
-        unsigned long long at = ms_cta_reserve((unsigned long long)nt, &st->tcnt, s_wsum, &s_cb);
+        unsigned long long at = ms_cta_reserve<BLOCK>((unsigned long long)nt, &st->tcnt, s_wsum, &s_cb);
         int pos = (int)at;
         for (int k = 0; k < nt; k++) st->touched[pos + k] = touched_here[k];
     }
 }
 
 // apply: new bits of every touched vertex; next frontier; clear the old one
-__global__ void __launch_bounds__(kMsBlock) k_ms_apply(MsState* st, cudaGraphConditionalHandle cond) {
-    __shared__ unsigned long long s_wsum[kMsBlock / 32];
+template <int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_ms_apply(MsState* st, cudaGraphConditionalHandle cond) {
+    __shared__ unsigned long long s_wsum[BLOCK / 32];
     __shared__ unsigned long long s_cb;
     __shared__ unsigned long long s_stat[2 * kMaxSlots];
     __shared__ int s_last[kMaxSlots];   // written only with this level's number
-    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += kMsBlock) s_stat[i] = 0;
-    for (int i = threadIdx.x; i < kMaxSlots; i += kMsBlock) s_last[i] = 0;
+    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += BLOCK) s_stat[i] = 0;
+    for (int i = threadIdx.x; i < kMaxSlots; i += BLOCK) s_last[i] = 0;
     __syncthreads();
     const int level = st->level;
     const int it = level - 1;
@@ -317,7 +322,7 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_apply(MsState* st, cudaGraphCon
             q = r.deg > 0;
         }
         unsigned long long mine = q ? (((unsigned long long)r.deg << 32) | 1ull) : 0ull;
-        unsigned long long at = ms_cta_reserve(mine, cout, s_wsum, &s_cb);
+        unsigned long long at = ms_cta_reserve<BLOCK>(mine, cout, s_wsum, &s_cb);
         if (q) {
             int pos = (int)(at & 0xFFFFFFFFull);
             unsigned off = (unsigned)(at >> 32);
@@ -328,9 +333,9 @@ __global__ void __launch_bounds__(kMsBlock) k_ms_apply(MsState* st, cudaGraphCon
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += kMsBlock)
+    for (int i = threadIdx.x; i < 2 * kMaxSlots; i += BLOCK)
         if (s_stat[i]) atomicAdd(st->stat + i, s_stat[i]);
-    for (int i = threadIdx.x; i < kMaxSlots; i += kMsBlock)
+    for (int i = threadIdx.x; i < kMaxSlots; i += BLOCK)
         if (s_last[i]) st->stat[2 * kMaxSlots + i] = (unsigned long long)level;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -377,7 +382,7 @@ void build_ms_graph(hn_graph* g, MsGraph& mg) {
         HN_CUDA(cudaGraphAddKernelNode(&fill, mg.graph, nullptr, 0, &p));
         p.func = (void*)k_ms_seed;
         p.gridDim = dim3(1);
-        p.blockDim = dim3(kMsBlock);
+        p.blockDim = dim3(kSeedBlock);
         HN_CUDA(cudaGraphAddKernelNode(&seed, mg.graph, &fill, 1, &p));
     }
     cudaGraphConditionalHandle handle;
@@ -392,14 +397,16 @@ void build_ms_graph(hn_graph* g, MsGraph& mg) {
     {
         void* args[] = {&mg.state};
         cudaKernelNodeParams p = {};
-        p.func = (void*)k_ms_push;
-        p.gridDim = dim3((unsigned)g->info.sms * 4);
-        p.blockDim = dim3(kMsBlock);
+        p.func = mg.block == 128 ? (void*)k_ms_push<128>
+               : mg.block == 512 ? (void*)k_ms_push<512> : (void*)k_ms_push<256>;
+        p.gridDim = dim3(mg.grid);
+        p.blockDim = dim3(mg.block);
         p.kernelParams = args;
         HN_CUDA(cudaGraphAddKernelNode(&push, body, nullptr, 0, &p));
         void* args2[] = {&mg.state, &handle};
-        p.func = (void*)k_ms_apply;
-        p.gridDim = dim3((unsigned)g->info.sms * 4);
+        p.func = mg.block == 128 ? (void*)k_ms_apply<128>
+               : mg.block == 512 ? (void*)k_ms_apply<512> : (void*)k_ms_apply<256>;
+        p.gridDim = dim3(mg.grid);
         p.kernelParams = args2;
         HN_CUDA(cudaGraphAddKernelNode(&apply, body, &push, 1, &p));
     }
@@ -448,13 +455,18 @@ extern "C" int hn_bfs_batch(hn_graph_t* g, const int32_t* sources, const int32_t
         if (slots && (slots[j] < 0 || slots[j] >= nslots))
             throw Error(HN_ERR_INVALID, "slot outside [0, nslots)");
     }
-    if (g->ms && (g->ms->nV != nV || g->nE / kMsChunk + 4 > g->ms->nchunk_cap)) {
+    const int block = (int)knob(kKnobMsBlock);
+    const unsigned grid = (unsigned)(g->info.sms * knob(kKnobMsCtasPerSm));
+    if (g->ms && (g->ms->nV != nV || g->nE / kMsChunk + 4 > g->ms->nchunk_cap ||
+                  g->ms->block != block || g->ms->grid != grid)) {
         HN_CUDA(cudaStreamSynchronize(s));
         free_ms_graph(g->ms);
         g->ms = nullptr;
     }
     if (!g->ms) {
         g->ms = new MsGraph();
+        g->ms->block = block;
+        g->ms->grid = grid;
         try {
             build_ms_graph(g, *g->ms);
         } catch (...) {

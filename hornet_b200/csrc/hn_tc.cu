@@ -99,10 +99,12 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
 // slot).  Every oriented edge (u,v) is counted by its tail u: the elements
 // of N+(v) are probed against table(u), after N+(v) is narrowed to
 // [min N+(u), max N+(u)] by two binary searches.  The (v, w) pairs of 32
-// candidates v at a time are split into 32 equal contiguous shares, so each
-// lane walks its share sequentially (coalescing-friendly, no per-pair
+// candidates v at a time are dealt to the lanes round-robin (lane l takes
+// pairs l, l+32, ...), so a warp's loads of w read consecutive words of the
+// same list; each lane advances its candidate monotonically (no per-pair
 // search).
-//   k_tc_warp: one warp per vertex with d+(u) <= kWarpCap; vertices handed
+//   k_tc_warp: one warp per vertex with d+(u) <= warp_cap (the tc.warp_cap
+//              knob, at most kWarpCap, the table's capacity); vertices handed
 //              out in chunks by an atomic counter; larger ones are listed;
 //   k_tc_cta:  one CTA per listed vertex, table in dynamic shared memory
 //              (up to kCtaCap entries), binary search of the sorted list in
@@ -112,7 +114,6 @@ constexpr int kTcWarps = 8;
 constexpr int kWarpCap = 512;
 constexpr int kWarpTab = 2 * kWarpCap;
 constexpr int kCtaCap = 16384;
-constexpr int kChunk = 16;
 
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
@@ -148,8 +149,7 @@ struct TcView {
 // against N+(u) (hash table `tab`, or binary search of the sorted global
 // list L when tab == nullptr).  Candidates v are taken 32 at a time; each
 // lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
-// searches, then the warp's pairs are split into 32 equal contiguous
-// shares, so each lane walks its share sequentially with no per-pair search
+// searches, then the group's pairs are dealt round-robin to the lanes
 // (one search over the 33-entry prefix per lane per group).
 template <bool PER_VERTEX>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
@@ -188,24 +188,22 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
         s_v[lane] = v;
         __syncwarp();
         const int T = s_pref[32];
-        // this lane's share of the pairs: [k0, k1)
-        const int k0 = (int)((long long)T * lane / 32);
-        const int k1 = (int)((long long)T * (lane + 1) / 32);
-        if (k0 < k1) {
-            int a = 0, b = 32;   // candidate slot of pair k0
+        if (lane < T) {
+            int a = 0, b = 32;   // candidate slot of pair `lane`
             while (b - a > 1) {
                 int mid = (a + b) >> 1;
-                if (s_pref[mid] <= k0) a = mid; else b = mid;
+                if (s_pref[mid] <= lane) a = mid; else b = mid;
             }
-            int end = s_pref[a + 1];
-            const int32_t* p = g.fwd + s_vb[a] + (k0 - s_pref[a]);
-            for (int k = k0; k < k1; k++) {
+            int start = s_pref[a], end = s_pref[a + 1];
+            const int32_t* base = g.fwd + s_vb[a];
+            for (int k = lane; k < T; k += 32) {
                 while (k >= end) {   // next non-empty candidate
                     a++;
+                    start = end;
                     end = s_pref[a + 1];
-                    p = g.fwd + s_vb[a];
+                    base = g.fwd + s_vb[a];
                 }
-                int w = *p++;
+                int w = base[k - start];
                 bool hit;
                 if (tab) {
                     hit = tab_find(tab, bits, w);
@@ -237,7 +235,7 @@ __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
-          int32_t* __restrict__ big) {
+          int32_t* __restrict__ big, int warp_cap, int chunk) {
     __shared__ int s_tab[kTcWarps][kWarpTab];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
@@ -248,15 +246,15 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
     unsigned long long mine = 0;
     while (true) {
         int u0 = 0;
-        if (lane == 0) u0 = atomicAdd(counters, kChunk);
+        if (lane == 0) u0 = atomicAdd(counters, chunk);
         u0 = __shfl_sync(0xFFFFFFFFu, u0, 0);
         if (u0 >= nV) break;
-        int u1 = u0 + kChunk < nV ? u0 + kChunk : nV;
+        int u1 = u0 + chunk < nV ? u0 + chunk : nV;
         for (int u = u0; u < u1; u++) {
             long long ub = g.offp[u];
             int du = (int)(g.offp[u + 1] - ub);
             if (du == 0) continue;
-            if (du > kWarpCap) {
+            if (du > warp_cap) {
                 if (lane == 0) big[atomicAdd(counters + 1, 1)] = u;
                 continue;
             }
@@ -281,7 +279,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
     }
 }
 
-// Listed vertices (d+(u) > kWarpCap): one CTA each.
+// Listed vertices (d+(u) > warp_cap): one CTA each.
 template <bool PER_VERTEX>
 __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
@@ -357,7 +355,9 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     int* counters = (int*)(g->d_scalar + 1);  // next vertex, big-list size
     HN_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(int), s));
     DevBuf<int32_t> big((size_t)g->nV + 1, s);
-    const long long gw = (long long)g->info.sms * 8;
+    const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
+    const int warp_cap = (int)knob(kKnobTcWarpCap);
+    const int chunk = (int)knob(kKnobTcChunk);
     const size_t dyn = (size_t)2 * kCtaCap * sizeof(int);   // hash table of the CTA path
     static bool attr_set = false;
     if (!attr_set) {
@@ -372,12 +372,12 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     if (d_per_vertex) {
         HN_CUDA(cudaMemsetAsync(d_per_vertex, 0, sizeof(unsigned long long) * g->nV, s));
         HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, view, g->nV, d_per_vertex, d_total,
-                  counters, big.get());
+                  counters, big.get(), warp_cap, chunk);
         HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, view, d_per_vertex, d_total,
                   counters, big.get());
     } else {
         HN_LAUNCH(k_tc_warp<false>, gw, kTcWarps * 32, 0, s, view, g->nV,
-                  (unsigned long long*)nullptr, d_total, counters, big.get());
+                  (unsigned long long*)nullptr, d_total, counters, big.get(), warp_cap, chunk);
         HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, view,
                   (unsigned long long*)nullptr, d_total, counters, big.get());
     }

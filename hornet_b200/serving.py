@@ -7,7 +7,8 @@ set).  The graph stays on the device for the whole run.  Two loops serve the
 same stream:
 
 * the plain per-request loop: one library call per request, in arrival
-  order (hn_insert / hn_erase, hn_bfs, hn_tc_local);
+  order (hn_insert / hn_erase, hn_bfs — or hn_bfs_do with single_bfs="do" —,
+  hn_tc_local);
 * the batched loop, which keeps arrival-order semantics — a query sees
   exactly the updates that arrived before it — while
   - coalescing a run of consecutive update batches into one
@@ -15,8 +16,10 @@ same stream:
     on a simple graph is what applying the batches in order gives),
   - answering a run of consecutive queries together: up to `max_slots` BFS
     sources in one hn_bfs_batch traversal (one slot per request, so every
-    request gets its own single-source distances) and all local-TC seed sets
-    in one hn_tc_local call,
+    request gets its own single-source distances) when the run holds at
+    least `msbfs_min` of them, otherwise one direction-optimising traversal
+    per BFS (hn_bfs_do: the same distances, fewer edges read); all local-TC
+    seed sets in one hn_tc_local call,
   - admitting a coalesced update only while its working memory fits in
     the free device memory (less a reserve); a run that does not fit is split.
 
@@ -75,7 +78,9 @@ class ServeReport:
                 "makespan_s": round(self.makespan_s, 4),
                 "throughput_rps": round(self.throughput_rps, 1), "latency_ms": self.latency_ms,
                 "library_calls": self.calls, "groups": self.groups,
-                "updates_split_for_memory": self.split_for_memory}
+                "updates_split_for_memory": self.split_for_memory,
+                "service_ms": getattr(self, "service_ms", None),
+                "single_bfs": getattr(self, "single_bfs", None)}
 
 
 def _pct(a, q):
@@ -92,10 +97,15 @@ class Server:
 
     def __init__(self, hornet: Hornet, batched: bool = True, max_slots: int = 64,
                  max_update_edges: int = 1 << 24, reserve_bytes: int = 2 << 30,
-                 free_bytes_fn=None):
+                 free_bytes_fn=None, single_bfs: str = "", msbfs_min: int = 4):
         import torch
         self.h = hornet
         self.batched = batched
+        # traversal for a BFS answered alone: "td" (BfsTopDown) or "do"
+        # (direction-optimising, same distances); groups of at least
+        # msbfs_min BFS queries go to one batched traversal
+        self.single_bfs = single_bfs or ("do" if batched else "td")
+        self.msbfs_min = max(2, int(msbfs_min))
         self.max_slots = max(1, min(64, int(max_slots)))
         self.max_update_edges = int(max_update_edges)
         self.reserve = int(reserve_bytes)
@@ -108,6 +118,7 @@ class Server:
         self.calls = 0
         self.split_for_memory = 0
         self.groups = {"update": 0, "bfs": 0, "tc_local": 0}
+        self.service_s = {"update": 0.0, "bfs": 0.0, "tc_local": 0.0}
 
     # ---- library calls ---------------------------------------------------
     def _update_plain(self, r: Request):
@@ -155,14 +166,22 @@ class Server:
         k = len(group)
         srcs = np.array([r.source for r in group], np.int32)
         stats = (BfsStats * k)()
-        if k == 1 and not self.batched:
-            _check(lib().hn_bfs(self.h.handle, int(srcs[0]), ctypes.c_void_p(self.dist.data_ptr()),
-                                HN_MEM_DEVICE, ctypes.byref(stats[0])))
-        else:
+        if k >= self.msbfs_min:
             _check(lib().hn_bfs_batch(self.h.handle, srcs.ctypes.data_as(_P), None, k, k,
                                       ctypes.c_void_p(self.dist.data_ptr()), HN_MEM_DEVICE,
                                       stats))
-        self.calls += 1
+            self.calls += 1
+        else:
+            for j in range(k):
+                row = ctypes.c_void_p(self.dist.data_ptr() + 4 * j * self.nV)
+                if self.single_bfs == "do":
+                    one = srcs[j:j + 1]
+                    _check(lib().hn_bfs_do(self.h.handle, one.ctypes.data_as(_P), 1, row,
+                                           HN_MEM_DEVICE, ctypes.byref(stats[j])))
+                else:
+                    _check(lib().hn_bfs(self.h.handle, int(srcs[j]), row, HN_MEM_DEVICE,
+                                        ctypes.byref(stats[j])))
+                self.calls += 1
         self.groups["bfs"] += 1
         idx = np.concatenate([j * self.nV + np.asarray(r.targets, np.int64)
                               for j, r in enumerate(group)])
@@ -190,6 +209,13 @@ class Server:
         return take_group(pending, self.batched, self.max_slots)
 
     def _execute(self, group: List[Request], results):
+        t0 = time.perf_counter()
+        self._execute_group(group, results)
+        kind = "update" if group[0].kind in UPDATE_KINDS else \
+            ("bfs" if group[0].kind == "bfs" else "tc_local")
+        self.service_s[kind] += time.perf_counter() - t0
+
+    def _execute_group(self, group: List[Request], results):
         if group[0].kind in UPDATE_KINDS:
             if self.batched:
                 self._update_group(group)
@@ -241,9 +267,12 @@ class Server:
                 lat_ms[kind] = {"n": int(len(sel)), "p50": round(_pct(sel, 50) * 1e3, 3),
                                 "p99": round(_pct(sel, 99) * 1e3, 3),
                                 "mean": round(float(sel.mean()) * 1e3, 3)}
-        return ServeReport("batched" if self.batched else "per_request", n, last,
-                           n / last if last > 0 else float("inf"), lat_ms, self.calls,
-                           dict(self.groups), self.split_for_memory, results)
+        rep = ServeReport("batched" if self.batched else "per_request", n, last,
+                          n / last if last > 0 else float("inf"), lat_ms, self.calls,
+                          dict(self.groups), self.split_for_memory, results)
+        rep.service_ms = {k: round(v * 1e3, 2) for k, v in self.service_s.items()}
+        rep.single_bfs = self.single_bfs
+        return rep
 
 
 def take_group(pending: deque, batched: bool, max_slots: int) -> List[Request]:

@@ -88,6 +88,25 @@ int64_t hn_kernel_launches(void);
 int hn_profile_enable(int on);
 int hn_profile_report(char* buf, int64_t len);
 
+/* Tuning knobs (process-wide; read when a call launches, so a change takes
+ * effect on the next call).  An autotuner sets them; the defaults are the
+ * built-in values.  Knobs:
+ *   bfs.ctas_per_sm     CTAs per SM of the BFS level kernel (1..8, 4)
+ *   bfs.do_alpha        direction-optimising switch to bottom-up when the
+ *                       frontier's edges exceed unexplored edges / alpha (14)
+ *   bfs.do_beta         back to top-down below nV / beta frontier vertices (24)
+ *   msbfs.block         batched-BFS block size: 128, 256 or 512 (256)
+ *   msbfs.ctas_per_sm   batched-BFS CTAs per SM (1..8, 4)
+ *   tc.warp_cap         oriented-degree bin boundary between the warp-per-
+ *                       vertex and CTA-per-vertex counting kernels (32..512, 512)
+ *   tc.chunk            vertices handed to a warp per atomic (1..256, 16)
+ *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)
+ * hn_tune_name(i) enumerates the names (NULL past the last one). */
+int hn_tune_set(const char* name, int64_t value);
+int hn_tune_get(const char* name, int64_t* value);
+int hn_tune_reset(void);
+const char* hn_tune_name(int32_t i);
+
 /* ---- graph construction (HornetInit + gpu::Hornet(HornetInit&)) ----------
  * Replaces hornet::HornetInit(nV, nE, offsets, edges)
  * (hornet/include/Core/HornetInitialize/HornetInit.cuh:70-73) and

@@ -104,11 +104,12 @@ def test_serving_batched_equals_plain_equals_oracle(rate):
                            median_edges=300, sigma=1.0, clip=(20, 3000), n_seeds=64)
     ref, g_end = oracle_replay(g, reqs)
     reports = {}
-    for batched in (False, True):
+    for batched, single, msmin in ((False, "td", 4), (False, "do", 4), (True, "do", 2)):
         h = build(g)
-        srv = S.Server(h, batched=batched, max_slots=16, reserve_bytes=0)
+        srv = S.Server(h, batched=batched, max_slots=16, reserve_bytes=0, single_bfs=single,
+                       msbfs_min=msmin)
         rep = srv.run(reqs)
-        assert S.same_results(rep.results, ref), f"batched={batched}"
+        assert S.same_results(rep.results, ref), f"batched={batched} single={single}"
         assert_same_graph(h, g_end)
         reports[batched] = rep
     assert reports[True].calls < reports[False].calls
