@@ -258,6 +258,24 @@ def roofline_entry(H, prefixes, algo_bytes_fn, peak, peak_kind, report, workload
             "peak_kind": peak_kind, "workload": workload}
 
 
+def tuning_setup(args, space, nV, nE, max_degree, run, same):
+    """Knobs for this workload: tuned now (--autotune, then saved) or loaded
+    from a saved entry for this device and workload signature (defaults
+    when there is none)."""
+    import torch
+    from hornet_b200 import autotune as A
+    devname = torch.cuda.get_device_name()
+    sig = A.signature(space, nV, nE, max_degree)
+    path = args.tuned_path or A.DEFAULT_PATH
+    if args.autotune:
+        best, log = A.tune(run, same, A.SPACES[space], reps=3)
+        base, top = log[0]["s"], min(x["s"] for x in log)
+        A.save(devname, sig, best, base / top, path=path)
+        return {"signature": sig, "knobs": best, "tuned_now": True, "trials": len(log),
+                "speedup_vs_default": round(base / top, 3)}
+    return {"signature": sig, "knobs": A.apply_saved(devname, sig, path), "tuned_now": False}
+
+
 def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_kind, barrier,
                  max_over_ranks, sum_over_ranks, scale):
     import torch
@@ -265,6 +283,15 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     sources = pick_sources(deg, 64, seed=2022 + rank)
     out = torch.empty(nV, dtype=torch.int32, device=f"cuda:{dev}")
     bfs = H.BfsTopDown(h)
+    tune8 = torch.empty((8, nV), dtype=torch.int32, device=f"cuda:{dev}")
+
+    def bfs8():
+        for j in range(8):
+            bfs.set_parameters(int(sources[j]))
+            bfs.run(out=tune8[j])
+        return tune8.clone()
+
+    tuning = {"bfs": tuning_setup(args, "bfs", nV, nE, h.max_degree(), bfs8, torch.equal)}
 
     def run_bfs(i):
         bfs.set_parameters(int(sources[i % len(sources)]))
@@ -326,9 +353,17 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
 
     also = {}
     if not args.no_extras and rank == 0:
-        also = static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale)
+        also = static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tuning)
         # direction-optimising BFS on the same sources (same distances)
         dev_out = torch.empty((1, nV), dtype=torch.int32, device=f"cuda:{dev}")
+
+        def bfs8_do():
+            for j in range(8):
+                bfs.run_multi([int(sources[j])], out=tune8[j:j + 1], direction_optimizing=True)
+            return tune8.clone()
+
+        tuning["bfs_do"] = tuning_setup(args, "bfs_do", nV, nE, h.max_degree(), bfs8_do,
+                                        torch.equal)
         for i in range(W):
             bfs.run_multi([int(sources[i % len(sources)])], out=dev_out, direction_optimizing=True)
         do_edges = [0]
@@ -364,15 +399,18 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
         "cpu_baseline": cpu,
         "gpu_launches": int(launches),
         "clocks": clk,
+        "tuning": tuning,
         "also": also,
     }
 
 
-def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale):
+def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tuning):
     import torch
     also = {}
     # triangle counting (orientation + intersection per run)
     tc = H.TriangleCounting2(h)
+    tuning["tc"] = tuning_setup(args, "tc", nV, nE, h.max_degree(), tc.run,
+                                lambda a, b: a == b)
     for _ in range(2):
         tc.run()
     reps = 3
@@ -625,6 +663,14 @@ def bench_batch(args, H, dev, stream, rank, world, peak, peak_kind, barrier, max
     out = torch.empty((S, nV), dtype=torch.int32, device=f"cuda:{dev}")
     pv = torch.empty(nV, dtype=torch.int64, device=f"cuda:{dev}")
 
+    def bfs_all():
+        gb.bfs(local, out)
+        return out.clone()
+
+    tuning = {"msbfs": tuning_setup(args, "msbfs", nV, nE, h.max_degree(), bfs_all, torch.equal),
+              "tc": tuning_setup(args, "tc", nV, nE, h.max_degree(),
+                                 lambda: gb.triangles(pv)[0].clone(), torch.equal)}
+
     def step():
         st = gb.bfs(local, out)
         tri, _ = gb.triangles(pv)
@@ -697,7 +743,8 @@ def bench_batch(args, H, dev, stream, rank, world, peak, peak_kind, barrier, max
                                 "sample_graphs": int(len(sample)),
                                 "ms_per_graph": round(tp / len(sample) * 1e3, 3)},
            "speedup_vs_per_request": round((ng / t) / per_rate, 2),
-           "results_identical_on_sample": agree, "build_s": round(build_s, 2)}
+           "results_identical_on_sample": agree, "build_s": round(build_s, 2),
+           "tuning": tuning}
     del per
     return res
 
@@ -845,6 +892,10 @@ def main():
     ap.add_argument("--cpu-sources", type=int, default=8)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="tune the knobs of each workload first and save them")
+    ap.add_argument("--tuned-path", default="",
+                    help="knob file to load / save (default: the package's tuned.json)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

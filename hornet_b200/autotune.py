@@ -34,8 +34,7 @@ from . import tune_get, tune_names, tune_reset, tune_set
 
 SPACES: Dict[str, Dict[str, List[int]]] = {
     "bfs": {"bfs.ctas_per_sm": [2, 3, 4, 6, 8]},
-    "bfs_do": {"bfs.do_alpha": [4, 8, 14, 24, 48], "bfs.do_beta": [8, 24, 64, 256],
-               "bfs.ctas_per_sm": [2, 4, 8]},
+    "bfs_do": {"bfs.do_alpha": [4, 8, 14, 24, 48], "bfs.do_beta": [8, 24, 64, 256]},
     "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8]},
     "tc": {"tc.warp_cap": [64, 128, 256, 512], "tc.chunk": [4, 16, 64],
            "tc.warp_ctas_per_sm": [4, 8, 12, 16]},
