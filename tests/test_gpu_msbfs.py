@@ -118,3 +118,20 @@ def test_batch_device_output_and_errors():
         H.BfsTopDown(h).run_batch(srcs, slots=np.array([0, 1, 4], np.int32), nslots=4 - 1)
     with pytest.raises(H.HornetError):
         H.BfsTopDown(h).run_batch(np.array([g.nV], np.int32))
+
+
+@pytest.mark.parametrize("block,ctas", [(128, 2), (512, 8), (256, 6)])
+def test_batch_block_size_knobs(block, ctas):
+    """Every batched-BFS launch shape the autotuner may pick gives the same
+    distances (the CUDA graph is rebuilt when a knob changes)."""
+    g = T.rmat_graph(11, 16, seed=13)
+    h = build(g)
+    srcs = np.arange(0, 2048, 64, dtype=np.int32)
+    ref, ref_stats = oracle_slots(g, srcs, range(len(srcs)), len(srcs))
+    try:
+        H.tune_set("msbfs.block", block)
+        H.tune_set("msbfs.ctas_per_sm", ctas)
+        out, st = H.BfsTopDown(h).run_batch(srcs)
+        check(out, st, ref, ref_stats)
+    finally:
+        H.tune_reset()

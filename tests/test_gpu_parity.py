@@ -345,3 +345,32 @@ def test_tc_local(name):
     np.testing.assert_array_equal(out.cpu().numpy().astype(np.uint64), pv[seeds])
     with pytest.raises(H.HornetError):
         tc.local(np.array([g.nV], np.int32))
+
+
+@pytest.mark.parametrize("knobs", [
+    {"tc.warp_cap": 32, "tc.chunk": 1, "tc.warp_ctas_per_sm": 1},
+    {"tc.warp_cap": 64, "tc.chunk": 256, "tc.warp_ctas_per_sm": 16},
+    {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
+    {"bfs.ctas_per_sm": 8, "bfs.do_alpha": 1 << 20, "bfs.do_beta": 1 << 20},
+])
+def test_tuning_knobs_keep_results(knobs):
+    """The knob extremes the autotuner can set change only the speed: TC
+    totals and per-vertex counts, TD and DO BFS distances stay exact."""
+    g = GRAPHS["rmat10"]()
+    h = build(g)
+    ref_tc, ref_pv = O.tc(g, per_vertex=True)
+    srcs = [0, 5, 77]
+    try:
+        for k, v in knobs.items():
+            H.tune_set(k, v)
+        tc = H.TriangleCounting2(h)
+        tc.init()
+        assert tc.run(per_vertex=True) == ref_tc
+        np.testing.assert_array_equal(tc.copyTCToHost(), ref_pv)
+        td, _ = H.BfsTopDown(h).run_multi(srcs)
+        do, _ = H.BfsTopDown(h).run_multi(srcs, direction_optimizing=True)
+        for i, s in enumerate(srcs):
+            np.testing.assert_array_equal(td[i], O.bfs(g, s)[0])
+            np.testing.assert_array_equal(do[i], td[i])
+    finally:
+        H.tune_reset()
