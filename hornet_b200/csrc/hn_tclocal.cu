@@ -11,15 +11,18 @@
 // seeds' degree prefix.  A lane intersects its pair alone when the shorter
 // list has at most kLaneMax entries (probing each entry of the shorter list
 // in the longer one by a binary search narrowed from the previous hit);
-// longer pairs are taken by the whole warp, lanes striding the shorter
-// list.  Per-seed sums are warp-aggregated before one atomic.
+// longer pairs are appended to a list that a second kernel spreads over the
+// whole grid, one warp per pair, lanes striding the shorter list.  (The
+// heavy pairs of one seed sit side by side in the pair order, so leaving
+// them to the warp that met them would serialise them.)  Per-seed sums are
+// warp-aggregated before one atomic.
 #include "hn_graph.cuh"
 
 namespace hn {
 namespace {
 
 constexpr int kTclBlock = 256;
-constexpr int kLaneMax = 32;
+constexpr int kLaneMax = 8;
 
 // entries of a[0..na) that occur in b[0..nb) (both sorted, no duplicates)
 __device__ __forceinline__ unsigned common_seq(const int32_t* __restrict__ a, int na,
@@ -54,7 +57,9 @@ __global__ void __launch_bounds__(kTclBlock) k_tcl_pairs(const VRec* __restrict_
                                                          const int32_t* __restrict__ pool,
                                                          const int32_t* __restrict__ seeds,
                                                          const long long* __restrict__ prefix,
-                                                         int n, unsigned long long* counts) {
+                                                         int n, unsigned long long* counts,
+                                                         long long* heavy_list,
+                                                         unsigned long long* heavy_n) {
     const int lane = threadIdx.x & 31;
     const long long total = prefix[n];
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -88,19 +93,12 @@ __global__ void __launch_bounds__(kTclBlock) k_tcl_pairs(const VRec* __restrict_
             if (na <= kLaneMax) c = common_seq(a, na, b, nb);
             else heavy = true;
         }
-        unsigned hm = __ballot_sync(0xFFFFFFFFu, heavy);
-        while (hm) {
-            const int l = __ffs(hm) - 1;
-            hm &= hm - 1;
-            const int32_t* wa = (const int32_t*)__shfl_sync(0xFFFFFFFFu, (unsigned long long)a, l);
-            const int32_t* wb = (const int32_t*)__shfl_sync(0xFFFFFFFFu, (unsigned long long)b, l);
-            const int wna = __shfl_sync(0xFFFFFFFFu, na, l);
-            const int wnb = __shfl_sync(0xFFFFFFFFu, nb, l);
-            unsigned wc = 0;
-            for (int j = lane; j < wna; j += 32) wc += find_sorted(wb, wnb, __ldg(wa + j)) ? 1u : 0u;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) wc += __shfl_xor_sync(0xFFFFFFFFu, wc, o);
-            if (lane == l) c = wc;
+        const unsigned hm = __ballot_sync(0xFFFFFFFFu, heavy);
+        if (hm) {
+            unsigned long long at = 0;
+            if (lane == 0) at = atomicAdd(heavy_n, (unsigned long long)__popc(hm));
+            at = __shfl_sync(0xFFFFFFFFu, at, 0);
+            if (heavy) heavy_list[at + __popc(hm & ((1u << lane) - 1u))] = p;
         }
         // lanes of one seed are contiguous: one atomic per run of equal i,
         // issued by the run's last lane with the run's sum
@@ -119,6 +117,45 @@ __global__ void __launch_bounds__(kTclBlock) k_tcl_pairs(const VRec* __restrict_
         const int h = 31 - __clz(heads & upto);
         const unsigned long long ex = __shfl_sync(0xFFFFFFFFu, incl - c, h);
         if (tail && i >= 0 && incl > ex) atomicAdd(counts + i, incl - ex);
+    }
+}
+
+// One warp per listed heavy pair: lanes stride the shorter list and probe
+// the longer one.
+__global__ void __launch_bounds__(kTclBlock) k_tcl_heavy(const VRec* __restrict__ vtab,
+                                                         const int32_t* __restrict__ pool,
+                                                         const int32_t* __restrict__ seeds,
+                                                         const long long* __restrict__ prefix,
+                                                         int n, unsigned long long* counts,
+                                                         const long long* __restrict__ heavy_list,
+                                                         const unsigned long long* heavy_n) {
+    const int lane = threadIdx.x & 31;
+    const long long nh = (long long)*heavy_n;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long h = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh;
+         h += warps) {
+        const long long p = heavy_list[h];
+        int lo = 0, hi = n;   // last i with prefix[i] <= p
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (__ldg(prefix + mid) <= p) lo = mid; else hi = mid;
+        }
+        const int i = lo;
+        const VRec rv = vtab[seeds[i]];
+        const int32_t u = __ldg(pool + rv.off + (p - __ldg(prefix + i)));
+        const VRec ru = vtab[u];
+        const int32_t* a = pool + rv.off;
+        const int32_t* b = pool + ru.off;
+        int na = rv.deg, nb = ru.deg;
+        if (na > nb) {
+            const int32_t* t = a; a = b; b = t;
+            int tn = na; na = nb; nb = tn;
+        }
+        unsigned c = 0;
+        for (int j = lane; j < na; j += 32) c += find_sorted(b, nb, __ldg(a + j)) ? 1u : 0u;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        if (lane == 0 && c) atomicAdd(counts + i, (unsigned long long)c);
     }
 }
 
@@ -172,8 +209,19 @@ extern "C" int hn_tc_local(hn_graph_t* g, const int32_t* seeds, int32_t k, uint6
         d_counts = cbuf.get();
     }
     HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * k, s));
+    // the pair count sizes the heavy-pair list
+    HN_CUDA(cudaMemcpyAsync(g->h_scalar + 4, prefix.get() + k, sizeof(long long),
+                            cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
+    const long long pairs = g->h_scalar[4];
+    DevBuf<long long> heavy((size_t)pairs + 1, s);
+    unsigned long long* heavy_n = (unsigned long long*)(g->d_scalar + 5);
+    HN_CUDA(cudaMemsetAsync(heavy_n, 0, sizeof(unsigned long long), s));
     HN_LAUNCH(k_tcl_pairs, (long long)g->info.sms * 8, kTclBlock, 0, s, g->vtab, g->pool, d_seeds,
-              prefix.get(), k, d_counts);
+              prefix.get(), k, d_counts, heavy.get(), heavy_n);
+    HN_LAUNCH(k_tcl_heavy, (long long)g->info.sms * 8, kTclBlock, 0, s, g->vtab, g->pool,
+              d_seeds, prefix.get(), k, d_counts, (const long long*)heavy.get(),
+              (const unsigned long long*)heavy_n);
     HN_LAUNCH(k_tcl_half, grid_for(g, k, 256), 256, 0, s, d_counts, k);
     if (mem == HN_MEM_HOST)
         HN_CUDA(cudaMemcpyAsync(counts, d_counts, sizeof(unsigned long long) * k,
