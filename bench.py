@@ -552,10 +552,22 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     for j, b in enumerate(sizes):
         ti = event_time(stream, lambda: step(2 * j))
         te = event_time(stream, lambda: step(2 * j + 1))
+        # stage breakdown (kernels, CUB calls, the host round trip) of one
+        # more insert and erase of the same batch
+        stages = {}
+        for which in (0, 1):
+            H.profile_enable(True)
+            step(2 * j + which)
+            r = H.profile_report()
+            H.profile_enable(False)
+            stages["insert" if which == 0 else "erase"] = {
+                k: round(v["ms"], 4) for k, v in sorted(r.items(), key=lambda kv: -kv[1]["ms"])}
         per_size.append({"batch": b, "insert_edges_per_s": round(b / ti, 1),
                          "erase_edges_per_s": round(b / te, 1),
+                         "insert_ms": round(ti * 1e3, 4), "erase_ms": round(te * 1e3, 4),
                          "insert_frac": round(model[j][0] / ti / 1e9 / peak, 4),
-                         "erase_frac": round(model[j][1] / te / 1e9 / peak, 4)})
+                         "erase_frac": round(model[j][1] / te / 1e9 / peak, 4),
+                         "stages_ms": stages})
     roof = {"kernel": "update path (sort, mark, scan, plan, assign, scatter, commit)",
             "bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": None,
@@ -681,7 +693,9 @@ def bench_batch(args, H, dev, stream, rank, world, peak, peak_kind, barrier, max
     barrier()
     t = event_time(stream, lambda: [step() for _ in range(K)]) / K
     t = max_over_ranks(t)
+    torch.cuda.nvtx.range_push("hn_msbfs")
     tb = event_time(stream, lambda: gb.bfs(local, out))
+    torch.cuda.nvtx.range_pop()
     edges = sum(x.edges_scanned for x in st)
     tri_host = tri.cpu().numpy()
 

@@ -18,6 +18,22 @@ extern bool g_profiling;
 void profile_begin(cudaStream_t s, cudaEvent_t* a);
 void profile_end(const char* name, cudaStream_t s, cudaEvent_t a);
 
+// Records the stream time of a region (library calls such as CUB sorts and
+// scans, or a host round trip) under `name` when profiling is enabled.
+struct ProfileScope {
+    const char* name;
+    cudaStream_t s;
+    cudaEvent_t ev = nullptr;
+    ProfileScope(const char* n, cudaStream_t st) : name(n), s(st) {
+        if (g_profiling) profile_begin(s, &ev);
+    }
+    ~ProfileScope() {
+        if (ev) profile_end(name, s, ev);
+    }
+    ProfileScope(const ProfileScope&) = delete;
+    ProfileScope& operator=(const ProfileScope&) = delete;
+};
+
 // Launch a kernel on `stream` and count it.  Grids of size 0 are skipped.
 #define HN_LAUNCH(kernel, grid, block, smem, stream, ...)                    \
     do {                                                                     \

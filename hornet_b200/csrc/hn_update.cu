@@ -333,6 +333,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     HN_CUDA(cudaMemsetAsync(st, 0, sizeof(AllocState), s));
     HN_LAUNCH(k_pack, grid_for(g, n, kB), kB, 0, s, b->src, b->dst, n, g->nV, L, keys.get(), st);
     {
+        ProfileScope ps("cub_sort_keys", s);
         cub::DoubleBuffer<unsigned long long> db(keys.get(), keys2.get());
         size_t tb = 0;
         HN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)n, 0, 2 * L, s));
@@ -352,6 +353,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     // 3. scan + compact
     DevBuf<unsigned long long> scan(n, s);
     {
+        ProfileScope ps("cub_scan_keep", s);
         size_t tb = 0;
         HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, val, scan.get(), (int)n, s));
         DevBuf<char> tmp(tb, s);
@@ -369,6 +371,8 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
               insert, g->vtab, seg_work.get(), seg_ncap.get(), st);
     // 5. host plan (the one synchronisation of the batch)
+    cudaEvent_t plan_ev = nullptr;   // profiled: the stream's idle time across the plan
+    if (g_profiling) profile_begin(s, &plan_ev);
     HN_CUDA(cudaMemcpyAsync(g->h_scalar, totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
                             s));
     HN_CUDA(cudaMemcpyAsync(g->h_alloc, st, sizeof(AllocState), cudaMemcpyDeviceToHost, s));
@@ -398,11 +402,13 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         long long after = (long long)plan.push_base[c] + g->h_alloc->push[c];
         ensure_free_list(g, c, after);
     }
+    if (plan_ev) profile_end("host_plan_round_trip", s, plan_ev);
     // 6. assign blocks
     HN_LAUNCH(k_assign, grid_for(g, nseg, kB), kB, 0, s, seg_ncap.get(), nseg, plan,
               (long long* const*)g->d_fl, st, seg_new_off.get());
     // 7. scatter-merge
     {
+        ProfileScope ps("cub_scan_work", s);
         size_t tb = 0;
         HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, seg_work.get(), seg_work.get(),
                                               (int)(nseg + 1), s));
