@@ -562,9 +562,20 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
             H.profile_enable(False)
             stages["insert" if which == 0 else "erase"] = {
                 k: round(v["ms"], 4) for k, v in sorted(r.items(), key=lambda kv: -kv[1]["ms"])}
+        # insert + incremental triangle count (then the erase restores)
+        bt_j = batches[j][0]
+        newtri = [0]
+
+        def ins_tc():
+            newtri[0] = h.insert_count_triangles(bt_j)[1]
+
+        tt = event_time(stream, ins_tc)
+        step(2 * j + 1)
         per_size.append({"batch": b, "insert_edges_per_s": round(b / ti, 1),
                          "erase_edges_per_s": round(b / te, 1),
                          "insert_ms": round(ti * 1e3, 4), "erase_ms": round(te * 1e3, 4),
+                         "insert_with_new_triangles_ms": round(tt * 1e3, 4),
+                         "new_triangles": int(newtri[0]),
                          "insert_frac": round(model[j][0] / ti / 1e9 / peak, 4),
                          "erase_frac": round(model[j][1] / te / 1e9 / peak, 4),
                          "stages_ms": stages})

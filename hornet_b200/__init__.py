@@ -106,6 +106,7 @@ _SIGNATURES = {
     "hn_tc": [_P, _P, _INT, _P],
     "hn_tc_local": [_P, _P, _I32, _P, _INT],
     "hn_update_coalesced": [_P, _I64, _P, _P, _P, _INT, _P, _P],
+    "hn_insert_count_triangles": [_P, _P, _P, _P],
     "hn_tune_set": [ctypes.c_char_p, _I64],
     "hn_tune_get": [ctypes.c_char_p, _P],
     "hn_tune_reset": [],
@@ -309,6 +310,14 @@ class Hornet:
         return off, adj
 
     get_csr = getCSR
+
+    def insert_count_triangles(self, batch: "BatchUpdate") -> Tuple[int, int]:
+        """insert(batch, True, True) that also returns the triangles it
+        created (hn_insert_count_triangles): (edges added, new triangles)."""
+        n, t = ctypes.c_int64(), ctypes.c_uint64()
+        _check(lib().hn_insert_count_triangles(self._h, batch.handle, ctypes.byref(n),
+                                               ctypes.byref(t)))
+        return n.value, t.value
 
     def update_coalesced(self, src, dst, ops) -> Tuple[int, int]:
         """A run of insert/erase batches applied as one (hn_update_coalesced):

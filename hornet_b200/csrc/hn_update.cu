@@ -320,7 +320,118 @@ __global__ void k_commit(const int32_t* __restrict__ seg_u, const int32_t* __res
     }
 }
 
-void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* applied) {
+// Keys (src << L | dst) of the edges an insert actually added, ascending.
+__global__ void k_new_keys(const int32_t* __restrict__ cdst, const int32_t* __restrict__ cseg,
+                           const int32_t* __restrict__ seg_u, long long kept, int L,
+                           unsigned long long* __restrict__ nkeys) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < kept;
+         i += (long long)gridDim.x * blockDim.x)
+        nkeys[i] = ((unsigned long long)(unsigned)seg_u[cseg[i]] << L) | (unsigned)cdst[i];
+}
+
+__device__ __forceinline__ bool key_in(const unsigned long long* __restrict__ keys, long long n,
+                                       unsigned long long k) {
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+        long long mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1; else hi = mid;
+    }
+    return lo < n && keys[lo] == k;
+}
+
+// Triangles created by an insert, counted on the updated graph: every
+// added edge (u, v) with u < v meets each w in N(u) ∩ N(v); the triangle
+// {u, v, w} holds k = 1 + [uw added] + [vw added] added edges and is met k
+// times, so tallies by k give  new = c1 + c2 / 2 + c3 / 3.  A lane takes an
+// edge whose shorter list has at most 32 entries; longer ones are taken by
+// the whole warp in turn.
+__global__ void __launch_bounds__(kB) k_tc_delta(const VRec* __restrict__ vtab,
+                                                 const int32_t* __restrict__ pool,
+                                                 const unsigned long long* __restrict__ nkeys,
+                                                 long long nk, int L,
+                                                 unsigned long long* __restrict__ tally) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long mask = (1ull << L) - 1;
+    unsigned long long c[3] = {0, 0, 0};
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nk;
+         base += stride) {
+        const long long p = base + lane;
+        bool heavy = false;
+        int u = 0, v = 0, na = 0, nb = 0;
+        const int32_t* a = nullptr;
+        const int32_t* b = nullptr;
+        if (p < nk) {
+            const unsigned long long k = nkeys[p];
+            u = (int)(k >> L);
+            v = (int)(k & mask);
+            if (u < v) {
+                const VRec ru = vtab[u], rv = vtab[v];
+                a = pool + ru.off;
+                na = ru.deg;
+                b = pool + rv.off;
+                nb = rv.deg;
+                if (na > nb) {
+                    const int32_t* t = a; a = b; b = t;
+                    int tn = na; na = nb; nb = tn;
+                }
+                if (na > 32) {
+                    heavy = true;
+                } else {
+                    int lo = 0;
+                    for (int i = 0; i < na && lo < nb; i++) {
+                        const int32_t x = a[i];
+                        int hi = nb;
+                        while (lo < hi) {
+                            int mid = (lo + hi) >> 1;
+                            if (b[mid] < x) lo = mid + 1; else hi = mid;
+                        }
+                        if (lo < nb && b[lo] == x) {
+                            lo++;
+                            const int kk = (int)key_in(nkeys, nk, ((unsigned long long)(unsigned)u << L) | (unsigned)x) +
+                                           (int)key_in(nkeys, nk, ((unsigned long long)(unsigned)v << L) | (unsigned)x);
+                            c[kk]++;
+                        }
+                    }
+                }
+            }
+        }
+        unsigned hm = __ballot_sync(0xFFFFFFFFu, heavy);
+        while (hm) {
+            const int l = __ffs(hm) - 1;
+            hm &= hm - 1;
+            const int32_t* wa = (const int32_t*)__shfl_sync(0xFFFFFFFFu, (unsigned long long)a, l);
+            const int32_t* wb = (const int32_t*)__shfl_sync(0xFFFFFFFFu, (unsigned long long)b, l);
+            const int wna = __shfl_sync(0xFFFFFFFFu, na, l);
+            const int wnb = __shfl_sync(0xFFFFFFFFu, nb, l);
+            const int wu = __shfl_sync(0xFFFFFFFFu, u, l);
+            const int wv = __shfl_sync(0xFFFFFFFFu, v, l);
+            for (int j = lane; j < wna; j += 32) {
+                const int32_t x = wa[j];
+                int lo = 0, hi = wnb;
+                while (lo < hi) {
+                    int mid = (lo + hi) >> 1;
+                    if (wb[mid] < x) lo = mid + 1; else hi = mid;
+                }
+                if (lo < wnb && wb[lo] == x) {
+                    const int kk = (int)key_in(nkeys, nk, ((unsigned long long)(unsigned)wu << L) | (unsigned)x) +
+                                   (int)key_in(nkeys, nk, ((unsigned long long)(unsigned)wv << L) | (unsigned)x);
+                    c[kk]++;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        unsigned long long x = c[k];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
+        if (lane == 0 && x) atomicAdd(tally + k, x);
+    }
+}
+
+void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* applied,
+                unsigned long long* new_triangles = nullptr) {
     cudaStream_t s = g->stream;
     const long long n = b->n;
     if (applied) *applied = 0;
@@ -383,7 +494,17 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     }
     const long long kept = g->h_scalar[0];
     const long long nseg = g->h_scalar[1];
-    if (kept == 0) return;
+    if (new_triangles) *new_triangles = 0;
+    if (kept == 0) {
+        if (plan_ev) profile_end("host_plan_round_trip", s, plan_ev);
+        return;
+    }
+    DevBuf<unsigned long long> nkeys;
+    if (new_triangles) {
+        nkeys.alloc((size_t)kept, s);
+        HN_LAUNCH(k_new_keys, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), seg_u.get(),
+                  kept, L, nkeys.get());
+    }
 
     Plan plan;
     unsigned long long bump = (g->bump_host + 3) & ~3ull;
@@ -441,6 +562,17 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     g->bump_host = bump;
     g->nE += insert ? kept : -kept;
     if (applied) *applied = kept;
+    if (new_triangles) {
+        unsigned long long* tally = (unsigned long long*)(g->d_scalar + 8);
+        HN_CUDA(cudaMemsetAsync(tally, 0, 3 * sizeof(unsigned long long), s));
+        HN_LAUNCH(k_tc_delta, grid_for(g, kept, kB), kB, 0, s, g->vtab, g->pool,
+                  (const unsigned long long*)nkeys.get(), kept, L, tally);
+        HN_CUDA(cudaMemcpyAsync(g->h_scalar + 8, tally, 3 * sizeof(long long),
+                                cudaMemcpyDeviceToHost, s));
+        HN_CUDA(cudaStreamSynchronize(s));
+        const unsigned long long* t = (const unsigned long long*)(g->h_scalar + 8);
+        *new_triangles = t[0] + t[1] / 2 + t[2] / 3;
+    }
     HN_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -562,6 +694,18 @@ int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
     HN_REQUIRE((flags & ~(HN_DEDUP_BATCH | HN_DEDUP_GRAPH)) == 0, "unknown flags");
     HN_CUDA(cudaSetDevice(g->device));
     run_update(g, b, flags, true, applied);
+    HN_API_END
+}
+
+int hn_insert_count_triangles(hn_graph_t* g, hn_batch_t* b, int64_t* applied,
+                              uint64_t* new_triangles) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && b && new_triangles, "null argument");
+    HN_REQUIRE(b->g == g, "batch belongs to another graph");
+    HN_CUDA(cudaSetDevice(g->device));
+    unsigned long long t = 0;
+    run_update(g, b, HN_DEDUP_BATCH | HN_DEDUP_GRAPH, true, applied, &t);
+    *new_triangles = t;
     HN_API_END
 }
 

@@ -178,6 +178,16 @@ int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied);
  * removed. */
 int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied);
 
+/* Insert with both dedup flags (as hn_insert) and count the triangles the
+ * insert created: *new_triangles = T(after) - T(before).  For an undirected
+ * simple graph and a batch holding both directions of every edge (the
+ * incremental triangle count after each insert of the dynamic-update
+ * workload; the reference has no dynamic triangle counting, and
+ * TriangleCounting2 (hornetsnest/src/Static/TriangleCounting/triangle2.cu)
+ * recounts the whole graph). */
+int hn_insert_count_triangles(hn_graph_t* g, hn_batch_t* b, int64_t* applied,
+                              uint64_t* new_triangles);
+
 /* A run of update batches applied as one: entry i inserts (ops[i] != 0) or
  * erases (ops[i] == 0) edge (src[i], dst[i]), the entries in the order the
  * batches arrived.  On a simple graph the result equals applying the

@@ -374,3 +374,29 @@ def test_tuning_knobs_keep_results(knobs):
             np.testing.assert_array_equal(do[i], td[i])
     finally:
         H.tune_reset()
+
+
+@pytest.mark.parametrize("name", ["rmat10", "er2000"])
+def test_insert_count_triangles(name):
+    """Triangles created by each insert == the oracle's T(after) - T(before),
+    over a sequence of batches (some edges already present, some repeated
+    inside a batch, triangles with 1, 2 and 3 new edges)."""
+    g = GRAPHS[name]()
+    h = build(g)
+    rng = np.random.default_rng(12)
+    for it in range(4):
+        s, d = T.uniform_new_edges(g, 400, seed=100 + it)
+        es, ed = g.coo()
+        pick = rng.integers(0, len(es), 50)
+        # a closed triangle of brand-new edges among three random vertices
+        tri = rng.choice(g.nV, 3, replace=False).astype(np.int32)
+        ts = np.array([tri[0], tri[1], tri[2], tri[1], tri[2], tri[0]], np.int32)
+        td = np.array([tri[1], tri[2], tri[0], tri[0], tri[1], tri[2]], np.int32)
+        bs = np.concatenate([s, es[pick], ts, s[:20]]).astype(np.int32)
+        bd = np.concatenate([d, ed[pick], td, d[:20]]).astype(np.int32)
+        before = O.tc(g)
+        g, n_ref = O.insert(g, bs, bd, 3)
+        n, new = h.insert_count_triangles(H.BatchUpdate(h, bs, bd))
+        assert n == n_ref
+        assert new == O.tc(g) - before
+    assert_same_graph(h, g)
