@@ -163,11 +163,16 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
 }
 
 // Per touched vertex: new degree / class; request and release counts.
-// seg_work[s] = old degree if the vertex changes, else 0.
-__global__ void k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
-                       const long long* __restrict__ totals, bool insert,
-                       const VRec* __restrict__ vtab, long long* __restrict__ seg_work,
-                       int32_t* __restrict__ seg_ncap, AllocState* st) {
+// seg_work[s] = old degree if the vertex changes, else 0.  The per-class
+// counts are gathered in shared memory and added once per CTA (a global
+// atomic per segment serialises on the few popular classes).
+__global__ void __launch_bounds__(kB)
+k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
+       const long long* __restrict__ totals, bool insert, const VRec* __restrict__ vtab,
+       long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap, AllocState* st) {
+    __shared__ int s_need[kNumClasses], s_push[kNumClasses];
+    for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_need[c] = s_push[c] = 0;
+    __syncthreads();
     long long nseg = totals[1];
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s <= nseg;
          s += (long long)gridDim.x * blockDim.x) {
@@ -179,40 +184,60 @@ __global__ void k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restr
         if (k > 0) {
             int nd = insert ? r.deg + k : r.deg - k;
             ncap = pow2_ceil(nd);
-            if (ncap > 0) atomicAdd(&st->need[cap_class(ncap)], 1);
-            if (r.cap > 0) atomicAdd(&st->push[cap_class(r.cap)], 1);
+            if (ncap > 0) atomicAdd(&s_need[cap_class(ncap)], 1);
+            if (r.cap > 0) atomicAdd(&s_push[cap_class(r.cap)], 1);
         }
         seg_ncap[s] = ncap;
         seg_work[s] = k > 0 ? r.deg : 0;
     }
+    __syncthreads();
+    for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) {
+        if (s_need[c]) atomicAdd(&st->need[c], s_need[c]);
+        if (s_push[c]) atomicAdd(&st->push[c], s_push[c]);
+    }
+}
+
+// Contiguous range of segments owned by this CTA.
+__device__ __forceinline__ void cta_range(long long n, long long& s0, long long& s1) {
+    const long long per = (n + gridDim.x - 1) / gridDim.x;
+    s0 = (long long)blockIdx.x * per;
+    s1 = s0 + per < n ? s0 + per : n;
 }
 
 // Block assignment: per class, the first take[c] requests pop the free list,
-// the rest are carved from the bump region of the class.
-__global__ void k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
-                         long long* const* __restrict__ fl, AllocState* st,
-                         long long* __restrict__ seg_new_off) {
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg;
-         s += (long long)gridDim.x * blockDim.x) {
+// the rest are carved from the bump region of the class.  Each CTA counts
+// its range's requests per class, reserves its ranks with one atomic per
+// class, then hands them out with shared atomics.
+__global__ void __launch_bounds__(kB)
+k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
+         long long* const* __restrict__ fl, AllocState* st,
+         long long* __restrict__ seg_new_off) {
+    __shared__ int s_cnt[kNumClasses], s_base[kNumClasses];
+    for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_cnt[c] = 0;
+    __syncthreads();
+    long long s0, s1;
+    cta_range(nseg, s0, s1);
+    for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         int ncap = seg_ncap[s];
-        int c = ncap > 0 ? cap_class(ncap) : -1;
-        unsigned mask = __activemask();
-        unsigned grp = __match_any_sync(mask, c);
-        int leader = __ffs(grp) - 1;
-        int lane = threadIdx.x & 31;
-        int base = 0;
-        if (c >= 0 && lane == leader) base = atomicAdd(&st->rank[c], __popc(grp));
-        base = __shfl_sync(mask, base, leader);
-        if (c >= 0) {
-            int r = base + __popc(grp & ((1u << lane) - 1));
-            long long off;
+        if (ncap > 0) atomicAdd(&s_cnt[cap_class(ncap)], 1);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) {
+        s_base[c] = s_cnt[c] ? atomicAdd(&st->rank[c], s_cnt[c]) : 0;
+        s_cnt[c] = 0;
+    }
+    __syncthreads();
+    for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        int ncap = seg_ncap[s];
+        long long off = 0;
+        if (ncap > 0) {
+            int c = cap_class(ncap);
+            int r = s_base[c] + atomicAdd(&s_cnt[c], 1);
             if (r < plan.take[c]) off = fl[c][plan.pop_top[c] - 1 - r];
             else off = (long long)(plan.bump_base[c] +
                                    ((unsigned long long)(r - plan.take[c]) << c));
-            seg_new_off[s] = off;
-        } else {
-            seg_new_off[s] = 0;
         }
+        seg_new_off[s] = off;
     }
 }
 
@@ -246,10 +271,25 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += kB) {
-            long long e = t.item0 + i;   // global item; rank r = e - seg start
-            int b = t.seg[i];
-            int x = pool[s_old[b] + e];
+        // all of this thread's old-list loads first (the pool is both read
+        // and written here, so a plain loop would wait for each store)
+        constexpr int IPT = Tile::TILE / kB;
+        int xs[IPT], bs[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = threadIdx.x + k * kB;
+            bs[k] = -1;
+            if (i < n) {
+                bs[k] = t.seg[i];
+                xs[k] = pool[s_old[bs[k]] + t.item0 + i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            if (bs[k] < 0) continue;
+            const int b = bs[k];
+            const int x = xs[k];
+            const long long e = t.item0 + threadIdx.x + k * kB;   // global item
             const int32_t* B = cdst + s_k0[b];
             long long nb = s_k1[b] - s_k0[b];
             if (INSERT) {
@@ -294,14 +334,30 @@ __global__ void k_scatter_new(const int32_t* __restrict__ cdst, const int32_t* _
     }
 }
 
-// New vertex records; old blocks pushed on their class free list.
-__global__ void k_commit(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
-                         const int32_t* __restrict__ seg_ncap,
-                         const long long* __restrict__ seg_new_off, long long nseg, bool insert,
-                         Plan plan, long long* const* __restrict__ fl, AllocState* st,
-                         VRec* __restrict__ vtab) {
-    for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s < nseg;
-         s += (long long)gridDim.x * blockDim.x) {
+// New vertex records; old blocks pushed on their class free list (ranks
+// reserved per CTA and class, as in k_assign).
+__global__ void __launch_bounds__(kB)
+k_commit(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
+         const int32_t* __restrict__ seg_ncap, const long long* __restrict__ seg_new_off,
+         long long nseg, bool insert, Plan plan, long long* const* __restrict__ fl,
+         AllocState* st, VRec* __restrict__ vtab) {
+    __shared__ int s_cnt[kNumClasses], s_base[kNumClasses];
+    for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_cnt[c] = 0;
+    __syncthreads();
+    long long s0, s1;
+    cta_range(nseg, s0, s1);
+    for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+        if (seg_ncap[s] < 0) continue;
+        int cap = vtab[seg_u[s]].cap;
+        if (cap > 0) atomicAdd(&s_cnt[cap_class(cap)], 1);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) {
+        s_base[c] = s_cnt[c] ? atomicAdd(&st->prank[c], s_cnt[c]) : 0;
+        s_cnt[c] = 0;
+    }
+    __syncthreads();
+    for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         int ncap = seg_ncap[s];
         if (ncap < 0) continue;
         int u = seg_u[s];
@@ -309,7 +365,7 @@ __global__ void k_commit(const int32_t* __restrict__ seg_u, const int32_t* __res
         VRec r = vtab[u];
         if (r.cap > 0) {
             int c = cap_class(r.cap);
-            int p = atomicAdd(&st->prank[c], 1);
+            int p = s_base[c] + atomicAdd(&s_cnt[c], 1);
             fl[c][plan.push_base[c] + p] = r.off;
         }
         VRec nr;
@@ -525,7 +581,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     }
     if (plan_ev) profile_end("host_plan_round_trip", s, plan_ev);
     // 6. assign blocks
-    HN_LAUNCH(k_assign, grid_for(g, nseg, kB), kB, 0, s, seg_ncap.get(), nseg, plan,
+    HN_LAUNCH(k_assign, grid_for(g, nseg, kB, 4), kB, 0, s, seg_ncap.get(), nseg, plan,
               (long long* const*)g->d_fl, st, seg_new_off.get());
     // 7. scatter-merge
     {
@@ -554,7 +610,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
                   g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
     }
     // 8. commit
-    HN_LAUNCH(k_commit, grid_for(g, nseg, kB), kB, 0, s, seg_u.get(), seg_kstart.get(),
+    HN_LAUNCH(k_commit, grid_for(g, nseg, kB, 4), kB, 0, s, seg_u.get(), seg_kstart.get(),
               seg_ncap.get(), seg_new_off.get(), nseg, insert, plan, (long long* const*)g->d_fl,
               st, g->vtab);
     for (int c = 0; c < kNumClasses; c++)
