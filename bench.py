@@ -326,8 +326,8 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     total_edges = sum_over_ranks(scanned[0])
     value = total_edges / t_max / 1e9
 
-    # ---- e2e: public API, host output buffer, wall clock ----
-    host_out = np.empty(nV, np.int32)
+    # ---- e2e: public API, pinned host output buffer, wall clock ----
+    host_out = torch.empty(nV, dtype=torch.int32, pin_memory=True).numpy()
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -586,8 +586,9 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
             "peak_kind": peak_kind, "per_batch_size": per_size,
             "note": "device time of whole insert/erase calls (includes the one host "
                     "synchronisation per batch)"}
-    # e2e: host batch arrays copied in every step
-    host = [(bs.cpu().numpy(), bd.cpu().numpy(), b) for (_, b, bs, bd) in batches]
+    # e2e: pinned host batch arrays copied in every step
+    host = [(bs.cpu().pin_memory().numpy(), bd.cpu().pin_memory().numpy(), b)
+            for (_, b, bs, bd) in batches]
     bt = H.BatchUpdate(h, host[0][0][:1], host[0][1][:1])
     torch.cuda.synchronize()
     t0 = time.perf_counter()

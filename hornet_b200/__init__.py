@@ -107,6 +107,7 @@ _SIGNATURES = {
     "hn_tc_local": [_P, _P, _I32, _P, _INT],
     "hn_update_coalesced": [_P, _I64, _P, _P, _P, _INT, _P, _P],
     "hn_insert_count_triangles": [_P, _P, _P, _P],
+    "hn_ktruss_keep": [_P, _I32, _P, _P],
     "hn_tune_set": [ctypes.c_char_p, _I64],
     "hn_tune_get": [ctypes.c_char_p, _P],
     "hn_tune_reset": [],
@@ -615,6 +616,15 @@ class KTruss(StaticAlgorithm):
 
     def getMaxK(self) -> int:
         return self.max_k
+
+    def runForKDynamic(self, K: int) -> int:
+        """KTruss::runForKDynamic (KTruss.cu:270-295): erase every edge below
+        the K-truss from the graph itself (hn_ktruss_keep).  Returns the
+        number of directed edges erased; max_k is the graph's max K before."""
+        k, n = ctypes.c_int32(), ctypes.c_int64()
+        _check(lib().hn_ktruss_keep(self.hornet.handle, int(K), ctypes.byref(k), ctypes.byref(n)))
+        self.max_k = k.value
+        return n.value
 
 
 # ---------------------------------------------------------------------------

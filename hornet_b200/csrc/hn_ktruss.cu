@@ -20,6 +20,8 @@
 // surviving edge sets, truss numbers and max_K are those of the reference
 // loop.  Edge ids are positions in the sorted CSR; undirected edge state
 // lives on the (u < v) position.
+#include <cub/cub.cuh>
+
 #include "hn_graph.cuh"
 
 namespace hn {
@@ -170,6 +172,29 @@ __global__ void k_kt_out(const int32_t* __restrict__ canon, const int32_t* __res
         out[e] = truss[canon[e]];
 }
 
+// Edges (in sorted-COO order) whose truss number is below K, compacted
+// into an erase batch: keep[e] = truss[e] < K, pos = exclusive scan of keep.
+__global__ void k_kt_below(const int32_t* __restrict__ truss, long long m, int K,
+                           int32_t* __restrict__ flag) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x)
+        flag[e] = truss[e] < K ? 1 : 0;
+}
+
+__global__ void k_kt_gather(const int32_t* __restrict__ flag, const int32_t* __restrict__ pos,
+                            const int32_t* __restrict__ src, const int32_t* __restrict__ dst,
+                            long long m, int32_t* __restrict__ osrc, int32_t* __restrict__ odst,
+                            long long* __restrict__ total) {
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x) {
+        if (flag[e]) {
+            osrc[pos[e]] = src[e];
+            odst[pos[e]] = dst[e];
+        }
+        if (e == m - 1) *total = (long long)pos[e] + flag[e];
+    }
+}
+
 int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
     cudaStream_t s = g->stream;
     const int nV = g->nV;
@@ -256,5 +281,51 @@ extern "C" int hn_ktruss(hn_graph_t* g, int32_t* max_k, int32_t* edge_truss, int
                                 cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
     if (max_k) *max_k = K;
+    HN_API_END
+}
+
+extern "C" int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t* removed) {
+    HN_API_BEGIN
+    HN_REQUIRE(g != nullptr, "graph is null");
+    HN_REQUIRE(K >= 2, "K must be at least 2");
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    if (removed) *removed = 0;
+    const long long m = g->nE;
+    if (m == 0) {
+        if (max_k) *max_k = 2;
+        return HN_OK;
+    }
+    DevBuf<int32_t> truss((size_t)m, s), src((size_t)m, s), dst((size_t)m, s), flag((size_t)m, s),
+        pos((size_t)m, s);
+    const int kmax = ktruss_run(g, truss.get());
+    int rc = hn_graph_export_coo(g, 1, src.get(), dst.get(), HN_MEM_DEVICE);
+    if (rc != HN_OK) return rc;
+    HN_LAUNCH(k_kt_below, grid_for(g, m, kB), kB, 0, s, truss.get(), m, K, flag.get());
+    {
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.get(), pos.get(), (int)m, s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, flag.get(), pos.get(), (int)m, s));
+        count_launch();
+    }
+    DevBuf<int32_t> esrc((size_t)m, s), edst((size_t)m, s);
+    long long* total = (long long*)(g->d_scalar + 6);
+    HN_LAUNCH(k_kt_gather, grid_for(g, m, kB), kB, 0, s, flag.get(), pos.get(), src.get(),
+              dst.get(), m, esrc.get(), edst.get(), total);
+    HN_CUDA(cudaMemcpyAsync(g->h_scalar + 6, total, sizeof(long long), cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
+    const long long nrem = g->h_scalar[6];
+    if (max_k) *max_k = kmax;
+    if (nrem == 0) return HN_OK;
+    // the below-K edges leave the graph through the ordinary erase pipeline
+    hn_batch_t* b = nullptr;
+    rc = hn_batch_create(g, nrem, esrc.get(), edst.get(), HN_MEM_DEVICE, &b);
+    if (rc != HN_OK) return rc;
+    int64_t n = 0;
+    rc = hn_erase(g, b, HN_DEDUP_BATCH, &n);
+    hn_batch_destroy(b);
+    if (rc != HN_OK) return rc;
+    if (removed) *removed = n;
     HN_API_END
 }

@@ -261,6 +261,13 @@ int hn_cc(hn_graph_t* g, int mode, int32_t* labels, int mem,
  * sorted-COO order, the largest k whose k-truss holds the edge (2 if none).
  * *max_k is host. */
 int hn_ktruss(hn_graph_t* g, int32_t* max_k, int32_t* edge_truss, int mem);
+/* KTruss::runForKDynamic(K) (hornetsnest/src/Static/KTruss/KTruss.cu:
+ * 270-295): the graph keeps only its K-truss.  Every edge whose truss
+ * number is below K is erased from the dynamic graph through the update
+ * pipeline (the reference peels by deleteEdgeBatch the same way).
+ * *max_k (may be NULL) receives the graph's max K before the erase,
+ * *removed (may be NULL) the directed edges erased. */
+int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t* removed);
 
 /* ---- operator primitives with built-in operators -----------------------
  * forAllEdges(hornet, vertex_array, size, op, lb) with the BinarySearch or

@@ -400,3 +400,23 @@ def test_insert_count_triangles(name):
         assert n == n_ref
         assert new == O.tc(g) - before
     assert_same_graph(h, g)
+
+
+@pytest.mark.parametrize("K", [3, 4, 6])
+def test_ktruss_keep_runForKDynamic(K):
+    """runForKDynamic(K): the graph keeps exactly the edges whose truss
+    number (oracle) is at least K; the rest leave through the erase path."""
+    g = T.rmat_graph(10, 16, seed=8)
+    h = build(g)
+    rk, ret = O.ktruss(g)
+    kt = H.KTruss(h)
+    removed = kt.runForKDynamic(K)
+    assert kt.getMaxK() == rk
+    s, d = g.coo()
+    keep = ret >= K
+    assert removed == int((~keep).sum())
+    hs, hd = h.getCOO(True)
+    np.testing.assert_array_equal(hs, s[keep])
+    np.testing.assert_array_equal(hd, d[keep])
+    # the kept graph is its own K-truss: running again removes nothing
+    assert kt.runForKDynamic(K) == 0
