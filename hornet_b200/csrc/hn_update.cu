@@ -245,7 +245,7 @@ using Tile = LbTile<kB, 4>;
 
 // Old adjacency of every changed vertex -> its new block.
 template <bool INSERT>
-__global__ void __launch_bounds__(kB)
+__global__ void __launch_bounds__(kB, 6)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
@@ -595,7 +595,9 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         count_launch();
     }
     // tiles are read from the device prefix; the grid is persistent
-    const long long grid_sc = (long long)g->info.sms * 4;
+    // six CTAs per SM (the shared-memory limit of the tile): each tile waits
+    // on a short chain of dependent loads, so more resident tiles hide it
+    const long long grid_sc = (long long)g->info.sms * 6;
     DevBuf<long long> splits;
     lb_splits(g, seg_work.get(), nseg, g->nE, Tile::TILE, splits);
     if (insert) {
