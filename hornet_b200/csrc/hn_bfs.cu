@@ -70,6 +70,8 @@ struct BfsState {
     long long edges_visited;     // sum of degrees of vertices reached so far
     int alpha;                   // direction-optimising switch thresholds
     int beta;
+    int dynamic_chunks;          // 1: CTAs take chunks from next_chunk
+    unsigned next_chunk;         // chunk counter of the current level
 };
 
 struct BfsGraph {
@@ -139,6 +141,7 @@ struct BfsSmem {
     unsigned start[kChunk + 2];   // window edge offsets (+ end)
     long long base[kChunk + 1];   // pool index = base + edge
     int nw;
+    unsigned next;                // this CTA's next chunk
     unsigned long long wsum[kBfsBlock / 32];
     unsigned long long cbase;
 };
@@ -249,7 +252,10 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
         const unsigned* qoff = st->qoff[cur];
         const int32_t* chunk = st->chunk[cur];
         const unsigned nchunks = (total + kChunk - 1) / kChunk;
-        for (unsigned c = blockIdx.x; c < nchunks; c += gridDim.x) {
+        const bool dyn = st->dynamic_chunks != 0;
+        if (threadIdx.x == 0) sm.next = dyn ? atomicAdd(&st->next_chunk, 1u) : blockIdx.x;
+        __syncthreads();
+        for (unsigned c = sm.next; c < nchunks; c = sm.next) {
             const unsigned e0 = c * kChunk;
             const unsigned e1 = e0 + kChunk < total ? e0 + kChunk : total;
             const int s0 = chunk[c];
@@ -298,6 +304,9 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
                 }
             }
             bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk, found);
+            // bfs_enqueue ends with a barrier, so every thread has read sm.next
+            if (threadIdx.x == 0) sm.next = dyn ? atomicAdd(&st->next_chunk, 1u) : c + gridDim.x;
+            __syncthreads();
         }
     } else {
         // bottom-up over all vertices, kIpt per thread, striped
@@ -345,6 +354,7 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
             unsigned long long mf = cn >> 32;
             nqoff[nn] = (unsigned)mf;
             st->ticket = 0;
+            st->next_chunk = 0;
             st->scanned += total;
             st->level = level + 1;
             if (DO) {
@@ -490,6 +500,8 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.bitmap = bg.bitmap;
         h.m_total = g->nE;
         h.alpha = (int)knob(kKnobBfsDoAlpha);
+        h.dynamic_chunks = (int)knob(kKnobBfsDynamicChunks);
+        h.next_chunk = 0;
         h.beta = (int)knob(kKnobBfsDoBeta);
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
         // profiling records the whole graph (one init + one expand per

@@ -112,6 +112,7 @@ enum Knob {
     kKnobTcWarpCap,
     kKnobTcChunk,
     kKnobTcWarpCtasPerSm,
+    kKnobBfsDynamicChunks,
     kNumKnobs
 };
 long long knob(Knob k);

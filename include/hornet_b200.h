@@ -101,6 +101,8 @@ int hn_profile_report(char* buf, int64_t len);
  *                       vertex and CTA-per-vertex counting kernels (32..512, 512)
  *   tc.chunk            vertices handed to a warp per atomic (1..256, 16)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)
+ *   bfs.dynamic_chunks  1: BFS CTAs take frontier chunks from a counter
+ *                       instead of round-robin (0..1, 0)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);
