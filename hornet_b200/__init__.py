@@ -108,6 +108,11 @@ _SIGNATURES = {
     "hn_update_coalesced": [_P, _I64, _P, _P, _P, _INT, _P, _P],
     "hn_insert_count_triangles": [_P, _P, _P, _P],
     "hn_ktruss_keep": [_P, _I32, _P, _P],
+    "hn_graph_create_csr_w": [_I32, _I64, _P, _P, _P, ctypes.c_uint32, _INT, _INT, _P],
+    "hn_graph_weighted": [_P, _P],
+    "hn_graph_export_coo_w": [_P, _INT, _P, _P, _P, _INT],
+    "hn_batch_create_w": [_P, _I64, _P, _P, _P, _INT, _P],
+    "hn_batch_reset_w": [_P, _I64, _P, _P, _P, _INT],
     "hn_tune_set": [ctypes.c_char_p, _I64],
     "hn_tune_get": [ctypes.c_char_p, _P],
     "hn_tune_reset": [],
@@ -194,6 +199,18 @@ def _ptr(a, dtype=None):
     return arr.ctypes.data_as(ctypes.c_void_p), HN_MEM_HOST, arr
 
 
+def _ptr_u32(a):
+    """Like _ptr for 32-bit edge weights: int32 / uint32 / float32 values
+    are passed as their raw 32-bit patterns."""
+    if _is_device(a):
+        assert a.element_size() == 4, "weights must be 32-bit"
+        return ctypes.c_void_p(a.data_ptr()), HN_MEM_DEVICE, a
+    arr = np.ascontiguousarray(a)
+    assert arr.dtype.itemsize == 4, "weights must be 32-bit"
+    arr = arr.view(np.uint32)
+    return arr.ctypes.data_as(ctypes.c_void_p), HN_MEM_HOST, arr
+
+
 def _out_ptr(a):
     if _is_device(a):
         return ctypes.c_void_p(a.data_ptr()), HN_MEM_DEVICE
@@ -216,6 +233,12 @@ class HornetInit:
         self.offsets = offsets
         self.edges = edges
         self.sorted = bool(sorted_adjacency)
+        self.weights = None
+
+    def insertEdgeData(self, weights) -> None:
+        """HornetInit::insertEdgeData (HornetInit.cuh:79-97) for one 32-bit
+        field per edge: int32, uint32 or float32 values (kept as raw bits)."""
+        self.weights = weights
 
     def nV(self) -> int:
         return self._nV
@@ -244,6 +267,13 @@ class Hornet:
         pa, mem_a, keep_a = _ptr(init.edges, np.int32)
         assert mem == mem_a, "offsets and edges must live in the same memory"
         flags = HN_CSR_SORTED if init.sorted else 0
+        if create and init.weights is not None:
+            assert not use64, "weighted graphs take int32 offsets"
+            pw, mem_w, keep_w = _ptr_u32(init.weights)
+            assert mem_w == mem, "weights must live with the CSR"
+            _check(lib().hn_graph_create_csr_w(init.nV(), init.nE(), po, pa, pw, flags, mem,
+                                               self._device, ctypes.byref(self._h)))
+            return
         if create:
             fn = lib().hn_graph_create_csr64 if use64 else lib().hn_graph_create_csr
             _check(fn(init.nV(), init.nE(), po, pa, flags, mem, self._device,
@@ -301,6 +331,23 @@ class Hornet:
         return src, dst
 
     get_coo = getCOO
+
+    def getCOOWeighted(self, dtype=np.uint32):
+        """getCOO(true) with the edge weights of a weighted graph:
+        (src, dst, weights); weights viewed as `dtype` (a 32-bit type)."""
+        n = self.nE()
+        src = np.empty(n, np.int32)
+        dst = np.empty(n, np.int32)
+        w = np.empty(n, np.uint32)
+        _check(lib().hn_graph_export_coo_w(self._h, 1, src.ctypes.data_as(_P),
+                                           dst.ctypes.data_as(_P), w.ctypes.data_as(_P),
+                                           HN_MEM_HOST))
+        return src, dst, w.view(dtype)
+
+    def is_weighted(self) -> bool:
+        v = ctypes.c_int32()
+        _check(lib().hn_graph_weighted(self._h, ctypes.byref(v)))
+        return bool(v.value)
 
     def getCSR(self):
         """getCSR(true): (offsets[nV+1], edges[nE]) host arrays."""
@@ -382,19 +429,28 @@ class BatchUpdate:
     """gpu::BatchUpdate built from a BatchUpdatePtr<HOST|DEVICE>(n, src, dst)
     (BatchUpdate.cuh:91-99); the batch owns a device copy."""
 
-    def __init__(self, hornet: Hornet, src, dst):
+    def __init__(self, hornet: Hornet, src, dst, weights=None):
         self._hornet = hornet
         self._h = ctypes.c_void_p()
         ps, mem, ks = _ptr(src, np.int32)
         pd, _, kd = _ptr(dst, np.int32)
         n = len(src) if not _is_device(src) else int(src.numel())
-        _check(lib().hn_batch_create(hornet.handle, n, ps, pd, mem, ctypes.byref(self._h)))
+        if weights is not None:
+            pw, _, kw = _ptr_u32(weights)
+            _check(lib().hn_batch_create_w(hornet.handle, n, ps, pd, pw, mem,
+                                           ctypes.byref(self._h)))
+        else:
+            _check(lib().hn_batch_create(hornet.handle, n, ps, pd, mem, ctypes.byref(self._h)))
 
-    def reset(self, src, dst) -> None:
+    def reset(self, src, dst, weights=None) -> None:
         ps, mem, ks = _ptr(src, np.int32)
         pd, _, kd = _ptr(dst, np.int32)
         n = len(src) if not _is_device(src) else int(src.numel())
-        _check(lib().hn_batch_reset(self._h, n, ps, pd, mem))
+        if weights is not None:
+            pw, _, kw = _ptr_u32(weights)
+            _check(lib().hn_batch_reset_w(self._h, n, ps, pd, pw, mem))
+        else:
+            _check(lib().hn_batch_reset(self._h, n, ps, pd, mem))
 
     @property
     def handle(self) -> ctypes.c_void_p:

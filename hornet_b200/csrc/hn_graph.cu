@@ -180,7 +180,8 @@ using Tile = LbTile<kLbBlock, kLbItems>;
 __global__ void __launch_bounds__(kLbBlock)
 k_fill_pool(const long long* __restrict__ off, int nV, long long nE,
             const int32_t* __restrict__ adj, const VRec* __restrict__ vtab,
-            int32_t* __restrict__ pool, const long long* __restrict__ splits, long long split_tiles) {
+            int32_t* __restrict__ pool, const long long* __restrict__ splits, long long split_tiles,
+            const uint32_t* __restrict__ w, uint32_t* __restrict__ wpool) {
     __shared__ Tile t;
     __shared__ long long dst_base[Tile::TILE + 1];
     long long ntiles = (nE + nV + Tile::TILE - 1) / Tile::TILE;
@@ -194,6 +195,7 @@ k_fill_pool(const long long* __restrict__ off, int nV, long long nE,
         for (int i = threadIdx.x; i < n; i += kLbBlock) {
             long long e = t.item0 + i;
             pool[dst_base[t.seg[i]] + e] = adj[e];
+            if (wpool) wpool[dst_base[t.seg[i]] + e] = w[e];
         }
         __syncthreads();
     }
@@ -214,7 +216,8 @@ __global__ void __launch_bounds__(kLbBlock)
 k_export(const long long* __restrict__ prefix, int nV, long long nE,
          const VRec* __restrict__ vtab, const int32_t* __restrict__ pool,
          int32_t* __restrict__ src, int32_t* __restrict__ dst,
-         const long long* __restrict__ splits, long long split_tiles) {
+         const long long* __restrict__ splits, long long split_tiles,
+         const uint32_t* __restrict__ wpool = nullptr, uint32_t* __restrict__ wout = nullptr) {
     __shared__ Tile t;
     __shared__ long long src_base[Tile::TILE + 1];
     long long ntiles = (nE + nV + Tile::TILE - 1) / Tile::TILE;
@@ -230,6 +233,7 @@ k_export(const long long* __restrict__ prefix, int nV, long long nE,
             int b = t.seg[i];
             if (src) src[e] = (int)(t.seg0 + b);
             dst[e] = pool[src_base[b] + e];
+            if (wout) wout[e] = wpool[src_base[b] + e];
         }
         __syncthreads();
     }
@@ -306,6 +310,16 @@ void ensure_pool(hn_graph* g, unsigned long long slots) {
                                 g->stream));
         HN_CUDA(cudaFreeAsync(g->pool, g->stream));
     }
+    if (g->weighted) {
+        uint32_t* nw = nullptr;
+        HN_CUDA(cudaMallocAsync((void**)&nw, ncap * sizeof(uint32_t), g->stream));
+        if (g->wpool) {
+            HN_CUDA(cudaMemcpyAsync(nw, g->wpool, g->pool_cap * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToDevice, g->stream));
+            HN_CUDA(cudaFreeAsync(g->wpool, g->stream));
+        }
+        g->wpool = nw;
+    }
     g->pool = np;
     g->pool_cap = ncap;
     HN_CUDA(cudaMemcpyAsync(&g->alloc->pool_cap, &g->pool_cap, sizeof(unsigned long long),
@@ -360,7 +374,7 @@ void export_csr64(hn_graph* g, long long* off, int32_t* adj) {
 }
 
 void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
-                    const int32_t* d_adj, bool sorted) {
+                    const int32_t* d_adj, bool sorted, const uint32_t* d_w) {
     cudaStream_t s = g->stream;
     // validation
     HN_CUDA(cudaMemsetAsync(g->alloc, 0, sizeof(AllocState), s));
@@ -396,14 +410,34 @@ void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
 
     // pool: exact fit plus headroom for updates
     if (g->pool) HN_CUDA(cudaFreeAsync(g->pool, s));
+    if (g->wpool) HN_CUDA(cudaFreeAsync(g->wpool, s));
     g->pool = nullptr;
+    g->wpool = nullptr;
     g->pool_cap = 0;
+    g->weighted = d_w != nullptr;
     ensure_pool(g, used + used / 2 + 1024);
 
     // sort adjacency lists if needed, then copy into the pool
     const int32_t* src_adj = d_adj;
+    const uint32_t* src_w = d_w;
     DevBuf<int32_t> sorted_adj;
-    if (!sorted && nE > 0) {
+    DevBuf<uint32_t> sorted_w;
+    if (!sorted && nE > 0 && d_w) {
+        // weights follow their edges; equal neighbours keep their input order
+        sorted_adj.alloc((size_t)nE, s);
+        sorted_w.alloc((size_t)nE, s);
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceSegmentedSort::StableSortPairs(nullptr, tb, d_adj, sorted_adj.get(), d_w,
+                                                          sorted_w.get(), nE, nV, d_off, d_off + 1,
+                                                          s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceSegmentedSort::StableSortPairs(tmp.get(), tb, d_adj, sorted_adj.get(),
+                                                          d_w, sorted_w.get(), nE, nV, d_off,
+                                                          d_off + 1, s));
+        count_launch();
+        src_adj = sorted_adj.get();
+        src_w = sorted_w.get();
+    } else if (!sorted && nE > 0) {
         sorted_adj.alloc((size_t)nE, s);
         size_t tb = 0;
         HN_CUDA(cub::DeviceSegmentedSort::SortKeys(nullptr, tb, d_adj, sorted_adj.get(), nE, nV,
@@ -418,7 +452,8 @@ void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
     DevBuf<long long> splits;
     lb_splits(g, d_off, nV, nE, Tile::TILE, splits);
     HN_LAUNCH(k_fill_pool, grid_for(g, ntiles, 1, 16), kLbBlock, 0, s, d_off, nV,
-              (long long)nE, src_adj, g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
+              (long long)nE, src_adj, g->vtab, g->pool, splits.get(), (long long)splits.n - 1,
+              src_w, g->weighted ? g->wpool : (uint32_t*)nullptr);
     HN_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -461,6 +496,7 @@ void free_graph_object(hn_graph* g) {
     g->ms = nullptr;
     if (g->vtab) cudaFreeAsync(g->vtab, g->stream);
     if (g->pool) cudaFreeAsync(g->pool, g->stream);
+    if (g->wpool) cudaFreeAsync(g->wpool, g->stream);
     if (g->stream) cudaStreamSynchronize(g->stream);
     cudaFree(g->alloc);
     cudaFreeHost(g->h_alloc);
@@ -509,7 +545,7 @@ void stage_csr(hn_graph* g, int32_t nV, int64_t nE, const OffT* off, const int32
 
 template <typename OffT>
 int create_impl(int32_t nV, int64_t nE, const OffT* off, const int32_t* adj, unsigned flags,
-                int mem, int device, hn_graph_t** out) {
+                int mem, int device, hn_graph_t** out, const uint32_t* w = nullptr) {
     HN_API_BEGIN
     HN_REQUIRE(out != nullptr, "out is null");
     *out = nullptr;
@@ -525,7 +561,19 @@ int create_impl(int32_t nV, int64_t nE, const OffT* off, const int32_t* adj, uns
         DevBuf<int32_t> d_adj_own;
         const int32_t* d_adj = nullptr;
         stage_csr(g, nV, nE, off, adj, mem, d_off, d_adj_own, d_adj);
-        build_from_csr(g, nV, nE, d_off.get(), d_adj, (flags & HN_CSR_SORTED) != 0);
+        DevBuf<uint32_t> d_w_own;
+        const uint32_t* d_w = w;
+        if (w && mem == HN_MEM_HOST) {
+            d_w_own.alloc((size_t)nE + 1, g->stream);
+            if (nE)
+                HN_CUDA(cudaMemcpyAsync(d_w_own.get(), w, sizeof(uint32_t) * (size_t)nE,
+                                        cudaMemcpyHostToDevice, g->stream));
+            d_w = d_w_own.get();
+        } else if (w && nE == 0) {
+            d_w_own.alloc(1, g->stream);
+            d_w = d_w_own.get();
+        }
+        build_from_csr(g, nV, nE, d_off.get(), d_adj, (flags & HN_CSR_SORTED) != 0, d_w);
     } catch (...) {
         free_graph_object(g);
         throw;
@@ -615,6 +663,23 @@ int hn_graph_create_csr(int32_t nV, int64_t nE, const int32_t* off, const int32_
     return create_impl<int32_t>(nV, nE, off, adj, flags, mem, device, out);
 }
 
+int hn_graph_create_csr_w(int32_t nV, int64_t nE, const int32_t* off, const int32_t* adj,
+                          const uint32_t* weights, unsigned flags, int mem, int device,
+                          hn_graph_t** out) {
+    if (!weights) {
+        set_last_error("weights are null");
+        return HN_ERR_INVALID;
+    }
+    return create_impl<int32_t>(nV, nE, off, adj, flags, mem, device, out, weights);
+}
+
+int hn_graph_weighted(const hn_graph_t* g, int32_t* weighted) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && weighted, "null argument");
+    *weighted = g->weighted ? 1 : 0;
+    HN_API_END
+}
+
 int hn_graph_create_csr64(int32_t nV, int64_t nE, const int64_t* off, const int32_t* adj,
                           unsigned flags, int mem, int device, hn_graph_t** out) {
     return create_impl<long long>(nV, nE, (const long long*)off, adj, flags, mem, device, out);
@@ -689,30 +754,46 @@ int hn_graph_max_degree(hn_graph_t* g, int32_t* max_degree, int32_t* max_id) {
 }
 
 int hn_graph_export_coo(hn_graph_t* g, int sorted, int32_t* src, int32_t* dst, int mem) {
+    return hn_graph_export_coo_w(g, sorted, src, dst, nullptr, mem);
+}
+
+int hn_graph_export_coo_w(hn_graph_t* g, int sorted, int32_t* src, int32_t* dst,
+                          uint32_t* weights, int mem) {
     (void)sorted;
     HN_API_BEGIN
     HN_REQUIRE(g && src && dst, "null argument");
+    HN_REQUIRE(!weights || g->weighted, "the graph has no weights");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     DevBuf<long long> prefix((size_t)g->nV + 1, s);
     degree_prefix(g, nullptr, g->nV, prefix.get());
     DevBuf<int32_t> ds, dd;
+    DevBuf<uint32_t> dw;
     int32_t *ps = src, *pd = dst;
+    uint32_t* pw = weights;
     if (mem == HN_MEM_HOST) {
         ds.alloc((size_t)g->nE, s);
         dd.alloc((size_t)g->nE, s);
         ps = ds.get();
         pd = dd.get();
+        if (weights) {
+            dw.alloc((size_t)g->nE, s);
+            pw = dw.get();
+        }
     }
     long long ntiles = (g->nE + g->nV + Tile::TILE - 1) / Tile::TILE;
     DevBuf<long long> splits;
     lb_splits(g, prefix.get(), g->nV, g->nE, Tile::TILE, splits);
     HN_LAUNCH(k_export, grid_for(g, ntiles, 1, 16), kLbBlock, 0, s, prefix.get(), g->nV,
-              g->nE, g->vtab, g->pool, ps, pd, splits.get(), (long long)splits.n - 1);
+              g->nE, g->vtab, g->pool, ps, pd, splits.get(), (long long)splits.n - 1,
+              (const uint32_t*)g->wpool, pw);
     if (mem == HN_MEM_HOST && g->nE) {
         HN_CUDA(cudaMemcpyAsync(src, ps, sizeof(int32_t) * g->nE, cudaMemcpyDeviceToHost, s));
         HN_CUDA(cudaMemcpyAsync(dst, pd, sizeof(int32_t) * g->nE, cudaMemcpyDeviceToHost, s));
+        if (weights)
+            HN_CUDA(cudaMemcpyAsync(weights, pw, sizeof(uint32_t) * g->nE,
+                                    cudaMemcpyDeviceToHost, s));
     }
     HN_CUDA(cudaStreamSynchronize(s));
     HN_API_END

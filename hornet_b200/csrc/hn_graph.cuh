@@ -159,6 +159,8 @@ struct hn_graph {
     hn::VRec* vtab = nullptr;      // nV records
     int32_t* pool = nullptr;       // edge pool
     unsigned long long pool_cap = 0;
+    bool weighted = false;         // one 32-bit value per edge slot in wpool
+    uint32_t* wpool = nullptr;     // edge weights, parallel to pool (weighted only)
 
     hn::AllocState* alloc = nullptr;      // device
     hn::AllocState* h_alloc = nullptr;    // pinned host mirror
@@ -182,7 +184,10 @@ struct hn_batch {
     int64_t n = 0;
     int32_t* src = nullptr;  // device copies (owned)
     int32_t* dst = nullptr;
+    uint32_t* w = nullptr;   // edge weights (owned)
+    bool has_w = false;      // the current contents carry weights
     size_t cap = 0;
+    size_t wcap = 0;
 };
 
 namespace hn {
@@ -200,7 +205,7 @@ void read_scalars(hn_graph* g, int count);
 // (Re)build the vertex table and pool from a device CSR with int64
 // offsets; adjacency is sorted when `sorted` is false.
 void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
-                    const int32_t* d_adj, bool sorted);
+                    const int32_t* d_adj, bool sorted, const uint32_t* d_w = nullptr);
 
 // Device exclusive prefix of degrees over `verts` (or all vertices when
 // verts == nullptr), n+1 entries written to `prefix`.

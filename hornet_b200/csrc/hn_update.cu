@@ -136,7 +136,8 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
                           const unsigned long long* __restrict__ scan, long long n, int L,
                           int32_t* __restrict__ cdst, int32_t* __restrict__ cseg,
                           int32_t* __restrict__ seg_u, int32_t* __restrict__ seg_kstart,
-                          long long* __restrict__ totals) {
+                          long long* __restrict__ totals, const uint32_t* __restrict__ wsorted,
+                          uint32_t* __restrict__ cw) {
     const unsigned long long mask = (1ull << L) - 1;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -151,6 +152,7 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
         if (v & 1) {
             cdst[pos] = (int)(k & mask);
             cseg[pos] = (int)seg;
+            if (cw) cw[pos] = wsorted[i];
         }
         if (i == n - 1) {
             long long kept = pos + (long long)(v & 1);
@@ -250,7 +252,8 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
               const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
-              const long long* __restrict__ splits, long long split_tiles) {
+              const long long* __restrict__ splits, long long split_tiles,
+              uint32_t* __restrict__ wpool) {
     __shared__ Tile t;
     __shared__ long long s_old[Tile::TILE + 1];
     __shared__ long long s_new[Tile::TILE + 1];
@@ -275,13 +278,16 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
         // and written here, so a plain loop would wait for each store)
         constexpr int IPT = Tile::TILE / kB;
         int xs[IPT], bs[IPT];
+        uint32_t ws[IPT];
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
             const int i = threadIdx.x + k * kB;
             bs[k] = -1;
+            ws[k] = 0;
             if (i < n) {
                 bs[k] = t.seg[i];
                 xs[k] = pool[s_old[bs[k]] + t.item0 + i];
+                if (wpool) ws[k] = wpool[s_old[bs[k]] + t.item0 + i];
             }
         }
 #pragma unroll
@@ -295,6 +301,7 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             if (INSERT) {
                 long long j = lower_bound_dev(B, nb, x);
                 pool[s_new[b] + e + j] = x;
+                if (wpool) wpool[s_new[b] + e + j] = ws[k];
             } else {
                 long long ub = upper_bound_dev(B, nb, x);
                 long long lb = ub;
@@ -309,7 +316,10 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
                     if (r > 0 && A[r - 1] == x) first = lower_bound_dev(A, r, x);
                     keep = (r - first) >= cnt;
                 }
-                if (keep) pool[s_new[b] + e - ub] = x;
+                if (keep) {
+                    pool[s_new[b] + e - ub] = x;
+                    if (wpool) wpool[s_new[b] + e - ub] = ws[k];
+                }
             }
         }
         __syncthreads();
@@ -322,7 +332,8 @@ __global__ void k_scatter_new(const int32_t* __restrict__ cdst, const int32_t* _
                               const int32_t* __restrict__ seg_u,
                               const int32_t* __restrict__ seg_kstart,
                               const long long* __restrict__ seg_new_off,
-                              const VRec* __restrict__ vtab, int32_t* __restrict__ pool) {
+                              const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
+                              const uint32_t* __restrict__ cw, uint32_t* __restrict__ wpool) {
     long long kept = totals[0];
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < kept;
          p += (long long)gridDim.x * blockDim.x) {
@@ -331,6 +342,7 @@ __global__ void k_scatter_new(const int32_t* __restrict__ cdst, const int32_t* _
         VRec r = vtab[seg_u[s]];
         long long pos = upper_bound_dev(pool + r.off, (long long)r.deg, x);
         pool[seg_new_off[s] + (p - seg_kstart[s]) + pos] = x;
+        if (wpool) wpool[seg_new_off[s] + (p - seg_kstart[s]) + pos] = cw ? cw[p] : 0u;
     }
 }
 
@@ -499,16 +511,34 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     DevBuf<unsigned long long> keys(n, s), keys2(n, s);
     HN_CUDA(cudaMemsetAsync(st, 0, sizeof(AllocState), s));
     HN_LAUNCH(k_pack, grid_for(g, n, kB), kB, 0, s, b->src, b->dst, n, g->nV, L, keys.get(), st);
+    // weights travel with their keys (a stable sort keeps the batch order
+    // of equal edges)
+    const bool carry_w = insert && g->weighted && b->has_w;
+    DevBuf<uint32_t> wv, wv2;
+    if (carry_w) {
+        wv.alloc(n, s);
+        wv2.alloc(n, s);
+        HN_CUDA(cudaMemcpyAsync(wv.get(), b->w, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+    }
     {
         ProfileScope ps("cub_sort_keys", s);
         cub::DoubleBuffer<unsigned long long> db(keys.get(), keys2.get());
         size_t tb = 0;
-        HN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)n, 0, 2 * L, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, db, (int)n, 0, 2 * L, s));
+        if (carry_w) {
+            cub::DoubleBuffer<uint32_t> dw(wv.get(), wv2.get());
+            HN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, db, dw, (int)n, 0, 2 * L, s));
+            DevBuf<char> tmp(tb, s);
+            HN_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, db, dw, (int)n, 0, 2 * L, s));
+            if (dw.Current() != wv.get()) std::swap(wv.p, wv2.p);
+        } else {
+            HN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)n, 0, 2 * L, s));
+            DevBuf<char> tmp(tb, s);
+            HN_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, db, (int)n, 0, 2 * L, s));
+        }
         count_launch();
         if (db.Current() != keys.get()) std::swap(keys.p, keys2.p);
     }
+    wv2.release();
     // 2. mark  (keys2 reused as the counter values)
     unsigned long long* val = keys2.get();
     if (insert)
@@ -530,8 +560,12 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     DevBuf<int32_t> cdst(n, s), cseg(n, s), seg_u(n, s), seg_kstart(n + 1, s), seg_ncap(n, s);
     DevBuf<long long> seg_work(n + 1, s), seg_new_off(n, s);
     long long* totals = g->d_scalar;
+    DevBuf<uint32_t> cw;
+    if (carry_w) cw.alloc(n, s);
     HN_LAUNCH(k_compact, grid_for(g, n, kB), kB, 0, s, keys.get(), val, scan.get(), n, L,
-              cdst.get(), cseg.get(), seg_u.get(), seg_kstart.get(), totals);
+              cdst.get(), cseg.get(), seg_u.get(), seg_kstart.get(), totals,
+              (const uint32_t*)wv.get(), cw.get());
+    wv.release();
     keys2.release();
     scan.release();
     // 4. plan
@@ -603,13 +637,14 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     if (insert) {
         HN_LAUNCH(k_scatter_old<true>, grid_sc, kB, 0, s, seg_work.get(), nseg,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
+                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
         HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), totals,
-                  seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool);
+                  seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool,
+                  (const uint32_t*)cw.get(), g->wpool);
     } else {
         HN_LAUNCH(k_scatter_old<false>, grid_sc, kB, 0, s, seg_work.get(),
                   nseg, seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1);
+                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
     }
     // 8. commit
     HN_LAUNCH(k_commit, grid_for(g, nseg, kB, 4), kB, 0, s, seg_u.get(), seg_kstart.get(),
@@ -683,13 +718,18 @@ extern "C" {
 
 int hn_batch_create(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t* dst, int mem,
                     hn_batch_t** out) {
+    return hn_batch_create_w(g, n, src, dst, nullptr, mem, out);
+}
+
+int hn_batch_create_w(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t* dst,
+                      const uint32_t* weights, int mem, hn_batch_t** out) {
     HN_API_BEGIN
     HN_REQUIRE(g && out, "null argument");
     *out = nullptr;
     hn_batch* b = new hn_batch();
     b->g = g;
     b->device = g->device;
-    int rc = hn_batch_reset(b, n, src, dst, mem);
+    int rc = hn_batch_reset_w(b, n, src, dst, weights, mem);
     if (rc != HN_OK) {
         delete b;
         return rc;
@@ -699,6 +739,11 @@ int hn_batch_create(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t*
 }
 
 int hn_batch_reset(hn_batch_t* b, int64_t n, const int32_t* src, const int32_t* dst, int mem) {
+    return hn_batch_reset_w(b, n, src, dst, nullptr, mem);
+}
+
+int hn_batch_reset_w(hn_batch_t* b, int64_t n, const int32_t* src, const int32_t* dst,
+                     const uint32_t* weights, int mem) {
     HN_API_BEGIN
     HN_REQUIRE(b != nullptr, "batch is null");
     HN_REQUIRE(n >= 0 && n <= 0x7FFFFFFF, "batch size must be in [0, 2^31)");
@@ -715,11 +760,21 @@ int hn_batch_reset(hn_batch_t* b, int64_t n, const int32_t* src, const int32_t* 
         HN_CUDA(cudaMalloc((void**)&b->dst, sizeof(int32_t) * (size_t)n));
         b->cap = (size_t)n;
     }
+    if (weights && (size_t)n > b->wcap) {
+        if (b->w) HN_CUDA(cudaFree(b->w));
+        b->w = nullptr;
+        b->wcap = 0;
+        HN_CUDA(cudaMalloc((void**)&b->w, sizeof(uint32_t) * (size_t)n));
+        b->wcap = (size_t)n;
+    }
     b->n = n;
+    b->has_w = weights != nullptr;
     if (n) {
         cudaMemcpyKind kind = mem == HN_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
         HN_CUDA(cudaMemcpyAsync(b->src, src, sizeof(int32_t) * (size_t)n, kind, g->stream));
         HN_CUDA(cudaMemcpyAsync(b->dst, dst, sizeof(int32_t) * (size_t)n, kind, g->stream));
+        if (weights)
+            HN_CUDA(cudaMemcpyAsync(b->w, weights, sizeof(uint32_t) * (size_t)n, kind, g->stream));
         HN_CUDA(cudaStreamSynchronize(g->stream));
     }
     HN_API_END
@@ -740,6 +795,7 @@ int hn_batch_destroy(hn_batch_t* b) {
     cudaSetDevice(b->device);
     if (b->src) cudaFree(b->src);
     if (b->dst) cudaFree(b->dst);
+    if (b->w) cudaFree(b->w);
     delete b;
     (void)cudaGetLastError();
     HN_API_END

@@ -124,6 +124,17 @@ int hn_graph_create_csr(int32_t nV, int64_t nE, const int32_t* off,
 int hn_graph_create_csr64(int32_t nV, int64_t nE, const int64_t* off,
                           const int32_t* adj, unsigned flags, int mem,
                           int device, hn_graph_t** out);
+/* A weighted graph: one 32-bit value per edge (an int32, a float's bits,
+ * ...), the HornetInit::insertEdgeData(...) form of the reference with one
+ * EdgeMetaType (hornet/include/Core/HornetInitialize/HornetInit.cuh:79-97,
+ * HornetInsertTestWeighted.cu).  weights[i] belongs to adj[i] and is in
+ * `mem`.  Updates carry the batch's weights (hn_batch_create_w; edges of an
+ * unweighted batch get 0); BFS, TC, CC and k-truss ignore them.
+ * hn_graph_reset_csr makes the graph unweighted. */
+int hn_graph_create_csr_w(int32_t nV, int64_t nE, const int32_t* off, const int32_t* adj,
+                          const uint32_t* weights, unsigned flags, int mem, int device,
+                          hn_graph_t** out);
+int hn_graph_weighted(const hn_graph_t* g, int32_t* weighted);
 /* gpu::Hornet::reset(HornetInit&) (HornetInitialize.i.cuh:190-204). */
 int hn_graph_reset_csr(hn_graph_t* g, int32_t nV, int64_t nE, const int32_t* off,
                        const int32_t* adj, unsigned flags, int mem);
@@ -144,6 +155,12 @@ int hn_graph_max_degree(hn_graph_t* g, int32_t* max_degree, int32_t* max_id);
  * `sorted` only documents intent. */
 int hn_graph_export_coo(hn_graph_t* g, int sorted, int32_t* src, int32_t* dst,
                         int mem);
+/* getCOO with the edge weights of a weighted graph (HornetInit::
+ * insertEdgeData + getCOO, HornetInit.cuh:79-97, HornetQuery.i.cuh:67-109,
+ * for one 32-bit field): weights[i] belongs to (src[i], dst[i]); equal
+ * (src, dst) pairs keep their insertion order. */
+int hn_graph_export_coo_w(hn_graph_t* g, int sorted, int32_t* src, int32_t* dst,
+                          uint32_t* weights, int mem);
 /* getCSR(true) (HornetQuery.i.cuh:111-151): off[nV+1], adj[nE]. */
 int hn_graph_export_csr(hn_graph_t* g, int32_t* off, int32_t* adj, int mem);
 /* Degrees of all vertices (int32[nV]). */
@@ -164,6 +181,13 @@ int hn_batch_create(hn_graph_t* g, int64_t n, const int32_t* src,
 /* Refill an existing batch (BatchUpdate::reset). */
 int hn_batch_reset(hn_batch_t* b, int64_t n, const int32_t* src,
                    const int32_t* dst, int mem);
+/* A batch with one 32-bit weight per edge (BatchUpdatePtr with one
+ * EdgeMetaType, BatchUpdate.cuh:91-99); weights are in `mem`.  Inserted
+ * edges take their batch weight; erase ignores weights. */
+int hn_batch_create_w(hn_graph_t* g, int64_t n, const int32_t* src, const int32_t* dst,
+                      const uint32_t* weights, int mem, hn_batch_t** out);
+int hn_batch_reset_w(hn_batch_t* b, int64_t n, const int32_t* src, const int32_t* dst,
+                     const uint32_t* weights, int mem);
 int hn_batch_size(const hn_batch_t* b, int64_t* n);
 int hn_batch_destroy(hn_batch_t* b);
 
