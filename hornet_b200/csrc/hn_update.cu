@@ -247,7 +247,7 @@ using Tile = LbTile<kB, 4>;
 
 // Old adjacency of every changed vertex -> its new block.
 template <bool INSERT>
-__global__ void __launch_bounds__(kB, 6)
+__global__ void __launch_bounds__(kB, 5)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
@@ -257,8 +257,9 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
     __shared__ Tile t;
     __shared__ long long s_old[Tile::TILE + 1];
     __shared__ long long s_new[Tile::TILE + 1];
-    __shared__ int s_k0[Tile::TILE + 1];
-    __shared__ int s_k1[Tile::TILE + 1];
+    __shared__ int s_k0[Tile::TILE + 1];   // the batch list of segment b, narrowed to
+    __shared__ int s_k1[Tile::TILE + 1];   // the old values this tile holds: [k0, k1)
+    __shared__ int s_kb[Tile::TILE + 1];   // batch entries of the segment before k0
     const long long total = prefix[nseg];
     long long ntiles = (total + nseg + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
@@ -266,11 +267,27 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
         for (int b = threadIdx.x; b <= t.nends; b += kB) {
             long long s = t.seg0 + b;
             if (s < nseg) {
-                long long st0 = t.seg_start(b);
-                s_old[b] = vtab[seg_u[s]].off - st0;
+                const long long st0 = t.seg_start(b);
+                const long long old_off = vtab[seg_u[s]].off;
+                s_old[b] = old_off - st0;
                 s_new[b] = seg_new_off[s] - st0;
-                s_k0[b] = seg_kstart[s];
-                s_k1[b] = seg_kstart[s + 1];
+                const int k0 = seg_kstart[s], k1 = seg_kstart[s + 1];
+                // a hub's list spans many tiles while its batch list is
+                // short: search only the batch entries that can fall between
+                // this tile's first and last old value
+                const long long lo_e = st0 > t.item0 ? st0 : t.item0;
+                const long long en = t.ends[b], tend = t.item0 + n;
+                const long long hi_e = en < tend ? en : tend;
+                int blo = 0, bhi = 0;
+                if (lo_e < hi_e && k1 > k0) {
+                    const int32_t a_lo = pool[old_off + (lo_e - st0)];
+                    const int32_t a_hi = pool[old_off + (hi_e - 1 - st0)];
+                    blo = (int)lower_bound_dev(cdst + k0, (long long)(k1 - k0), a_lo);
+                    bhi = (int)upper_bound_dev(cdst + k0, (long long)(k1 - k0), a_hi);
+                }
+                s_k0[b] = k0 + blo;
+                s_k1[b] = k0 + bhi;
+                s_kb[b] = blo;
             }
         }
         __syncthreads();
@@ -299,14 +316,16 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             const int32_t* B = cdst + s_k0[b];
             long long nb = s_k1[b] - s_k0[b];
             if (INSERT) {
-                long long j = lower_bound_dev(B, nb, x);
+                long long j = s_kb[b] + lower_bound_dev(B, nb, x);
                 pool[s_new[b] + e + j] = x;
                 if (wpool) wpool[s_new[b] + e + j] = ws[k];
             } else {
-                long long ub = upper_bound_dev(B, nb, x);
-                long long lb = ub;
-                if (ub > 0 && B[ub - 1] == x) lb = lower_bound_dev(B, ub, x);
-                long long cnt = ub - lb;  // copies of x to delete
+                // every batch copy of x lies inside the narrowed range
+                long long ubl = upper_bound_dev(B, nb, x);
+                long long lbl = ubl;
+                if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound_dev(B, ubl, x);
+                long long cnt = ubl - lbl;  // copies of x to delete
+                long long ub = s_kb[b] + ubl;
                 bool keep = true;
                 if (cnt > 0) {
                     // rank of this copy among equal values of the old list
@@ -629,9 +648,9 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         count_launch();
     }
     // tiles are read from the device prefix; the grid is persistent
-    // six CTAs per SM (the shared-memory limit of the tile): each tile waits
+    // five CTAs per SM (the shared-memory limit of the tile): each tile waits
     // on a short chain of dependent loads, so more resident tiles hide it
-    const long long grid_sc = (long long)g->info.sms * 6;
+    const long long grid_sc = (long long)g->info.sms * 5;
     DevBuf<long long> splits;
     lb_splits(g, seg_work.get(), nseg, g->nE, Tile::TILE, splits);
     if (insert) {
