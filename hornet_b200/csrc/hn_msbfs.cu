@@ -269,9 +269,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_ms_push(MsState* st) {
                 }
             }
         }
-        unsigned long long at = ms_cta_reserve<BLOCK>((unsigned long long)nt, &st->tcnt, s_wsum, &s_cb);
-        int pos = (int)at;
-        for (int k = 0; k < nt; k++) st->touched[pos + k] = touched_here[k];
+        // nothing newly touched in the whole chunk (common late in the
+        // traversal): skip the scan; the barrier still guards the window
+        if (__syncthreads_or(nt > 0)) {
+            unsigned long long at =
+                ms_cta_reserve<BLOCK>((unsigned long long)nt, &st->tcnt, s_wsum, &s_cb);
+            int pos = (int)at;
+            for (int k = 0; k < nt; k++) st->touched[pos + k] = touched_here[k];
+        }
     }
 }
 
