@@ -149,8 +149,7 @@ struct BfsSmem {
 // CTA-wide enqueue of this thread's claimed vertices w[k] (claim[k]):
 // distances written, vertices with edges appended to the next frontier with
 // their adjacency base and edge offset; ONE atomic per call reserves both
-// the queue slots and the edge range.  Must be called by all threads; ends
-// with a barrier on every path.
+// the queue slots and the edge range.  Must be called by all threads.
 __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
                                             const bool (&claim)[kIpt], int level,
                                             const VRec* __restrict__ vtab, int32_t* dist,
@@ -158,12 +157,6 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
                                             long long* nqbase, unsigned* nqoff, int32_t* nchunk,
                                             int& found) {
     const int lane = threadIdx.x & 31;
-    // most chunks of the late levels claim nothing: skip the scan then (the
-    // barrier also protects the chunk's shared window, as the full path does)
-    bool any = false;
-#pragma unroll
-    for (int k = 0; k < kIpt; k++) any |= claim[k];
-    if (!__syncthreads_or(any)) return;
     long long roff[kIpt];
     unsigned rdeg[kIpt];
     unsigned long long mine = 0;   // (degree sum << 32) | queued count
