@@ -72,6 +72,8 @@ struct BfsState {
     int beta;
     int dynamic_chunks;          // 1: CTAs take chunks from next_chunk
     unsigned next_chunk;         // chunk counter of the current level
+    int warp_strided;            // 1: a warp's edges are lane-strided (coalesced loads)
+    int pad2;
 };
 
 struct BfsGraph {
@@ -253,6 +255,7 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
         const int32_t* chunk = st->chunk[cur];
         const unsigned nchunks = (total + kChunk - 1) / kChunk;
         const bool dyn = st->dynamic_chunks != 0;
+        const bool warp_strided = st->warp_strided != 0;
         if (threadIdx.x == 0) sm.next = dyn ? atomicAdd(&st->next_chunk, 1u) : blockIdx.x;
         __syncthreads();
         for (unsigned c = sm.next; c < nchunks; c = sm.next) {
@@ -269,28 +272,70 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
             }
             if (threadIdx.x == 0) sm.nw = nw;
             __syncthreads();
-            // this thread's edges [a, b)
-            const unsigned a = e0 + threadIdx.x * kIpt;
-            const unsigned b = a + kIpt < e1 ? a + kIpt : e1;
             int w[kIpt];
             bool claim[kIpt];
 #pragma unroll
             for (int k = 0; k < kIpt; k++) { w[k] = -1; claim[k] = false; }
-            if (a < b) {
-                int lo = 0, hi = sm.nw;        // last j with start[j] <= a
-                while (hi - lo > 1) {
-                    int mid = (lo + hi) >> 1;
-                    if (sm.start[mid] <= a) lo = mid; else hi = mid;
-                }
-                int j = lo;
+            bool mine_any = false;
+            if (warp_strided) {
+                // the warp's 32*kIpt edges, lane-strided: each load reads 32
+                // consecutive edges (one window for high-degree vertices);
+                // windows are searched inside the warp's own window range
+                const unsigned wb = e0 + (threadIdx.x >> 5) * (32 * kIpt);
+                if (wb < e1) {
+                    const unsigned wl = wb + 32 * kIpt - 1 < e1 - 1 ? wb + 32 * kIpt - 1 : e1 - 1;
+                    int jw0 = 0, jw1 = 0;
+                    {
+                        int lo = 0, hi = sm.nw;   // last j with start[j] <= wb
+                        while (hi - lo > 1) {
+                            int mid = (lo + hi) >> 1;
+                            if (sm.start[mid] <= wb) lo = mid; else hi = mid;
+                        }
+                        jw0 = lo;
+                        hi = sm.nw;               // last j with start[j] <= wl
+                        while (hi - lo > 1) {
+                            int mid = (lo + hi) >> 1;
+                            if (sm.start[mid] <= wl) lo = mid; else hi = mid;
+                        }
+                        jw1 = lo;
+                    }
 #pragma unroll
-                for (int k = 0; k < kIpt; k++) {
-                    unsigned e = a + k;
-                    if (e < b) {
-                        while (sm.start[j + 1] <= e) j++;
-                        w[k] = __ldg(pool + sm.base[j] + e);
+                    for (int k = 0; k < kIpt; k++) {
+                        const unsigned e = wb + k * 32 + (threadIdx.x & 31);
+                        if (e < e1) {
+                            int lo = jw0, hi = jw1 + 1;
+                            while (hi - lo > 1) {
+                                int mid = (lo + hi) >> 1;
+                                if (sm.start[mid] <= e) lo = mid; else hi = mid;
+                            }
+                            w[k] = __ldg(pool + sm.base[lo] + e);
+                            mine_any = true;
+                        }
                     }
                 }
+            } else {
+                // this thread's edges [a, b)
+                const unsigned a = e0 + threadIdx.x * kIpt;
+                const unsigned b = a + kIpt < e1 ? a + kIpt : e1;
+                if (a < b) {
+                    mine_any = true;
+                    int lo = 0, hi = sm.nw;        // last j with start[j] <= a
+                    while (hi - lo > 1) {
+                        int mid = (lo + hi) >> 1;
+                        if (sm.start[mid] <= a) lo = mid; else hi = mid;
+                    }
+                    int j = lo;
+#pragma unroll
+                    for (int k = 0; k < kIpt; k++) {
+                        unsigned e = a + k;
+                        if (e < b) {
+                            while (sm.start[j + 1] <= e) j++;
+                            w[k] = __ldg(pool + sm.base[j] + e);
+                        }
+                    }
+                }
+            }
+            if (mine_any) {
                 unsigned word[kIpt];
 #pragma unroll
                 for (int k = 0; k < kIpt; k++)
@@ -501,6 +546,7 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.m_total = g->nE;
         h.alpha = (int)knob(kKnobBfsDoAlpha);
         h.dynamic_chunks = (int)knob(kKnobBfsDynamicChunks);
+        h.warp_strided = (int)knob(kKnobBfsWarpStrided);
         h.next_chunk = 0;
         h.beta = (int)knob(kKnobBfsDoBeta);
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));

@@ -113,6 +113,7 @@ enum Knob {
     kKnobTcChunk,
     kKnobTcWarpCtasPerSm,
     kKnobBfsDynamicChunks,
+    kKnobBfsWarpStrided,
     kNumKnobs
 };
 long long knob(Knob k);

@@ -103,6 +103,9 @@ int hn_profile_report(char* buf, int64_t len);
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)
  *   bfs.dynamic_chunks  1: BFS CTAs take frontier chunks from a counter
  *                       instead of round-robin (0..1, 0)
+ *   bfs.warp_strided    1: a warp's frontier edges are dealt to lanes
+ *                       round-robin (coalesced loads) instead of 8
+ *                       consecutive edges per thread (0..1, 0)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);

@@ -352,6 +352,8 @@ def test_tc_local(name):
     {"tc.warp_cap": 64, "tc.chunk": 256, "tc.warp_ctas_per_sm": 16},
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
+    {"bfs.warp_strided": 1},
+    {"bfs.warp_strided": 1, "bfs.dynamic_chunks": 1, "bfs.ctas_per_sm": 8},
     {"bfs.ctas_per_sm": 8, "bfs.do_alpha": 1 << 20, "bfs.do_beta": 1 << 20},
 ])
 def test_tuning_knobs_keep_results(knobs):
