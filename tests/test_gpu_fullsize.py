@@ -138,8 +138,16 @@ def test_update_round_trip(big):
     b = 1_000_000
     bs = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda()
     bd = torch.from_numpy(rng.integers(0, nV, b).astype(np.int32)).cuda()
+    # keep the pairs absent from the graph, once each: then insert + erase
+    # of the batch is an exact round trip
+    gkeys = (srcv.long() << 32) | adj.long()
+    bkeys = torch.unique((bs.long() << 32) | bd.long())
+    pos = torch.searchsorted(gkeys, bkeys).clamp(max=gkeys.numel() - 1)
+    bkeys = bkeys[gkeys[pos] != bkeys]
+    bs, bd = (bkeys >> 32).int(), (bkeys & 0xFFFFFFFF).int()
     batch = H.BatchUpdate(h, bs, bd)
     added = h.insert(batch, True, True)
+    assert added == bkeys.numel()
     assert h.nE() == adj.numel() + added
     off2 = torch.empty(nV + 1, dtype=torch.int32, device="cuda")
     adj2 = torch.empty(h.nE(), dtype=torch.int32, device="cuda")
