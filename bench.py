@@ -923,9 +923,16 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the knobs of each workload first and save them")
+    ap.add_argument("--knob", action="append", default=[],
+                    help="name=value tuning knob set before the run (repeatable)")
     ap.add_argument("--tuned-path", default="",
                     help="knob file to load / save (default: the package's tuned.json)")
     args = ap.parse_args()
+    if args.knob and args.impl != "reference":
+        import hornet_b200 as H
+        for kv in args.knob:
+            k, v = kv.split("=")
+            H.tune_set(k, int(v))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -73,7 +73,9 @@ struct BfsState {
     int dynamic_chunks;          // 1: CTAs take chunks from next_chunk
     unsigned next_chunk;         // chunk counter of the current level
     int warp_strided;            // 1: a warp's edges are lane-strided (coalesced loads)
-    int pad2;
+    int cont;                    // 1 while another level follows (host-driven loop)
+    int host_driven;             // 1: no conditional node (levels launched by the host)
+    int pad3;
 };
 
 struct BfsGraph {
@@ -415,7 +417,9 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
                     if ((long long)nn * st->beta < st->nV && nn < (unsigned)nq) st->mode = 0;
                 }
             }
-            cudaGraphSetConditional(cond, (nn > 0 && level < st->nV) ? 1u : 0u);
+            const unsigned more = (nn > 0 && level < st->nV) ? 1u : 0u;
+            st->cont = (int)more;
+            if (!st->host_driven) cudaGraphSetConditional(cond, more);
         }
     }
 }
@@ -547,6 +551,7 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.alpha = (int)knob(kKnobBfsDoAlpha);
         h.dynamic_chunks = (int)knob(kKnobBfsDynamicChunks);
         h.warp_strided = (int)knob(kKnobBfsWarpStrided);
+        h.host_driven = (int)knob(kKnobBfsHostLevels);
         h.next_chunk = 0;
         h.beta = (int)knob(kKnobBfsDoBeta);
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
@@ -554,10 +559,30 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         // level) under the name of its dominant kernel
         cudaEvent_t ev0 = nullptr;
         if (g_profiling) profile_begin(s, &ev0);
-        HN_CUDA(cudaGraphLaunch(bg.exec[direction_optimizing ? 1 : 0], s));
+        if (h.host_driven) {
+            // host-driven levels: one ordinary launch per level (each level
+            // can be profiled on its own), one host round trip per level
+            k_bfs3_init<<<(unsigned)grid_for(g, nV, 256), 256, 0, s>>>(bg.state);
+            HN_CUDA(cudaGetLastError());
+            count_launch();
+            for (int lv = 0; lv <= nV; lv++) {
+                if (direction_optimizing)
+                    k_bfs_level<true><<<bg.grid, kBfsBlock, 0, s>>>(bg.state, 0);
+                else
+                    k_bfs_level<false><<<bg.grid, kBfsBlock, 0, s>>>(bg.state, 0);
+                HN_CUDA(cudaGetLastError());
+                count_launch();
+                HN_CUDA(cudaMemcpyAsync(&bg.h_state->cont, &bg.state->cont, sizeof(int),
+                                        cudaMemcpyDeviceToHost, s));
+                HN_CUDA(cudaStreamSynchronize(s));
+                if (!bg.h_state->cont) break;
+            }
+        } else {
+            HN_CUDA(cudaGraphLaunch(bg.exec[direction_optimizing ? 1 : 0], s));
+            count_launch(2);
+        }
         if (ev0)
             profile_end(direction_optimizing ? "k_bfs_level<true>" : "k_bfs_level<false>", s, ev0);
-        count_launch(2);
         HN_CUDA(cudaMemcpyAsync(bg.h_state, bg.state, sizeof(BfsState), cudaMemcpyDeviceToHost, s));
         if (mem == HN_MEM_HOST)
             HN_CUDA(cudaMemcpyAsync(dist + (size_t)i * nV, out, sizeof(int32_t) * nV,

@@ -49,9 +49,10 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"tc.warp_ctas_per_sm", 8, 1, 16, false},
     {"bfs.dynamic_chunks", 0, 0, 1, false},
     {"bfs.warp_strided", 0, 0, 1, false},
+    {"bfs.host_levels", 0, 0, 1, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {4}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}};
+    {4}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

@@ -114,6 +114,7 @@ enum Knob {
     kKnobTcWarpCtasPerSm,
     kKnobBfsDynamicChunks,
     kKnobBfsWarpStrided,
+    kKnobBfsHostLevels,
     kNumKnobs
 };
 long long knob(Knob k);

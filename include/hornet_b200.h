@@ -106,6 +106,9 @@ int hn_profile_report(char* buf, int64_t len);
  *   bfs.warp_strided    1: a warp's frontier edges are dealt to lanes
  *                       round-robin (coalesced loads) instead of 8
  *                       consecutive edges per thread (0..1, 0)
+ *   bfs.host_levels     1: launch the BFS levels one by one from the host
+ *                       (for per-level profiling) instead of the CUDA
+ *                       graph's device-side loop (0..1, 0)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);

@@ -353,6 +353,7 @@ def test_tc_local(name):
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
     {"bfs.warp_strided": 1},
+    {"bfs.host_levels": 1, "bfs.warp_strided": 1},
     {"bfs.warp_strided": 1, "bfs.dynamic_chunks": 1, "bfs.ctas_per_sm": 8},
     {"bfs.ctas_per_sm": 8, "bfs.do_alpha": 1 << 20, "bfs.do_beta": 1 << 20},
 ])
