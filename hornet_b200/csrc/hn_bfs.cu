@@ -44,7 +44,7 @@
 
 namespace hn {
 
-constexpr int kBfsBlock = 256;
+constexpr int kBfsBlock = 128;
 constexpr int kIpt = 8;                          // edges per thread per chunk
 constexpr int kChunk = kBfsBlock * kIpt;         // edges per chunk
 
@@ -228,7 +228,7 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
 // Breadth-First Search", SC 2012).  Both produce the next frontier queue, so
 // the direction may change at any level; distances are the same either way.
 template <bool DO>
-__global__ void __launch_bounds__(kBfsBlock, 4)
+__global__ void __launch_bounds__(kBfsBlock, 8)
 k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
     __shared__ BfsSmem sm;
     const int level = st->level;

@@ -39,7 +39,7 @@ struct KnobDef {
     bool pow2;   // value must be a power of two
 };
 const KnobDef kKnobs[kNumKnobs] = {
-    {"bfs.ctas_per_sm", 4, 1, 8, false},
+    {"bfs.ctas_per_sm", 8, 1, 16, false},
     {"bfs.do_alpha", 14, 1, 1 << 20, false},
     {"bfs.do_beta", 24, 1, 1 << 20, false},
     {"msbfs.block", 256, 128, 512, true},
@@ -52,7 +52,7 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"bfs.host_levels", 0, 0, 1, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {4}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}};
+    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

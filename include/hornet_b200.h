@@ -91,7 +91,8 @@ int hn_profile_report(char* buf, int64_t len);
 /* Tuning knobs (process-wide; read when a call launches, so a change takes
  * effect on the next call).  An autotuner sets them; the defaults are the
  * built-in values.  Knobs:
- *   bfs.ctas_per_sm     CTAs per SM of the BFS level kernel (1..8, 4)
+ *   bfs.ctas_per_sm     CTAs per SM of the BFS level kernel, 128 threads
+ *                       each (1..16, 8)
  *   bfs.do_alpha        direction-optimising switch to bottom-up when the
  *                       frontier's edges exceed unexplored edges / alpha (14)
  *   bfs.do_beta         back to top-down below nV / beta frontier vertices (24)
