@@ -451,6 +451,16 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
                            peak_kind, rep, f"R-MAT scale {scale} CC")
     also["cc"] = {"metric": "CC edges/s", "value": round(nE / t, 1), "unit": "edges/s",
                   "components": cc.n_components, "ms": round(t * 1e3, 3), "roofline": croof}
+    # k-truss decomposition (all K, incremental peel), timed once
+    if not args.no_ktruss:
+        kt = H.KTruss(h)
+        t0 = time.perf_counter()
+        kmax = kt.run()
+        tk = time.perf_counter() - t0
+        also["ktruss"] = {"metric": "k-truss edges/s", "value": round(nE / tk, 1),
+                          "unit": "edges/s", "max_k": int(kmax), "ms": round(tk * 1e3, 3),
+                          "note": "all K from 3 to max_k; host-timed single run "
+                                  "(one host round trip per peel round)"}
     # one 1M-edge uniform insert + erase on the same graph
     rng = np.random.default_rng(77)
     b = 1_000_000
@@ -921,6 +931,7 @@ def main():
     ap.add_argument("--cpu-sources", type=int, default=8)
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-ktruss", action="store_true")
     ap.add_argument("--autotune", action="store_true",
                     help="tune the knobs of each workload first and save them")
     ap.add_argument("--knob", action="append", default=[],
