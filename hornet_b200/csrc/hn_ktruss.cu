@@ -84,20 +84,46 @@ __global__ void k_kt_support(const long long* __restrict__ off, const int32_t* _
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(nalive, mine);
 }
 
-__global__ void k_kt_frontier(long long m, int K, const int32_t* __restrict__ sup,
+// Frontier of round K: alive edges of the list L with support < K - 2.
+__global__ void k_kt_frontier(const int32_t* __restrict__ L, int nL, int K,
+                              const int32_t* __restrict__ sup,
                               const unsigned char* __restrict__ alive,
                               unsigned char* __restrict__ inF, int32_t* __restrict__ F,
                               int* __restrict__ nF) {
-    for (long long e0 = blockIdx.x * (long long)blockDim.x; e0 < m;
-         e0 += (long long)gridDim.x * blockDim.x) {
-        long long e = e0 + threadIdx.x;
-        bool take = e < m && alive[e] && sup[e] < K - 2;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < nL;
+         i0 += (long long)gridDim.x * blockDim.x) {
+        long long i = i0 + threadIdx.x;
+        int e = i < nL ? L[i] : 0;
+        bool take = i < nL && alive[e] && sup[e] < K - 2;
         int p = warp_append(nF, take);
         if (take) {
-            F[p] = (int)e;
+            F[p] = e;
             inF[e] = 1;
         }
     }
+}
+
+// Alive-edge list: from all canonical edges (L == nullptr, n = m) or from
+// the previous list, dropping peeled edges; *minsup receives the smallest
+// support left, so the next round can start at the first K that peels.
+__global__ void k_kt_compact(const int32_t* __restrict__ L, long long n,
+                             const unsigned char* __restrict__ alive,
+                             const int32_t* __restrict__ sup, int32_t* __restrict__ out,
+                             int* __restrict__ nout, int* __restrict__ minsup) {
+    int mn = 0x7FFFFFFF;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n;
+         i0 += (long long)gridDim.x * blockDim.x) {
+        long long i = i0 + threadIdx.x;
+        int e = i < n ? (L ? L[i] : (int)i) : 0;
+        bool take = i < n && alive[e];
+        int p = warp_append(nout, take);
+        if (take) {
+            out[p] = e;
+            mn = min(mn, sup[e]);
+        }
+    }
+    for (int o = 16; o; o >>= 1) mn = min(mn, __shfl_down_sync(0xFFFFFFFFu, mn, o));
+    if ((threadIdx.x & 31) == 0 && mn != 0x7FFFFFFF) atomicMin(minsup, mn);
 }
 
 __device__ __forceinline__ void kt_dec(int x, int K, int32_t* sup, int32_t* NF, int* nNF) {
@@ -225,12 +251,31 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
     int K = 3;
     int* nF = cnt + 1;
     int* nNF = cnt + 2;
-    const long long grid = grid_for(g, m, kB);
+    int* nL = cnt + 3;      // alive-list length
+    int* minsup = cnt + 4;  // smallest support on the alive list
+    // the frontier of each K scans only the alive edges, and K jumps to the
+    // first value that peels anything (min support + 3): R-MAT graphs reach
+    // max K in the hundreds while most edges leave at small K
+    DevBuf<int32_t> L((size_t)remaining + 1, s), L2((size_t)remaining + 1, s);
+    auto compact = [&](const int32_t* in, long long n) {
+        HN_CUDA(cudaMemsetAsync(nL, 0, sizeof(int), s));
+        const int big = 0x7FFFFFFF;
+        HN_CUDA(cudaMemcpyAsync(minsup, &big, sizeof(int), cudaMemcpyHostToDevice, s));
+        HN_LAUNCH(k_kt_compact, grid_for(g, n, kB), kB, 0, s, in, n, alive.get(), sup.get(),
+                  L2.get(), nL, minsup);
+        std::swap(L.p, L2.p);
+        HN_CUDA(cudaMemcpyAsync(g->h_scalar, cnt, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
+        HN_CUDA(cudaStreamSynchronize(s));
+        return ((int*)g->h_scalar)[3];
+    };
+    int n_alive = compact(nullptr, m);
     while (true) {
         if (remaining <= 0) { K--; break; }
+        const int ms = ((int*)g->h_scalar)[4];
+        if (ms + 3 > K) K = ms + 3;
         HN_CUDA(cudaMemsetAsync(nF, 0, sizeof(int), s));
-        HN_LAUNCH(k_kt_frontier, grid, kB, 0, s, m, K, sup.get(), alive.get(), inF.get(), F.get(),
-                  nF);
+        HN_LAUNCH(k_kt_frontier, grid_for(g, n_alive, kB), kB, 0, s, L.get(), n_alive, K,
+                  sup.get(), alive.get(), inF.get(), F.get(), nF);
         HN_CUDA(cudaMemcpyAsync(g->h_scalar, nF, sizeof(int), cudaMemcpyDeviceToHost, s));
         HN_CUDA(cudaStreamSynchronize(s));
         int nf = ((int*)g->h_scalar)[0];
@@ -241,7 +286,7 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
                       nNF);
             HN_LAUNCH(k_kt_retire, grid_for(g, nf, kB), kB, 0, s, F.get(), nf, NF.get(), nNF, K,
                       alive.get(), inF.get(), truss.get());
-            HN_LAUNCH(k_kt_mark, grid_for(g, m, kB), kB, 0, s, NF.get(), nNF, inF.get());
+            HN_LAUNCH(k_kt_mark, grid_for(g, nf, kB), kB, 0, s, NF.get(), nNF, inF.get());
             remaining -= nf;
             HN_CUDA(cudaMemcpyAsync(g->h_scalar, nNF, sizeof(int), cudaMemcpyDeviceToHost, s));
             HN_CUDA(cudaStreamSynchronize(s));
@@ -249,6 +294,7 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
             std::swap(F.p, NF.p);
         }
         if (remaining <= 0) { K--; break; }
+        n_alive = compact(L.get(), n_alive);
         K++;
     }
     if (d_edge_truss)
