@@ -131,39 +131,92 @@ __device__ __forceinline__ void kt_dec(int x, int K, int32_t* sup, int32_t* NF, 
     if (old == K - 2) NF[atomicAdd(nNF, 1)] = x;
 }
 
+// One common neighbour w of a frontier edge e = (u, v): e1 = (u, w) or
+// (v, w) and e2 the other, in canonical ids.  Each destroyed triangle is
+// charged exactly once (see the decrement rule above).
+__device__ __forceinline__ void kt_triangle(int e, int e1, int e2, int K,
+                                            const unsigned char* __restrict__ alive,
+                                            const unsigned char* __restrict__ inF,
+                                            int32_t* sup, int32_t* NF, int* nNF) {
+    if (!alive[e1] || !alive[e2]) return;
+    bool f1 = inF[e1], f2 = inF[e2];
+    if (!f1 && !f2) {
+        kt_dec(e1, K, sup, NF, nNF);
+        kt_dec(e2, K, sup, NF, nNF);
+    } else if (f1 && !f2) {
+        if (e < e1) kt_dec(e2, K, sup, NF, nNF);
+    } else if (!f1 && f2) {
+        if (e < e2) kt_dec(e1, K, sup, NF, nNF);
+    }
+}
+
+// Frontier edges whose shorter list has at most 32 entries: a thread each.
+// Longer ones go to a list for k_kt_peel_heavy (a warp each): the dense
+// core's hub-hub edges would otherwise run one long intersection per thread.
 __global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __restrict__ adj,
                           const int32_t* __restrict__ src, const int32_t* __restrict__ canon,
                           const int32_t* __restrict__ F, int nF, int K,
                           const unsigned char* __restrict__ alive,
                           const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
-                          int32_t* __restrict__ NF, int* __restrict__ nNF) {
-    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nF;
-         f += (long long)gridDim.x * blockDim.x) {
-        int e = F[f];
-        int u = src[e], v = adj[e];
-        long long au = off[u], la = off[u + 1] - au;
-        long long bv = off[v], lb = off[v + 1] - bv;
-        bool swapped = la > lb;
-        long long pa = swapped ? bv : au, pb = swapped ? au : bv;
-        long long na = swapped ? lb : la, nb = swapped ? la : lb;
-        long long lo = 0;
-        for (long long i = 0; i < na && lo < nb; i++) {
-            int w = adj[pa + i];
-            long long p = lo + lower_bound_dev(adj + pb + lo, nb - lo, w);
-            lo = p;
-            if (p >= nb || adj[pb + p] != w) continue;
-            lo = p + 1;
-            int e1 = canon[pa + i], e2 = canon[pb + p];
-            if (!alive[e1] || !alive[e2]) continue;
-            bool f1 = inF[e1], f2 = inF[e2];
-            if (!f1 && !f2) {
-                kt_dec(e1, K, sup, NF, nNF);
-                kt_dec(e2, K, sup, NF, nNF);
-            } else if (f1 && !f2) {
-                if (e < e1) kt_dec(e2, K, sup, NF, nNF);
-            } else if (!f1 && f2) {
-                if (e < e2) kt_dec(e1, K, sup, NF, nNF);
+                          int32_t* __restrict__ NF, int* __restrict__ nNF,
+                          int32_t* __restrict__ heavy, int* __restrict__ nheavy) {
+    for (long long f0 = blockIdx.x * (long long)blockDim.x; f0 < nF;
+         f0 += (long long)gridDim.x * blockDim.x) {
+        const long long f = f0 + threadIdx.x;
+        bool big = false;
+        int e = 0;
+        if (f < nF) {
+            e = F[f];
+            int u = src[e], v = adj[e];
+            long long au = off[u], la = off[u + 1] - au;
+            long long bv = off[v], lb = off[v + 1] - bv;
+            bool swapped = la > lb;
+            long long pa = swapped ? bv : au, pb = swapped ? au : bv;
+            long long na = swapped ? lb : la, nb = swapped ? la : lb;
+            if (na > 32) {
+                big = true;
+            } else {
+                long long lo = 0;
+                for (long long i = 0; i < na && lo < nb; i++) {
+                    int w = adj[pa + i];
+                    long long p = lo + lower_bound_dev(adj + pb + lo, nb - lo, w);
+                    lo = p;
+                    if (p >= nb || adj[pb + p] != w) continue;
+                    lo = p + 1;
+                    kt_triangle(e, canon[pa + i], canon[pb + p], K, alive, inF, sup, NF, nNF);
+                }
             }
+        }
+        int slot = warp_append(nheavy, big);
+        if (big) heavy[slot] = e;
+    }
+}
+
+__global__ void k_kt_peel_heavy(const long long* __restrict__ off,
+                                const int32_t* __restrict__ adj,
+                                const int32_t* __restrict__ src,
+                                const int32_t* __restrict__ canon,
+                                const int32_t* __restrict__ heavy, const int* __restrict__ nheavy,
+                                int K, const unsigned char* __restrict__ alive,
+                                const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
+                                int32_t* __restrict__ NF, int* __restrict__ nNF) {
+    const int lane = threadIdx.x & 31;
+    const long long nh = *nheavy;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long h = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh;
+         h += warps) {
+        const int e = heavy[h];
+        const int u = src[e], v = adj[e];
+        const long long au = off[u], la = off[u + 1] - au;
+        const long long bv = off[v], lb = off[v + 1] - bv;
+        const bool swapped = la > lb;
+        const long long pa = swapped ? bv : au, pb = swapped ? au : bv;
+        const long long na = swapped ? lb : la, nb = swapped ? la : lb;
+        for (long long i = lane; i < na; i += 32) {
+            const int w = adj[pa + i];
+            const long long p = lower_bound_dev(adj + pb, nb, w);
+            if (p < nb && adj[pb + p] == w)
+                kt_triangle(e, canon[pa + i], canon[pb + p], K, alive, inF, sup, NF, nNF);
         }
     }
 }
@@ -251,8 +304,10 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
     int K = 3;
     int* nF = cnt + 1;
     int* nNF = cnt + 2;
-    int* nL = cnt + 3;      // alive-list length
-    int* minsup = cnt + 4;  // smallest support on the alive list
+    int* nheavy = cnt + 3;  // frontier edges left to k_kt_peel_heavy (right after nNF)
+    int* nL = cnt + 4;      // alive-list length
+    int* minsup = cnt + 5;  // smallest support on the alive list
+    DevBuf<int32_t> H((size_t)m, s);
     // the frontier of each K scans only the alive edges, and K jumps to the
     // first value that peels anything (min support + 3): R-MAT graphs reach
     // max K in the hundreds while most edges leave at small K
@@ -266,12 +321,12 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         std::swap(L.p, L2.p);
         HN_CUDA(cudaMemcpyAsync(g->h_scalar, cnt, 8 * sizeof(int), cudaMemcpyDeviceToHost, s));
         HN_CUDA(cudaStreamSynchronize(s));
-        return ((int*)g->h_scalar)[3];
+        return ((int*)g->h_scalar)[4];
     };
     int n_alive = compact(nullptr, m);
     while (true) {
         if (remaining <= 0) { K--; break; }
-        const int ms = ((int*)g->h_scalar)[4];
+        const int ms = ((int*)g->h_scalar)[5];
         if (ms + 3 > K) K = ms + 3;
         HN_CUDA(cudaMemsetAsync(nF, 0, sizeof(int), s));
         HN_LAUNCH(k_kt_frontier, grid_for(g, n_alive, kB), kB, 0, s, L.get(), n_alive, K,
@@ -280,10 +335,13 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         HN_CUDA(cudaStreamSynchronize(s));
         int nf = ((int*)g->h_scalar)[0];
         while (nf > 0) {
-            HN_CUDA(cudaMemsetAsync(nNF, 0, sizeof(int), s));
+            HN_CUDA(cudaMemsetAsync(nNF, 0, 2 * sizeof(int), s));   // nNF, nheavy
             HN_LAUNCH(k_kt_peel, grid_for(g, nf, 128), 128, 0, s, off.get(), adj.get(), src.get(),
                       canon.get(), F.get(), nf, K, alive.get(), inF.get(), sup.get(), NF.get(),
-                      nNF);
+                      nNF, H.get(), nheavy);
+            HN_LAUNCH(k_kt_peel_heavy, grid_for(g, (long long)nf * 32, 256), 256, 0, s, off.get(),
+                      adj.get(), src.get(), canon.get(), (const int32_t*)H.get(),
+                      (const int*)nheavy, K, alive.get(), inF.get(), sup.get(), NF.get(), nNF);
             HN_LAUNCH(k_kt_retire, grid_for(g, nf, kB), kB, 0, s, F.get(), nf, NF.get(), nNF, K,
                       alive.get(), inF.get(), truss.get());
             HN_LAUNCH(k_kt_mark, grid_for(g, nf, kB), kB, 0, s, NF.get(), nNF, inF.get());
