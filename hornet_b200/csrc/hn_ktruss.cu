@@ -56,32 +56,77 @@ __global__ void k_kt_canon(const long long* __restrict__ off, const int32_t* __r
 }
 
 // support of each canonical edge = |N(u) ∩ N(v)|
+// Support of every canonical edge (u < v): |N(u) ∩ N(v)|.  Edges whose
+// shorter list exceeds 32 entries are listed for k_kt_support_heavy (a warp
+// each), as in the peel.
 __global__ void k_kt_support(const long long* __restrict__ off, const int32_t* __restrict__ adj,
                              const int32_t* __restrict__ src, long long m,
                              int32_t* __restrict__ sup, unsigned char* __restrict__ alive,
-                             int* __restrict__ nalive) {
+                             int* __restrict__ nalive, int32_t* __restrict__ heavy,
+                             int* __restrict__ nheavy) {
     int mine = 0;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
-         e += (long long)gridDim.x * blockDim.x) {
-        int u = src[e], v = adj[e];
-        if (u >= v) { alive[e] = 0; continue; }
+    for (long long e0 = blockIdx.x * (long long)blockDim.x; e0 < m;
+         e0 += (long long)gridDim.x * blockDim.x) {
+        const long long e = e0 + threadIdx.x;
+        bool big = false;
+        if (e < m) {
+            int u = src[e], v = adj[e];
+            if (u >= v) {
+                alive[e] = 0;
+            } else {
+                const int32_t* A = adj + off[u];
+                long long la = off[u + 1] - off[u];
+                const int32_t* B = adj + off[v];
+                long long lb = off[v + 1] - off[v];
+                if (la > lb) { const int32_t* T = A; A = B; B = T; long long t = la; la = lb; lb = t; }
+                if (la > 32) {
+                    big = true;
+                    sup[e] = 0;
+                } else {
+                    int cnt = 0;
+                    long long lo = 0;
+                    for (long long i = 0; i < la && lo < lb; i++) {
+                        long long p = lo + lower_bound_dev(B + lo, lb - lo, A[i]);
+                        if (p < lb && B[p] == A[i]) { cnt++; lo = p + 1; } else lo = p;
+                    }
+                    sup[e] = cnt;
+                }
+                alive[e] = 1;
+                mine++;
+            }
+        }
+        int slot = warp_append(nheavy, big);
+        if (big) heavy[slot] = (int)e;
+    }
+    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(nalive, mine);
+}
+
+__global__ void k_kt_support_heavy(const long long* __restrict__ off,
+                                   const int32_t* __restrict__ adj,
+                                   const int32_t* __restrict__ src,
+                                   const int32_t* __restrict__ heavy,
+                                   const int* __restrict__ nheavy, int32_t* __restrict__ sup) {
+    const int lane = threadIdx.x & 31;
+    const long long nh = *nheavy;
+    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long h = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh;
+         h += warps) {
+        const int e = heavy[h];
+        const int u = src[e], v = adj[e];
         const int32_t* A = adj + off[u];
         long long la = off[u + 1] - off[u];
         const int32_t* B = adj + off[v];
         long long lb = off[v + 1] - off[v];
         if (la > lb) { const int32_t* T = A; A = B; B = T; long long t = la; la = lb; lb = t; }
         int cnt = 0;
-        long long lo = 0;
-        for (long long i = 0; i < la && lo < lb; i++) {
-            long long p = lo + lower_bound_dev(B + lo, lb - lo, A[i]);
-            if (p < lb && B[p] == A[i]) { cnt++; lo = p + 1; } else lo = p;
+        for (long long i = lane; i < la; i += 32) {
+            const long long p = lower_bound_dev(B, lb, A[i]);
+            cnt += (p < lb && B[p] == A[i]) ? 1 : 0;
         }
-        sup[e] = cnt;
-        alive[e] = 1;
-        mine++;
+        for (int o = 16; o; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
+        if (lane == 0) sup[e] = cnt;
     }
-    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
-    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(nalive, mine);
 }
 
 // Frontier of round K: alive edges of the list L with support < K - 2.
@@ -295,8 +340,11 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         throw Error(HN_ERR_INVALID, "k-truss needs a simple symmetric graph");
     HN_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
     HN_CUDA(cudaMemsetAsync(inF.get(), 0, (size_t)m, s));
+    DevBuf<int32_t> H((size_t)m, s);   // heavy edges (support, then each peel round)
     HN_LAUNCH(k_kt_support, grid_for(g, m, kB), kB, 0, s, off.get(), adj.get(), src.get(), m,
-              sup.get(), alive.get(), cnt);
+              sup.get(), alive.get(), cnt, H.get(), cnt + 3);
+    HN_LAUNCH(k_kt_support_heavy, grid_for(g, m, 256), 256, 0, s, off.get(), adj.get(),
+              src.get(), (const int32_t*)H.get(), (const int*)(cnt + 3), sup.get());
     // truss numbers start at 2 (0x02020202 per int is not 2; fill by kernel-free memset of 0
     // then write on retirement: every edge is retired exactly once)
     read_scalars(g, 1);
@@ -307,7 +355,6 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
     int* nheavy = cnt + 3;  // frontier edges left to k_kt_peel_heavy (right after nNF)
     int* nL = cnt + 4;      // alive-list length
     int* minsup = cnt + 5;  // smallest support on the alive list
-    DevBuf<int32_t> H((size_t)m, s);
     // the frontier of each K scans only the alive edges, and K jumps to the
     // first value that peels anything (min support + 3): R-MAT graphs reach
     // max K in the hundreds while most edges leave at small K
