@@ -129,6 +129,15 @@ __global__ void k_kt_support_heavy(const long long* __restrict__ off,
     }
 }
 
+// Positions of the current lists whose (canonical) edge is still alive.
+__global__ void k_kt_live_pos(const int32_t* __restrict__ canon, long long n,
+                              const unsigned char* __restrict__ alive,
+                              int32_t* __restrict__ flag) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x)
+        flag[p] = alive[canon[p]] ? 1 : 0;
+}
+
 // Frontier of round K: alive edges of the list L with support < K - 2.
 __global__ void k_kt_frontier(const int32_t* __restrict__ L, int nL, int K,
                               const int32_t* __restrict__ sup,
@@ -200,6 +209,7 @@ __device__ __forceinline__ void kt_triangle(int e, int e1, int e2, int K,
 // core's hub-hub edges would otherwise run one long intersection per thread.
 __global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __restrict__ adj,
                           const int32_t* __restrict__ src, const int32_t* __restrict__ canon,
+                          const int32_t* __restrict__ eadj,
                           const int32_t* __restrict__ F, int nF, int K,
                           const unsigned char* __restrict__ alive,
                           const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
@@ -212,7 +222,7 @@ __global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __re
         int e = 0;
         if (f < nF) {
             e = F[f];
-            int u = src[e], v = adj[e];
+            int u = src[e], v = eadj[e];
             long long au = off[u], la = off[u + 1] - au;
             long long bv = off[v], lb = off[v + 1] - bv;
             bool swapped = la > lb;
@@ -241,6 +251,7 @@ __global__ void k_kt_peel_heavy(const long long* __restrict__ off,
                                 const int32_t* __restrict__ adj,
                                 const int32_t* __restrict__ src,
                                 const int32_t* __restrict__ canon,
+                                const int32_t* __restrict__ eadj,
                                 const int32_t* __restrict__ heavy, const int* __restrict__ nheavy,
                                 int K, const unsigned char* __restrict__ alive,
                                 const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
@@ -251,7 +262,7 @@ __global__ void k_kt_peel_heavy(const long long* __restrict__ off,
     for (long long h = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh;
          h += warps) {
         const int e = heavy[h];
-        const int u = src[e], v = adj[e];
+        const int u = src[e], v = eadj[e];
         const long long au = off[u], la = off[u + 1] - au;
         const long long bv = off[v], lb = off[v + 1] - bv;
         const bool swapped = la > lb;
@@ -371,6 +382,59 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         return ((int*)g->h_scalar)[4];
     };
     int n_alive = compact(nullptr, m);
+    // the peel intersects adjacency lists; once most edges are gone the
+    // lists are rebuilt from the alive edges only (hubs of the dense core
+    // otherwise keep their full original lists)
+    long long* loff = off.get();
+    int32_t* ladj = adj.get();
+    int32_t* lcanon = canon.get();
+    long long lm = m;
+    DevBuf<long long> coff;
+    DevBuf<int32_t> cadj, ccanon, cflag;
+    auto shrink_lists = [&]() {
+        const long long keep = 2LL * n_alive;
+        if (keep * 2 > lm) return;
+        cflag.alloc((size_t)lm, s);
+        HN_LAUNCH(k_kt_live_pos, grid_for(g, lm, kB), kB, 0, s, (const int32_t*)lcanon, lm,
+                  alive.get(), cflag.get());
+        DevBuf<long long> noff((size_t)nV + 1, s);
+        {
+            size_t tb = 0;
+            HN_CUDA(cub::DeviceSegmentedReduce::Sum(nullptr, tb, cflag.get(), noff.get(), nV, loff,
+                                                    loff + 1, s));
+            DevBuf<char> tmp(tb, s);
+            HN_CUDA(cub::DeviceSegmentedReduce::Sum(tmp.get(), tb, cflag.get(), noff.get(), nV,
+                                                    loff, loff + 1, s));
+            HN_CUDA(cudaMemsetAsync(noff.get() + nV, 0, sizeof(long long), s));
+            tb = 0;
+            HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, noff.get(), noff.get(), nV + 1, s));
+            DevBuf<char> tmp2(tb, s);
+            HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.get(), tb, noff.get(), noff.get(), nV + 1,
+                                                  s));
+            count_launch(2);
+        }
+        DevBuf<int32_t> nadj((size_t)keep + 1, s), ncanon((size_t)keep + 1, s);
+        {
+            int* nsel = cnt + 6;
+            size_t tb = 0;
+            HN_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, ladj, cflag.get(), nadj.get(), nsel,
+                                               lm, s));
+            DevBuf<char> tmp(tb, s);
+            HN_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, ladj, cflag.get(), nadj.get(), nsel,
+                                               lm, s));
+            HN_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, lcanon, cflag.get(), ncanon.get(),
+                                               nsel, lm, s));
+            count_launch(2);
+        }
+        coff = std::move(noff);
+        cadj = std::move(nadj);
+        ccanon = std::move(ncanon);
+        loff = coff.get();
+        ladj = cadj.get();
+        lcanon = ccanon.get();
+        lm = keep;
+        cflag.release();
+    };
     while (true) {
         if (remaining <= 0) { K--; break; }
         const int ms = ((int*)g->h_scalar)[5];
@@ -383,11 +447,13 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         int nf = ((int*)g->h_scalar)[0];
         while (nf > 0) {
             HN_CUDA(cudaMemsetAsync(nNF, 0, 2 * sizeof(int), s));   // nNF, nheavy
-            HN_LAUNCH(k_kt_peel, grid_for(g, nf, 128), 128, 0, s, off.get(), adj.get(), src.get(),
-                      canon.get(), F.get(), nf, K, alive.get(), inF.get(), sup.get(), NF.get(),
-                      nNF, H.get(), nheavy);
-            HN_LAUNCH(k_kt_peel_heavy, grid_for(g, (long long)nf * 32, 256), 256, 0, s, off.get(),
-                      adj.get(), src.get(), canon.get(), (const int32_t*)H.get(),
+            HN_LAUNCH(k_kt_peel, grid_for(g, nf, 128), 128, 0, s, (const long long*)loff,
+                      (const int32_t*)ladj, src.get(), (const int32_t*)lcanon,
+                      (const int32_t*)adj.get(), F.get(), nf, K, alive.get(), inF.get(), sup.get(),
+                      NF.get(), nNF, H.get(), nheavy);
+            HN_LAUNCH(k_kt_peel_heavy, grid_for(g, (long long)nf * 32, 256), 256, 0, s,
+                      (const long long*)loff, (const int32_t*)ladj, src.get(),
+                      (const int32_t*)lcanon, (const int32_t*)adj.get(), (const int32_t*)H.get(),
                       (const int*)nheavy, K, alive.get(), inF.get(), sup.get(), NF.get(), nNF);
             HN_LAUNCH(k_kt_retire, grid_for(g, nf, kB), kB, 0, s, F.get(), nf, NF.get(), nNF, K,
                       alive.get(), inF.get(), truss.get());
@@ -400,6 +466,7 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         }
         if (remaining <= 0) { K--; break; }
         n_alive = compact(L.get(), n_alive);
+        shrink_lists();
         K++;
     }
     if (d_edge_truss)
