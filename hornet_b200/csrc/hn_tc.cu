@@ -129,6 +129,19 @@ __device__ __forceinline__ void tab_insert(int* tab, int bits, int w) {
     }
 }
 
+// Filter bit of w for a table of 2^bits slots: the top bits+3 bits of the
+// same product, so a filter of 8 bits per slot (2^(bits-2) words) rejects
+// most absent values with one shared-memory load and no probe loop.
+__device__ __forceinline__ unsigned tc_fbit(int w, int bits) {
+    return ((unsigned)w * 2654435761u) >> (32 - (bits + 3));
+}
+
+__device__ __forceinline__ void tab_insert_f(int* tab, unsigned* filt, int bits, int w) {
+    tab_insert(tab, bits, w);
+    const unsigned f = tc_fbit(w, bits);
+    atomicOr(filt + (f >> 5), 1u << (f & 31));
+}
+
 __device__ __forceinline__ bool tab_find(const int* tab, int bits, int w) {
     unsigned mask = (1u << bits) - 1;
     unsigned h = tc_hash(w, bits);
@@ -153,7 +166,8 @@ struct TcView {
 // (one search over the 33-entry prefix per lane per group).
 template <bool PER_VERTEX>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
-    int u, const int32_t* __restrict__ L, int du, const int* tab, int bits, int cand_begin,
+    int u, const int32_t* __restrict__ L, int du, const int* tab, const unsigned* filt, int bits,
+    int cand_begin,
     int cand_step, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
     int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
@@ -206,7 +220,8 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                 int w = base[k - start];
                 bool hit;
                 if (tab) {
-                    hit = tab_find(tab, bits, w);
+                    const unsigned f = tc_fbit(w, bits);
+                    hit = ((filt[f >> 5] >> (f & 31)) & 1u) && tab_find(tab, bits, w);
                 } else {
                     int lo = 0, hi = du;
                     while (lo < hi) {
@@ -237,6 +252,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
           int32_t* __restrict__ big, int warp_cap, int chunk) {
     __shared__ int s_tab[kTcWarps][kWarpTab];
+    __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
@@ -260,12 +276,14 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             }
             int bits = 32 - __clz(2 * du - 1);   // table of 2^bits >= 2*du slots
             if (bits < 5) bits = 5;
+            unsigned* filt = s_filt[warp];
             for (int i = lane; i < (1 << bits); i += 32) tab[i] = -1;
+            for (int i = lane; i < (1 << (bits - 2)); i += 32) filt[i] = 0u;
             __syncwarp();
-            for (int i = lane; i < du; i += 32) tab_insert(tab, bits, g.fwd[ub + i]);
+            for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
             __syncwarp();
-            mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, bits, 0, 1, g, s_pref[warp],
-                                               s_vb[warp], s_v[warp], per_vertex);
+            mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, 0, 1, g,
+                                               s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
             __syncwarp();
         }
     }
@@ -298,16 +316,20 @@ k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
         long long ub = g.offp[u];
         int du = (int)(g.offp[u + 1] - ub);
         const int* tab = nullptr;
+        unsigned* filt = (unsigned*)(s_dyn + 2 * kCtaCap);
         int bits = 0;
         if (du <= kCtaCap) {
             bits = 32 - __clz(2 * du - 1);
+            if (bits < 5) bits = 5;
             for (int j = threadIdx.x; j < (1 << bits); j += blockDim.x) s_dyn[j] = -1;
+            for (int j = threadIdx.x; j < (1 << (bits - 2)); j += blockDim.x) filt[j] = 0u;
             __syncthreads();
-            for (int j = threadIdx.x; j < du; j += blockDim.x) tab_insert(s_dyn, bits, g.fwd[ub + j]);
+            for (int j = threadIdx.x; j < du; j += blockDim.x)
+                tab_insert_f(s_dyn, filt, bits, g.fwd[ub + j]);
             tab = s_dyn;
         }
         __syncthreads();
-        mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, bits, warp, kTcWarps, g,
+        mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, warp, kTcWarps, g,
                                            s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
         __syncthreads();
     }
@@ -358,7 +380,8 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
     const int warp_cap = (int)knob(kKnobTcWarpCap);
     const int chunk = (int)knob(kKnobTcChunk);
-    const size_t dyn = (size_t)2 * kCtaCap * sizeof(int);   // hash table of the CTA path
+    // hash table of the CTA path + its filter (8 bits per slot)
+    const size_t dyn = (size_t)2 * kCtaCap * sizeof(int) + (size_t)2 * kCtaCap / 4 * sizeof(unsigned);
     static bool attr_set = false;
     if (!attr_set) {
         HN_CUDA(cudaFuncSetAttribute(k_tc_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
