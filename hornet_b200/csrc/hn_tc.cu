@@ -211,9 +211,18 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
             int start = s_pref[a], end = s_pref[a + 1];
             const int32_t* base = g.fwd + s_vb[a];
             for (int k = lane; k < T; k += 32) {
-                while (k >= end) {   // next non-empty candidate
+                if (k >= end) {   // the candidate holding pair k
                     a++;
-                    start = end;
+                    if (s_pref[a + 1] <= k) {
+                        // short lists: k skipped several candidates; search
+                        // s_pref[a..32] (s_pref[32] = T > k) instead of walking
+                        int hi = 32;
+                        while (hi - a > 1) {
+                            int mid = (a + hi) >> 1;
+                            if (s_pref[mid] <= k) a = mid; else hi = mid;
+                        }
+                    }
+                    start = s_pref[a];
                     end = s_pref[a + 1];
                     base = g.fwd + s_vb[a];
                 }
