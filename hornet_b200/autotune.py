@@ -39,7 +39,7 @@ SPACES: Dict[str, Dict[str, List[int]]] = {
     "bfs_do": {"bfs.do_alpha": [4, 8, 14, 24, 48], "bfs.do_beta": [8, 24, 64, 256]},
     "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8]},
     "tc": {"tc.warp_cap": [64, 128, 256, 512], "tc.chunk": [4, 16, 64],
-           "tc.warp_ctas_per_sm": [4, 8, 12, 16]},
+           "tc.warp_ctas_per_sm": [4, 8, 12, 16], "tc.narrow_min": [0, 8, 32, 128]},
 }
 
 DEFAULT_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")

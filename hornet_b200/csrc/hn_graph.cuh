@@ -126,6 +126,7 @@ enum Knob {
     kKnobBfsDynamicChunks,
     kKnobBfsWarpStrided,
     kKnobBfsHostLevels,
+    kKnobTcNarrowMin,
     kNumKnobs
 };
 long long knob(Knob k);

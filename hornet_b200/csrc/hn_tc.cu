@@ -167,7 +167,7 @@ struct TcView {
 template <bool PER_VERTEX>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int* tab, const unsigned* filt, int bits,
-    int cand_begin,
+    int narrow_min, int cand_begin,
     int cand_step, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
     int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
@@ -182,12 +182,19 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
             long long b0 = g.offp[v], b1 = g.offp[v + 1];
             const int32_t* lst = g.fwd + b0;
             int n = (int)(b1 - b0);
-            // [first element >= lo_w, first element > hi_w)
+            // [first element >= lo_w, first element > hi_w); lists of at most
+            // narrow_min entries are probed whole (two dependent searches
+            // cost more than the few extra filter probes)
             int lo = 0, hi = n;
-            while (lo < hi) { int m = (lo + hi) >> 1; if (lst[m] < lo_w) lo = m + 1; else hi = m; }
-            int s0 = lo;
-            hi = n;
-            while (lo < hi) { int m = (lo + hi) >> 1; if (lst[m] <= hi_w) lo = m + 1; else hi = m; }
+            int s0 = 0;
+            if (n > narrow_min) {
+                while (lo < hi) { int m = (lo + hi) >> 1; if (lst[m] < lo_w) lo = m + 1; else hi = m; }
+                s0 = lo;
+                hi = n;
+                while (lo < hi) { int m = (lo + hi) >> 1; if (lst[m] <= hi_w) lo = m + 1; else hi = m; }
+            } else {
+                lo = n;
+            }
             xb = b0 + s0;
             dx = lo - s0;
         }
@@ -259,7 +266,7 @@ __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
-          int32_t* __restrict__ big, int warp_cap, int chunk) {
+          int32_t* __restrict__ big, int warp_cap, int chunk, int narrow_min) {
     __shared__ int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     __shared__ int s_pref[kTcWarps][33];
@@ -291,7 +298,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             __syncwarp();
             for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
             __syncwarp();
-            mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, 0, 1, g,
+            mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, narrow_min, 0, 1, g,
                                                s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
             __syncwarp();
         }
@@ -311,7 +318,7 @@ template <bool PER_VERTEX>
 __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
-         const int32_t* __restrict__ big) {
+         const int32_t* __restrict__ big, int narrow_min) {
     extern __shared__ int s_dyn[];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
@@ -338,7 +345,8 @@ k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
             tab = s_dyn;
         }
         __syncthreads();
-        mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, warp, kTcWarps, g,
+        mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, narrow_min, warp,
+                                           kTcWarps, g,
                                            s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
         __syncthreads();
     }
@@ -389,6 +397,7 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
     const int warp_cap = (int)knob(kKnobTcWarpCap);
     const int chunk = (int)knob(kKnobTcChunk);
+    const int narrow_min = (int)knob(kKnobTcNarrowMin);
     // hash table of the CTA path + its filter (8 bits per slot)
     const size_t dyn = (size_t)2 * kCtaCap * sizeof(int) + (size_t)2 * kCtaCap / 4 * sizeof(unsigned);
     static bool attr_set = false;
@@ -404,14 +413,15 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     if (d_per_vertex) {
         HN_CUDA(cudaMemsetAsync(d_per_vertex, 0, sizeof(unsigned long long) * g->nV, s));
         HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, view, g->nV, d_per_vertex, d_total,
-                  counters, big.get(), warp_cap, chunk);
+                  counters, big.get(), warp_cap, chunk, narrow_min);
         HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, view, d_per_vertex, d_total,
-                  counters, big.get());
+                  counters, big.get(), narrow_min);
     } else {
         HN_LAUNCH(k_tc_warp<false>, gw, kTcWarps * 32, 0, s, view, g->nV,
-                  (unsigned long long*)nullptr, d_total, counters, big.get(), warp_cap, chunk);
+                  (unsigned long long*)nullptr, d_total, counters, big.get(), warp_cap, chunk,
+                  narrow_min);
         HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, view,
-                  (unsigned long long*)nullptr, d_total, counters, big.get());
+                  (unsigned long long*)nullptr, d_total, counters, big.get(), narrow_min);
     }
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];

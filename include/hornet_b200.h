@@ -101,6 +101,8 @@ int hn_profile_report(char* buf, int64_t len);
  *   tc.warp_cap         oriented-degree bin boundary between the warp-per-
  *                       vertex and CTA-per-vertex counting kernels (32..512, 512)
  *   tc.chunk            vertices handed to a warp per atomic (1..256, 16)
+ *   tc.narrow_min       candidate lists longer than this are first narrowed
+ *                       to the [min, max] of N+(u) by two searches (0..1024, 0)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)
  *   bfs.dynamic_chunks  1: BFS CTAs take frontier chunks from a counter
  *                       instead of round-robin (0..1, 0)

@@ -350,6 +350,7 @@ def test_tc_local(name):
 @pytest.mark.parametrize("knobs", [
     {"tc.warp_cap": 32, "tc.chunk": 1, "tc.warp_ctas_per_sm": 1},
     {"tc.warp_cap": 64, "tc.chunk": 256, "tc.warp_ctas_per_sm": 16},
+    {"tc.narrow_min": 1024, "tc.warp_cap": 128},
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
     {"bfs.warp_strided": 1},
