@@ -105,6 +105,7 @@ _SIGNATURES = {
     "hn_bfs_batch": [_P, _P, _P, _I32, _I32, _P, _INT, _P],
     "hn_tc": [_P, _P, _INT, _P],
     "hn_tc_local": [_P, _P, _I32, _P, _INT],
+    "hn_tc_owner": [_P, _P, _INT, _P],
     "hn_update_coalesced": [_P, _I64, _P, _P, _P, _INT, _P, _P],
     "hn_insert_count_triangles": [_P, _P, _P, _P],
     "hn_ktruss_keep": [_P, _I32, _P, _P],

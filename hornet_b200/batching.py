@@ -12,9 +12,9 @@ the same per-graph results:
   with `sources_per_graph` slots computes every (graph, source) pair; the
   graphs are disjoint, so a slot's distances inside graph i are graph i's
   own BFS from its source j.
-* Triangles: the union's per-vertex counts summed over each graph's
-  vertex range (every triangle lies inside one graph and is credited to
-  each of its three vertices, hence the division by 3).
+* Triangles: the union's owner counts (hn_tc_owner: each triangle credited
+  once, to its lowest vertex in the degree orientation) summed over each
+  graph's vertex range; every triangle lies inside one graph.
 """
 from __future__ import annotations
 
@@ -60,13 +60,15 @@ class GraphBatch:
 
     def triangles(self, per_vertex):
         """Per-graph triangle counts (device int64 tensor [n_graphs]);
-        per_vertex is a device int64 scratch tensor [nV]."""
+        per_vertex is a device int64 scratch tensor [nV] that receives the
+        owner counts (each triangle credited once, to a vertex of its own
+        graph)."""
         import torch
         total = ctypes.c_uint64()
-        _check(lib().hn_tc(self.hornet.handle, ctypes.c_void_p(per_vertex.data_ptr()),
-                           HN_MEM_DEVICE, ctypes.byref(total)))
+        _check(lib().hn_tc_owner(self.hornet.handle, ctypes.c_void_p(per_vertex.data_ptr()),
+                                 HN_MEM_DEVICE, ctypes.byref(total)))
         csum = torch.cumsum(per_vertex, 0)
         ends = torch.as_tensor(self.bases + self.sizes - 1, device=per_vertex.device)
         at_end = csum[ends]
         prev = torch.cat([at_end.new_zeros(1), at_end[:-1]])
-        return (at_end - prev) // 3, total.value
+        return at_end - prev, total.value

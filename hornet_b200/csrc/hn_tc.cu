@@ -153,6 +153,14 @@ __device__ __forceinline__ bool tab_find(const int* tab, int bits, int w) {
     }
 }
 
+// Owner credit: the warp's triangles found from u, added to counts[u] once
+// (each triangle is found once, from its lowest vertex in the orientation).
+__device__ __forceinline__ void tc_credit_owner(unsigned long long* counts, int u,
+                                                unsigned long long c) {
+    for (int o = 16; o; o >>= 1) c += __shfl_down_sync(0xFFFFFFFFu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(counts + u, c);
+}
+
 struct TcView {
     const long long* offp;   // oriented offsets
     const int32_t* fwd;      // oriented lists
@@ -164,7 +172,7 @@ struct TcView {
 // lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
 // searches, then the group's pairs are dealt round-robin to the lanes
 // (one search over the 33-entry prefix per lane per group).
-template <bool PER_VERTEX>
+template <int MODE>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int* tab, const unsigned* filt, int bits,
     int narrow_min, int cand_begin,
@@ -248,7 +256,7 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                 }
                 if (hit) {
                     cnt++;
-                    if (PER_VERTEX) {
+                    if (MODE == 1) {
                         atomicAdd(per_vertex + w, 1ull);
                         atomicAdd(per_vertex + u, 1ull);
                         atomicAdd(per_vertex + s_v[a], 1ull);
@@ -261,7 +269,7 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
     return cnt;
 }
 
-template <bool PER_VERTEX>
+template <int MODE>
 __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
@@ -298,8 +306,11 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             __syncwarp();
             for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
             __syncwarp();
-            mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, narrow_min, 0, 1, g,
-                                               s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
+            const unsigned long long cu = tc_vertex_warp<MODE>(u, g.fwd + ub, du, tab, filt, bits,
+                                                               narrow_min, 0, 1, g, s_pref[warp],
+                                                               s_vb[warp], s_v[warp], per_vertex);
+            mine += cu;
+            if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
             __syncwarp();
         }
     }
@@ -314,7 +325,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
 }
 
 // Listed vertices (d+(u) > warp_cap): one CTA each.
-template <bool PER_VERTEX>
+template <int MODE>
 __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
@@ -345,9 +356,12 @@ k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
             tab = s_dyn;
         }
         __syncthreads();
-        mine += tc_vertex_warp<PER_VERTEX>(u, g.fwd + ub, du, tab, filt, bits, narrow_min, warp,
-                                           kTcWarps, g,
-                                           s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
+        const unsigned long long cu = tc_vertex_warp<MODE>(u, g.fwd + ub, du, tab, filt, bits,
+                                                           narrow_min, warp, kTcWarps, g,
+                                                           s_pref[warp], s_vb[warp], s_v[warp],
+                                                           per_vertex);
+        mine += cu;
+        if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
         __syncthreads();
     }
     for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
@@ -387,42 +401,48 @@ void build_oriented(hn_graph* g, Oriented& o) {
               o.fwd.get(), o.offp.get(), splits.get(), (long long)splits.n - 1);
 }
 
-unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_per_vertex) {
+// mode 0: total only; 1: per-vertex counts (each triangle credited to its
+// three vertices); 2: owner counts (each triangle credited once, to its
+// lowest vertex in the degree orientation).
+template <int MODE>
+void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_counts,
+                     unsigned long long* d_total, int* counters, int32_t* big, size_t dyn) {
+    cudaStream_t s = g->stream;
+    const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
+    const long long gc = (long long)g->info.sms;
+    const int warp_cap = (int)knob(kKnobTcWarpCap);
+    const int chunk = (int)knob(kKnobTcChunk);
+    const int narrow_min = (int)knob(kKnobTcNarrowMin);
+    static bool attr_set = false;   // one attribute per instantiation
+    if (!attr_set) {
+        HN_CUDA(cudaFuncSetAttribute(k_tc_cta<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)dyn));
+        attr_set = true;
+    }
+    HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, 0, s, view, g->nV, d_counts, d_total, counters,
+              big, warp_cap, chunk, narrow_min);
+    HN_LAUNCH(k_tc_cta<MODE>, gc, kTcWarps * 32, dyn, s, view, d_counts, d_total, counters, big,
+              narrow_min);
+}
+
+unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_counts,
+                                   int mode) {
     cudaStream_t s = g->stream;
     unsigned long long* d_total = (unsigned long long*)g->d_scalar;
     HN_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
     int* counters = (int*)(g->d_scalar + 1);  // next vertex, big-list size
     HN_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(int), s));
     DevBuf<int32_t> big((size_t)g->nV + 1, s);
-    const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
-    const int warp_cap = (int)knob(kKnobTcWarpCap);
-    const int chunk = (int)knob(kKnobTcChunk);
-    const int narrow_min = (int)knob(kKnobTcNarrowMin);
     // hash table of the CTA path + its filter (8 bits per slot)
     const size_t dyn = (size_t)2 * kCtaCap * sizeof(int) + (size_t)2 * kCtaCap / 4 * sizeof(unsigned);
-    static bool attr_set = false;
-    if (!attr_set) {
-        HN_CUDA(cudaFuncSetAttribute(k_tc_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)dyn));
-        HN_CUDA(cudaFuncSetAttribute(k_tc_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)dyn));
-        attr_set = true;
-    }
-    const long long gc = (long long)g->info.sms;
     TcView view{o.offp.get(), o.fwd.get()};
-    if (d_per_vertex) {
-        HN_CUDA(cudaMemsetAsync(d_per_vertex, 0, sizeof(unsigned long long) * g->nV, s));
-        HN_LAUNCH(k_tc_warp<true>, gw, kTcWarps * 32, 0, s, view, g->nV, d_per_vertex, d_total,
-                  counters, big.get(), warp_cap, chunk, narrow_min);
-        HN_LAUNCH(k_tc_cta<true>, gc, kTcWarps * 32, dyn, s, view, d_per_vertex, d_total,
-                  counters, big.get(), narrow_min);
-    } else {
-        HN_LAUNCH(k_tc_warp<false>, gw, kTcWarps * 32, 0, s, view, g->nV,
-                  (unsigned long long*)nullptr, d_total, counters, big.get(), warp_cap, chunk,
-                  narrow_min);
-        HN_LAUNCH(k_tc_cta<false>, gc, kTcWarps * 32, dyn, s, view,
-                  (unsigned long long*)nullptr, d_total, counters, big.get(), narrow_min);
-    }
+    if (d_counts) HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * g->nV, s));
+    if (!d_counts)
+        launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), dyn);
+    else if (mode == 2)
+        launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), dyn);
+    else
+        launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), dyn);
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];
 }
@@ -456,6 +476,33 @@ extern "C" int hn_tc(hn_graph_t* g, uint64_t* per_vertex, int mem, uint64_t* tot
     unsigned long long t = count_triangles(g, o, d_pv);
     if (per_vertex && mem == HN_MEM_HOST)
         HN_CUDA(cudaMemcpyAsync(per_vertex, d_pv, sizeof(unsigned long long) * g->nV,
+                                cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
+    if (total) *total = t;
+    HN_API_END
+}
+
+extern "C" int hn_tc_owner(hn_graph_t* g, uint64_t* counts, int mem, uint64_t* total) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && counts, "null argument");
+    HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    if (g->nV == 0) {
+        if (total) *total = 0;
+        return HN_OK;
+    }
+    Oriented o;
+    build_oriented(g, o);
+    DevBuf<unsigned long long> buf;
+    unsigned long long* d_c = (unsigned long long*)counts;
+    if (mem == HN_MEM_HOST) {
+        buf.alloc((size_t)g->nV, s);
+        d_c = buf.get();
+    }
+    unsigned long long t = count_triangles(g, o, d_c, 2);
+    if (mem == HN_MEM_HOST)
+        HN_CUDA(cudaMemcpyAsync(counts, d_c, sizeof(unsigned long long) * g->nV,
                                 cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
     if (total) *total = t;

@@ -14,9 +14,11 @@ struct Oriented {
 // Build N+(u) = {v in N(u) : (deg u, u) < (deg v, v)} for every vertex.
 void build_oriented(hn_graph* g, Oriented& o);
 
-// Triangles of the oriented graph; per-vertex counts when d_per_vertex
-// is non-null (device array of nV entries).  Synchronises.
+// Triangles of the oriented graph.  With d_counts (device array of nV
+// entries): mode 1 = per-vertex counts (each triangle credited to its three
+// vertices), mode 2 = owner counts (each triangle credited once, to its
+// lowest vertex in the orientation).  Synchronises.
 unsigned long long count_triangles(hn_graph* g, const Oriented& o,
-                                   unsigned long long* d_per_vertex);
+                                   unsigned long long* d_counts, int mode = 1);
 
 }  // namespace hn

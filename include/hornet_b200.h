@@ -284,6 +284,13 @@ int hn_tc(hn_graph_t* g, uint64_t* per_vertex, int mem, uint64_t* total);
  * simple (no self loops or repeated edges).  seeds and counts are both in
  * `mem`; counts is uint64[k]. */
 int hn_tc_local(hn_graph_t* g, const int32_t* seeds, int32_t k, uint64_t* counts, int mem);
+/* Owner counts: counts[v] = triangles whose lowest vertex in the degree
+ * orientation is v, so each triangle is credited exactly once (sums over
+ * any vertex set that contains whole triangles, e.g. one graph of a
+ * disjoint union, are that set's triangle count).  Cheaper than the
+ * per-vertex form of hn_tc (one atomic per vertex, not three per
+ * triangle).  No reference counterpart; counts is uint64[nV] in `mem`. */
+int hn_tc_owner(hn_graph_t* g, uint64_t* counts, int mem, uint64_t* total);
 
 /* CC::run (hornetsnest/src/Static/ConnectedComponents/CC.cu:133-156).
  * mode HN_CC_MIN_ID or HN_CC_REFERENCE.  labels: int32[nV];
