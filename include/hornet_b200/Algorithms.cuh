@@ -128,6 +128,12 @@ public:
     }
     vid_t getMaxK() const { return _maxK; }
     const std::vector<int32_t>& edgeTruss() const { return _edge_truss; }
+    // KTruss::runForKDynamic (KTruss.cu:270-295): the graph itself keeps
+    // only its K-truss (edges below it are erased through the update path)
+    void runForKDynamic(int max_K) {
+        int64_t removed = 0;
+        ::hornet::hn_check(hn_ktruss_keep(hornet.handle(), max_K, &_maxK, &removed));
+    }
     void release() override {}
     bool validate() override { return true; }
 

@@ -142,6 +142,20 @@ int main(int argc, char** argv) {
     CC cc(hornet_gpu);
     cc.run_min_label();
     std::printf("cc_components %d\n", cc.components());
+    // KTruss on a fresh copy of the (simple, symmetric) input graph:
+    // runForKDynamic(3) keeps exactly the edges whose truss number is >= 3
+    {
+        HornetGPU kg(init);
+        KTruss kt(kg);
+        kt.init();
+        kt.run();
+        long long at_least3 = 0;
+        for (int t : kt.edgeTruss()) at_least3 += t >= 3;
+        const int maxk = kt.getMaxK();
+        kt.runForKDynamic(3);
+        const bool ok = (long long)kg.nE() == at_least3 && kt.getMaxK() == maxk;
+        std::printf("ktruss_max %d\nktruss_keep %s\n", maxk, ok ? "PASSED" : "NOT PASSED");
+    }
     cudaFree(d_dist);
     cudaFree(d_cnt);
     cudaError_t e = cudaDeviceSynchronize();

@@ -41,3 +41,5 @@ def test_shim_reference_style_program():
         np.testing.assert_array_equal(cnt, np.diff(g.off))
         ncomp = int(r.stdout.split("cc_components")[1].split()[0])
         assert ncomp == O.cc_min_label(g)[1]
+        assert "ktruss_keep PASSED" in r.stdout
+        assert int(r.stdout.split("ktruss_max")[1].split()[0]) == O.ktruss(g)[0]
