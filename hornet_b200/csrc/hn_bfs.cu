@@ -91,6 +91,14 @@ struct BfsGraph {
     cudaGraph_t graph[2] = {nullptr, nullptr};      // [0] top-down, [1] direction-optimising
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     unsigned grid = 0;                              // level-kernel CTAs baked in
+    // multi-source calls: pinned per-source states (the next source's state
+    // is staged while the previous BFS runs), a copy stream and events so a
+    // host-bound distance array is copied out while the next BFS runs
+    static constexpr int kRing = 64;
+    BfsState* h_ring = nullptr;                     // pinned, kRing entries
+    cudaStream_t copy = nullptr;
+    cudaEvent_t done[2] = {nullptr, nullptr};       // BFS into buffer b finished
+    cudaEvent_t copied[2] = {nullptr, nullptr};     // buffer b copied to the host
 };
 
 namespace {
@@ -480,6 +488,13 @@ void free_bfs_graph(BfsGraph* bg) {
         if (bg->exec[i]) cudaGraphExecDestroy(bg->exec[i]);
         if (bg->graph[i]) cudaGraphDestroy(bg->graph[i]);
     }
+    if (bg->copy) cudaStreamSynchronize(bg->copy);
+    for (int i = 0; i < 2; i++) {
+        if (bg->done[i]) cudaEventDestroy(bg->done[i]);
+        if (bg->copied[i]) cudaEventDestroy(bg->copied[i]);
+    }
+    if (bg->copy) cudaStreamDestroy(bg->copy);
+    if (bg->h_ring) cudaFreeHost(bg->h_ring);
     if (bg->state) cudaFree(bg->state);
     if (bg->h_state) cudaFreeHost(bg->h_state);
     if (bg->qbuf) cudaFree(bg->qbuf);
@@ -525,13 +540,33 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
             throw Error(HN_ERR_INVALID, "BFS source outside [0, nV)");
     if (g->nE >= 0xFFFFFFFFll) throw Error(HN_ERR_CAPACITY, "BFS needs nE < 2^32");
     BfsGraph& bg = bfs_graph_of(g);
+    if (!bg.h_ring) {
+        HN_CUDA(cudaMallocHost((void**)&bg.h_ring, sizeof(BfsState) * BfsGraph::kRing));
+        HN_CUDA(cudaStreamCreateWithFlags(&bg.copy, cudaStreamNonBlocking));
+        for (int b = 0; b < 2; b++) {
+            HN_CUDA(cudaEventCreateWithFlags(&bg.done[b], cudaEventDisableTiming));
+            HN_CUDA(cudaEventCreateWithFlags(&bg.copied[b], cudaEventDisableTiming));
+        }
+    }
+    const bool host_out = mem == HN_MEM_HOST;
+    // host output: two device buffers; BFS i writes buffer i % 2 while the
+    // copy stream drains buffer (i - 1) % 2 to the host
     DevBuf<int32_t> d_dist;
-    if (mem == HN_MEM_HOST) d_dist.alloc((size_t)nV, s);
+    if (host_out) d_dist.alloc((size_t)2 * nV, s);
+    const bool host_driven = knob(kKnobBfsHostLevels) != 0;
     std::vector<BfsState> snap(k > 0 ? k : 1);
+    HN_CUDA(cudaStreamSynchronize(s));   // the ring's previous contents are read
     for (int i = 0; i < k; i++) {
-        int32_t* out = mem == HN_MEM_HOST ? d_dist.get() : dist + (size_t)i * nV;
-        BfsState& h = *bg.h_state;
-        HN_CUDA(cudaStreamSynchronize(s));  // h_state is reused per source
+        const int r = i % BfsGraph::kRing;
+        if (i > 0 && r == 0) {
+            // ring wrapped: collect the snapshots of the last kRing sources
+            HN_CUDA(cudaStreamSynchronize(s));
+            for (int j = 0; j < BfsGraph::kRing; j++) snap[i - BfsGraph::kRing + j] = bg.h_ring[j];
+        }
+        const int b = i & 1;
+        int32_t* out = host_out ? d_dist.get() + (size_t)b * nV : dist + (size_t)i * nV;
+        if (host_out && i >= 2) HN_CUDA(cudaStreamWaitEvent(s, bg.copied[b], 0));
+        BfsState& h = bg.h_ring[r];
         h = BfsState{};
         h.src = sources[i];
         h.nV = nV;
@@ -549,17 +584,17 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.bitmap = bg.bitmap;
         h.m_total = g->nE;
         h.alpha = (int)knob(kKnobBfsDoAlpha);
+        h.beta = (int)knob(kKnobBfsDoBeta);
         h.dynamic_chunks = (int)knob(kKnobBfsDynamicChunks);
         h.warp_strided = (int)knob(kKnobBfsWarpStrided);
-        h.host_driven = (int)knob(kKnobBfsHostLevels);
+        h.host_driven = host_driven ? 1 : 0;
         h.next_chunk = 0;
-        h.beta = (int)knob(kKnobBfsDoBeta);
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
         // profiling records the whole graph (one init + one expand per
         // level) under the name of its dominant kernel
         cudaEvent_t ev0 = nullptr;
         if (g_profiling) profile_begin(s, &ev0);
-        if (h.host_driven) {
+        if (host_driven) {
             // host-driven levels: one ordinary launch per level (each level
             // can be profiled on its own), one host round trip per level
             k_bfs3_init<<<(unsigned)grid_for(g, nV, 256), 256, 0, s>>>(bg.state);
@@ -583,12 +618,22 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         }
         if (ev0)
             profile_end(direction_optimizing ? "k_bfs_level<true>" : "k_bfs_level<false>", s, ev0);
-        HN_CUDA(cudaMemcpyAsync(bg.h_state, bg.state, sizeof(BfsState), cudaMemcpyDeviceToHost, s));
-        if (mem == HN_MEM_HOST)
+        // the finished state back into this source's ring slot (ordered
+        // before the next source's state upload on the same stream)
+        HN_CUDA(cudaMemcpyAsync(&h, bg.state, sizeof(BfsState), cudaMemcpyDeviceToHost, s));
+        if (host_out) {
+            HN_CUDA(cudaEventRecord(bg.done[b], s));
+            HN_CUDA(cudaStreamWaitEvent(bg.copy, bg.done[b], 0));
             HN_CUDA(cudaMemcpyAsync(dist + (size_t)i * nV, out, sizeof(int32_t) * nV,
-                                    cudaMemcpyDeviceToHost, s));
-        HN_CUDA(cudaStreamSynchronize(s));
-        snap[i] = *bg.h_state;
+                                    cudaMemcpyDeviceToHost, bg.copy));
+            HN_CUDA(cudaEventRecord(bg.copied[b], bg.copy));
+        }
+    }
+    HN_CUDA(cudaStreamSynchronize(s));
+    if (host_out) HN_CUDA(cudaStreamSynchronize(bg.copy));
+    if (k > 0) {
+        const int first = ((k - 1) / BfsGraph::kRing) * BfsGraph::kRing;
+        for (int i = first; i < k; i++) snap[i] = bg.h_ring[i - first];
     }
     if (stats)
         for (int i = 0; i < k; i++) {

@@ -462,3 +462,24 @@ def test_graph_batch_triangles_per_graph():
     tri, total = gb.triangles(pv)
     np.testing.assert_array_equal(tri.cpu().numpy(), [O.tc(gi) for gi in graphs])
     assert total == O.tc(u)
+
+
+def test_bfs_multi_many_sources_host_and_device():
+    """More sources than the library's 64-entry staging ring, host output
+    (copies overlapped with the next BFS) and device output: every row and
+    every per-source statistic equals the oracle's."""
+    import torch
+    g = GRAPHS["rmat12_nonpow2"]()
+    h = build(g)
+    rng = np.random.default_rng(17)
+    srcs = rng.integers(0, g.nV, 150).astype(np.int32)
+    host = torch.empty((150, g.nV), dtype=torch.int32, pin_memory=True).numpy()
+    out, st = H.BfsTopDown(h).run_multi(srcs, out=host)
+    dev = torch.empty((150, g.nV), dtype=torch.int32, device="cuda")
+    _, st_do = H.BfsTopDown(h).run_multi(srcs, out=dev, direction_optimizing=True)
+    for i, s in enumerate(srcs):
+        ref, scanned = O.bfs(g, int(s))
+        np.testing.assert_array_equal(out[i], ref)
+        assert st[i].edges_scanned == scanned and st_do[i].edges_scanned == scanned
+        assert st[i].visited == int((ref != O.INF).sum()) == st_do[i].visited
+    np.testing.assert_array_equal(dev.cpu().numpy(), out)
