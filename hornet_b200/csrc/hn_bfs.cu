@@ -152,16 +152,21 @@ __global__ void k_bfs3_init(BfsState* st) {
 struct BfsSmem {
     unsigned start[kChunk + 2];   // window edge offsets (+ end)
     long long base[kChunk + 1];   // pool index = base + edge
+    int claimed[kChunk];          // vertices claimed in this chunk
+    int nclaimed;
     int nw;
     unsigned next;                // this CTA's next chunk
     unsigned long long wsum[kBfsBlock / 32];
     unsigned long long cbase;
 };
 
-// CTA-wide enqueue of this thread's claimed vertices w[k] (claim[k]):
-// distances written, vertices with edges appended to the next frontier with
-// their adjacency base and edge offset; ONE atomic per call reserves both
-// the queue slots and the edge range.  Must be called by all threads.
+// CTA-wide enqueue of the chunk's claimed vertices.  The claims are first
+// gathered into shared memory (one shared atomic per warp), then each thread
+// takes an equal contiguous share of them: distance written, and vertices
+// with edges appended to the next frontier with their adjacency base and
+// edge offset; ONE atomic per call reserves both the queue slots and the
+// edge range.  Holding no per-claim arrays keeps the kernel's register
+// count, and so its residency, down.  Must be called by all threads.
 __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
                                             const bool (&claim)[kIpt], int level,
                                             const VRec* __restrict__ vtab, int32_t* dist,
@@ -169,26 +174,40 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
                                             long long* nqbase, unsigned* nqoff, int32_t* nchunk,
                                             int& found) {
     const int lane = threadIdx.x & 31;
-    long long roff[kIpt];
-    unsigned rdeg[kIpt];
-    unsigned long long mine = 0;   // (degree sum << 32) | queued count
+    if (threadIdx.x == 0) sm.nclaimed = 0;
+    __syncthreads();
+    {
+        int mine = 0;
 #pragma unroll
-    for (int k = 0; k < kIpt; k++) {
-        rdeg[k] = 0;
-        roff[k] = 0;
-        if (claim[k]) {
-            VRec r = vtab[w[k]];
-            rdeg[k] = (unsigned)r.deg;
-            roff[k] = r.off;
+        for (int k = 0; k < kIpt; k++) mine += claim[k] ? 1 : 0;
+        int incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int x = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += x;
         }
+        const int wtot = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        int wbase = 0;
+        if (lane == 31 && wtot) wbase = atomicAdd(&sm.nclaimed, wtot);
+        wbase = __shfl_sync(0xFFFFFFFFu, wbase, 31);
+        int at = wbase + incl - mine;
+#pragma unroll
+        for (int k = 0; k < kIpt; k++)
+            if (claim[k]) sm.claimed[at++] = w[k];
     }
-#pragma unroll
-    for (int k = 0; k < kIpt; k++) {
-        if (claim[k]) {
-            dist[w[k]] = level;
-            found++;
-            if (rdeg[k]) mine += ((unsigned long long)rdeg[k] << 32) | 1ull;
-        }
+    __syncthreads();
+    const int n = sm.nclaimed;
+    if (n == 0) return;   // uniform: every thread read the same count
+    const int per = (n + kBfsBlock - 1) / kBfsBlock;
+    const int i0 = threadIdx.x * per;
+    const int i1 = i0 + per < n ? i0 + per : n;
+    unsigned long long mine = 0;   // (degree sum << 32) | queued count
+    for (int i = i0; i < i1; i++) {
+        const int v = sm.claimed[i];
+        const int d = vtab[v].deg;
+        dist[v] = level;
+        found++;
+        if (d) mine += ((unsigned long long)d << 32) | 1ull;
     }
     unsigned long long incl = mine;
 #pragma unroll
@@ -215,15 +234,16 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
     unsigned long long at = sm.cbase + sm.wsum[warp] + (incl - mine);
     int pos = (int)(at & 0xFFFFFFFFull);
     unsigned off = (unsigned)(at >> 32);
-#pragma unroll
-    for (int k = 0; k < kIpt; k++) {
-        if (claim[k] && rdeg[k]) {
-            nqv[pos] = w[k];
-            nqbase[pos] = roff[k];
+    for (int i = i0; i < i1; i++) {
+        const int v = sm.claimed[i];
+        const VRec r = vtab[v];   // second read of the record: an L1 hit
+        if (r.deg) {
+            nqv[pos] = v;
+            nqbase[pos] = r.off;
             nqoff[pos] = off;
-            mark_chunks(nchunk, off, rdeg[k], pos);
+            mark_chunks(nchunk, off, (unsigned)r.deg, pos);
             pos++;
-            off += rdeg[k];
+            off += (unsigned)r.deg;
         }
     }
     __syncthreads();
@@ -236,7 +256,7 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
 // Breadth-First Search", SC 2012).  Both produce the next frontier queue, so
 // the direction may change at any level; distances are the same either way.
 template <bool DO>
-__global__ void __launch_bounds__(kBfsBlock, 8)
+__global__ void __launch_bounds__(kBfsBlock, 12)
 k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
     __shared__ BfsSmem sm;
     const int level = st->level;
