@@ -674,6 +674,21 @@ class KTruss(StaticAlgorithm):
     def getMaxK(self) -> int:
         return self.max_k
 
+    def runForK(self, K: int):
+        """KTruss::runForK (KTruss.cu:114-119) + copyOffsetArrayHost: the
+        K-truss of the graph (not modified) as CSR offsets (nV + 1) and the
+        surviving edges (src, dst) in sorted-COO order."""
+        self.run()
+        s, d = self.hornet.getCOO(True)
+        keep = self.edge_truss >= K
+        off = np.zeros(self.hornet.nV() + 1, np.int64)
+        np.add.at(off, s[keep].astype(np.int64) + 1, 1)
+        self.offsets = np.cumsum(off).astype(np.int32)
+        return self.offsets, s[keep], d[keep]
+
+    def copyOffsetArrayHost(self):
+        return self.offsets
+
     def runForKDynamic(self, K: int) -> int:
         """KTruss::runForKDynamic (KTruss.cu:270-295): erase every edge below
         the K-truss from the graph itself (hn_ktruss_keep).  Returns the

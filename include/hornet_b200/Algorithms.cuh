@@ -10,6 +10,7 @@
 #pragma once
 
 #include <cstdint>
+#include <algorithm>
 #include <vector>
 
 #include "Hornet.cuh"
@@ -128,6 +129,24 @@ public:
     }
     vid_t getMaxK() const { return _maxK; }
     const std::vector<int32_t>& edgeTruss() const { return _edge_truss; }
+    // KTruss::runForK (KTruss.cu:114-119): the K-truss of the graph, as the
+    // CSR offsets (nV + 1) of its surviving edges in sorted-COO order
+    // (copyOffsetArrayHost, KTruss.cu:44-47); the graph is not modified
+    void runForK(int K) {
+        run();
+        const int32_t nV = hornet.nV();
+        std::vector<int32_t> src((size_t)hornet.nE()), dst((size_t)hornet.nE());
+        if (!src.empty())
+            ::hornet::hn_check(hn_graph_export_coo(hornet.handle(), 1, src.data(), dst.data(),
+                                                   HN_MEM_HOST));
+        _offsets.assign((size_t)nV + 1, 0);
+        for (size_t e = 0; e < src.size(); e++)
+            if (_edge_truss[e] >= K) _offsets[(size_t)src[e] + 1]++;
+        for (int32_t v = 0; v < nV; v++) _offsets[(size_t)v + 1] += _offsets[(size_t)v];
+    }
+    void copyOffsetArrayHost(vid_t* host_offset_array) const {
+        std::copy(_offsets.begin(), _offsets.end(), host_offset_array);
+    }
     // KTruss::runForKDynamic (KTruss.cu:270-295): the graph itself keeps
     // only its K-truss (edges below it are erased through the update path)
     void runForKDynamic(int max_K) {
@@ -140,6 +159,7 @@ public:
 private:
     int32_t _maxK = 0;
     std::vector<int32_t> _edge_truss;
+    std::vector<int32_t> _offsets;
 };
 
 }  // namespace hornets_nest

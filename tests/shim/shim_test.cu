@@ -152,8 +152,12 @@ int main(int argc, char** argv) {
         long long at_least3 = 0;
         for (int t : kt.edgeTruss()) at_least3 += t >= 3;
         const int maxk = kt.getMaxK();
+        kt.runForK(3);
+        std::vector<int> koff((size_t)nV + 1);
+        kt.copyOffsetArrayHost(koff.data());
+        const bool off_ok = koff[(size_t)nV] == at_least3;
         kt.runForKDynamic(3);
-        const bool ok = (long long)kg.nE() == at_least3 && kt.getMaxK() == maxk;
+        const bool ok = off_ok && (long long)kg.nE() == at_least3 && kt.getMaxK() == maxk;
         std::printf("ktruss_max %d\nktruss_keep %s\n", maxk, ok ? "PASSED" : "NOT PASSED");
     }
     cudaFree(d_dist);

@@ -427,6 +427,13 @@ def test_ktruss_keep_runForKDynamic(K):
     np.testing.assert_array_equal(hd, d[keep])
     # the kept graph is its own K-truss: running again removes nothing
     assert kt.runForKDynamic(K) == 0
+    # runForK on a fresh copy: same surviving edges, graph unchanged
+    h2 = build(g)
+    kt2 = H.KTruss(h2)
+    off, ks, kd = kt2.runForK(K)
+    np.testing.assert_array_equal(ks, s[keep])
+    np.testing.assert_array_equal(kd, d[keep])
+    assert off[-1] == int(keep.sum()) and h2.nE() == g.nE
 
 
 @pytest.mark.parametrize("name", ["rmat10", "er2000"])
