@@ -37,7 +37,8 @@ SPACES: Dict[str, Dict[str, List[int]]] = {
     "bfs": {"bfs.ctas_per_sm": [4, 6, 8, 12, 16], "bfs.dynamic_chunks": [0, 1],
             "bfs.warp_strided": [0, 1]},
     "bfs_do": {"bfs.do_alpha": [4, 8, 14, 24, 48], "bfs.do_beta": [8, 24, 64, 256]},
-    "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8]},
+    "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8],
+              "msbfs.bottom_up": [0, 1]},
     "tc": {"tc.warp_cap": [64, 128, 256, 512], "tc.chunk": [4, 16, 64],
            "tc.warp_ctas_per_sm": [4, 8, 12, 16], "tc.narrow_min": [0, 8, 32, 128]},
 }

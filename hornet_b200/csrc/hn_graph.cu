@@ -51,9 +51,10 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"bfs.warp_strided", 0, 0, 1, false},
     {"bfs.host_levels", 0, 0, 1, false},
     {"tc.narrow_min", 0, 0, 1024, false},
+    {"msbfs.bottom_up", 1, 0, 1, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}};
+    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

@@ -127,6 +127,7 @@ enum Knob {
     kKnobBfsWarpStrided,
     kKnobBfsHostLevels,
     kKnobTcNarrowMin,
+    kKnobMsBottomUp,
     kNumKnobs
 };
 long long knob(Knob k);

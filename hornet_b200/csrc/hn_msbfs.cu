@@ -51,8 +51,13 @@ struct MsState {
     const int32_t* src;
     const int32_t* slot;
     int nsrc;
-    int pad;
+    int mode;                       // 0 top-down (push + apply), 1 bottom-up (apply scans)
     unsigned long long* stat;       // [3*kMaxSlots]: visited, scanned, last level per slot
+    int prev_nq;                    // size of the previous frontier (its fronts are cleared)
+    int bottom_up;                  // bottom-up levels allowed
+    int alpha, beta;                // direction switch thresholds
+    long long m_total;              // edges of the graph
+    unsigned long long all_mask;    // slots that hold at least one source
 };
 
 struct MsGraph {
@@ -160,6 +165,7 @@ __global__ void __launch_bounds__(kSeedBlock) k_ms_seed(MsState* st) {
             v = st->src[j];
             int b = st->slot ? st->slot[j] : j;
             unsigned long long bit = 1ull << b;
+            atomicOr(&st->all_mask, bit);
             unsigned long long old = atomicOr(st->front[0] + v, bit);
             unsigned long long olds = atomicOr(st->seen + v, bit);
             first = old == 0;
@@ -207,6 +213,17 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) k_ms_push(MsState* st) {
     const int nq = (int)(cin & 0xFFFFFFFFull);
     const unsigned total = (unsigned)(cin >> 32);
     const int cur = it & 1;
+    {
+        // the previous frontier's masks are spent: its buffer is the one this
+        // level's apply writes, and bottom-up levels read every vertex's mask
+        const int pn = st->prev_nq;
+        const int32_t* pq = st->q[cur ^ 1];
+        unsigned long long* pf = st->front[cur ^ 1];
+        for (long long i = blockIdx.x * (long long)BLOCK + threadIdx.x; i < pn;
+             i += (long long)gridDim.x * BLOCK)
+            pf[pq[i]] = 0ull;
+    }
+    if (st->mode == 1) return;   // bottom-up level: apply does the work
     const int32_t* q = st->q[cur];
     const long long* qbase = st->qbase[cur];
     const unsigned* qoff = st->qoff[cur];
@@ -301,21 +318,47 @@ __global__ void __launch_bounds__(BLOCK) k_ms_apply(MsState* st, cudaGraphCondit
     unsigned long long* nxt = st->nxt;
     unsigned long long* nfront = st->front[nx];
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < nt; i0 += stride) {
+    const bool bu = st->mode == 1;
+    const unsigned long long* cfront = st->front[nx ^ 1];
+    const unsigned long long all = st->all_mask;
+    const int nq_in = (int)(st->cnt[it % 3] & 0xFFFFFFFFull);
+    const long long n_items = bu ? (long long)nV : nt;
+    for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < n_items; i0 += stride) {
         long long i = i0 + threadIdx.x;
         bool q = false;
         int v = 0;
         VRec r;
         r.deg = 0;
         r.off = 0;
-        if (i < nt) {
+        unsigned long long nw = 0;
+        if (bu && i < n_items) {
+            // bottom-up: v takes, for every slot it still misses, the first
+            // neighbour on that slot's frontier; stops once nothing is missing
+            v = (int)i;
+            unsigned long long todo = all & ~seen[v];
+            if (todo) {
+                r = vtab[v];
+                const int32_t* nb = st->pool + r.off;
+                for (int e = 0; e < r.deg && todo; e++) {
+                    const unsigned long long m = cfront[__ldg(nb + e)] & todo;
+                    nw |= m;
+                    todo &= ~m;
+                }
+                if (nw) {
+                    seen[v] |= nw;
+                    nfront[v] = nw;
+                }
+            }
+        } else if (!bu && i < nt) {
             v = st->touched[i];
             unsigned long long x = nxt[v];
             nxt[v] = 0;
-            unsigned long long nw = x & ~seen[v];
+            nw = x & ~seen[v];
             seen[v] |= nw;
             nfront[v] = nw;
             r = vtab[v];
+        }
+        if (nw) {
             while (nw) {
                 int bb = __ffsll((long long)nw) - 1;
                 nw &= nw - 1;
@@ -354,6 +397,17 @@ __global__ void __launch_bounds__(BLOCK) k_ms_apply(MsState* st, cudaGraphCondit
             st->ticket = 0;
             st->tcnt = 0;
             st->level = level + 1;
+            st->prev_nq = nq_in;
+            if (st->bottom_up) {
+                // bottom-up while the next frontier's edges exceed m/alpha;
+                // back to top-down once it holds fewer than nV/beta vertices
+                const long long mf = (long long)(c >> 32);
+                if (st->mode == 0) {
+                    if (mf * st->alpha > st->m_total) st->mode = 1;
+                } else if ((long long)nn * st->beta < nV) {
+                    st->mode = 0;
+                }
+            }
             cudaGraphSetConditional(cond, (nn > 0 && level < nV) ? 1u : 0u);
         }
     }
@@ -518,6 +572,10 @@ extern "C" int hn_bfs_batch(hn_graph_t* g, const int32_t* sources, const int32_t
     h.slot = slots ? d_slot.get() : nullptr;
     h.nsrc = k;
     h.stat = mg.stat;
+    h.bottom_up = (int)knob(kKnobMsBottomUp);
+    h.alpha = (int)knob(kKnobBfsDoAlpha);
+    h.beta = (int)knob(kKnobBfsDoBeta);
+    h.m_total = g->nE;
     HN_CUDA(cudaMemcpyAsync(mg.state, &h, sizeof(MsState), cudaMemcpyHostToDevice, s));
     cudaEvent_t ev0 = nullptr;
     if (g_profiling) profile_begin(s, &ev0);

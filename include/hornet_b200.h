@@ -103,6 +103,8 @@ int hn_profile_report(char* buf, int64_t len);
  *   tc.chunk            vertices handed to a warp per atomic (1..256, 16)
  *   tc.narrow_min       candidate lists longer than this are first narrowed
  *                       to the [min, max] of N+(u) by two searches (0..1024, 0)
+ *   msbfs.bottom_up     1: batched BFS runs bottom-up levels while the
+ *                       frontier is large (bfs.do_alpha / do_beta switch) (0..1, 1)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)
  *   bfs.dynamic_chunks  1: BFS CTAs take frontier chunks from a counter
  *                       instead of round-robin (0..1, 0)

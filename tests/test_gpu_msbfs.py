@@ -120,8 +120,8 @@ def test_batch_device_output_and_errors():
         H.BfsTopDown(h).run_batch(np.array([g.nV], np.int32))
 
 
-@pytest.mark.parametrize("block,ctas", [(128, 2), (512, 8), (256, 6)])
-def test_batch_block_size_knobs(block, ctas):
+@pytest.mark.parametrize("block,ctas,bu", [(128, 2, 1), (512, 8, 0), (256, 6, 1), (256, 4, 0)])
+def test_batch_block_size_knobs(block, ctas, bu):
     """Every batched-BFS launch shape the autotuner may pick gives the same
     distances (the CUDA graph is rebuilt when a knob changes)."""
     g = T.rmat_graph(11, 16, seed=13)
@@ -131,6 +131,25 @@ def test_batch_block_size_knobs(block, ctas):
     try:
         H.tune_set("msbfs.block", block)
         H.tune_set("msbfs.ctas_per_sm", ctas)
+        H.tune_set("msbfs.bottom_up", bu)
+        out, st = H.BfsTopDown(h).run_batch(srcs)
+        check(out, st, ref, ref_stats)
+    finally:
+        H.tune_reset()
+
+
+@pytest.mark.parametrize("alpha,beta", [(1, 1 << 20), (1 << 20, 1), (14, 24)])
+def test_batch_bottom_up_switching(alpha, beta):
+    """Bottom-up levels from the first level on (alpha 1), never (huge
+    alpha), and the default switch: distances and statistics unchanged."""
+    g = T.rmat_graph(12, 16, seed=23)
+    h = build(g)
+    srcs = np.arange(0, 4096, 97, dtype=np.int32)
+    ref, ref_stats = oracle_slots(g, srcs, range(len(srcs)), len(srcs))
+    try:
+        H.tune_set("msbfs.bottom_up", 1)
+        H.tune_set("bfs.do_alpha", alpha)
+        H.tune_set("bfs.do_beta", beta)
         out, st = H.BfsTopDown(h).run_batch(srcs)
         check(out, st, ref, ref_stats)
     finally:
