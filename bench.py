@@ -844,7 +844,8 @@ def bench_serve(args, H, dev, rank, world):
         for mode in ("per_request", "per_request_do", "batched"):
             h = H.hornet_from_device_arrays(nV, nE, off_d, adj_d, device=dev)
             srv = S.Server(h, batched=mode == "batched",
-                           single_bfs="do" if mode != "per_request" else "td")
+                           single_bfs="do" if mode != "per_request" else "td",
+                           msbfs_min=args.msbfs_min)
             srv.run(warm)                       # CUDA graphs built, read-only
             srv.calls, srv.split_for_memory = 0, 0
             srv.groups = {k: 0 for k in srv.groups}
@@ -927,6 +928,8 @@ def main():
     ap.add_argument("--workload", default="static", choices=["static", "update", "batch", "serve"])
     ap.add_argument("--rates", default="250,500,1000,2000,0")
     ap.add_argument("--requests", type=int, default=1000)
+    ap.add_argument("--msbfs-min", type=int, default=2,
+                    help="serve: smallest run of BFS queries answered by one batched traversal")
     ap.add_argument("--graphs", type=int, default=4096)
     ap.add_argument("--sample-graphs", type=int, default=128)
     ap.add_argument("--scale", type=int, default=0)
