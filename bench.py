@@ -928,7 +928,7 @@ def main():
     ap.add_argument("--workload", default="static", choices=["static", "update", "batch", "serve"])
     ap.add_argument("--rates", default="250,500,1000,2000,0")
     ap.add_argument("--requests", type=int, default=1000)
-    ap.add_argument("--msbfs-min", type=int, default=2,
+    ap.add_argument("--msbfs-min", type=int, default=4,
                     help="serve: smallest run of BFS queries answered by one batched traversal")
     ap.add_argument("--graphs", type=int, default=4096)
     ap.add_argument("--sample-graphs", type=int, default=128)
