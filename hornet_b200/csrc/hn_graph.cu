@@ -12,6 +12,7 @@
 //   3. warp-aggregated per-class ranks place each vertex's block;
 //   4. a merge-path load-balanced copy moves the CSR into the pool.
 #include <cub/cub.cuh>
+#include <cuda.h>
 
 #include <cstdio>
 #include <cstring>
@@ -303,9 +304,173 @@ void check_device_error(hn_graph* g) {
     }
 }
 
+// ---- growable device arrays (CUDA virtual memory management) -------------
+// The driver entry points are fetched through the runtime
+// (cudaGetDriverEntryPoint), so the library does not link the driver
+// library itself.
+struct VmArray {
+    CUdeviceptr base = 0;
+    size_t reserved = 0;   // bytes of address space
+    size_t mapped = 0;     // bytes backed by device memory
+    size_t gran = 0;
+    int device = 0;
+    std::vector<std::pair<CUmemGenericAllocationHandle, size_t>> chunks;
+};
+
+namespace {
+typedef CUresult (*PfnGran)(size_t*, const CUmemAllocationProp*, CUmemAllocationGranularity_flags);
+typedef CUresult (*PfnReserve)(CUdeviceptr*, size_t, size_t, CUdeviceptr, unsigned long long);
+typedef CUresult (*PfnAddrFree)(CUdeviceptr, size_t);
+typedef CUresult (*PfnCreate)(CUmemGenericAllocationHandle*, size_t, const CUmemAllocationProp*,
+                              unsigned long long);
+typedef CUresult (*PfnRelease)(CUmemGenericAllocationHandle);
+typedef CUresult (*PfnMap)(CUdeviceptr, size_t, size_t, CUmemGenericAllocationHandle,
+                           unsigned long long);
+typedef CUresult (*PfnUnmap)(CUdeviceptr, size_t);
+typedef CUresult (*PfnAccess)(CUdeviceptr, size_t, const CUmemAccessDesc*, size_t);
+typedef CUresult (*PfnDeviceGet)(CUdevice*, int);
+typedef CUresult (*PfnDevAttr)(int*, CUdevice_attribute, CUdevice);
+
+struct VmApi {
+    PfnGran gran = nullptr;
+    PfnReserve reserve = nullptr;
+    PfnAddrFree addr_free = nullptr;
+    PfnCreate create = nullptr;
+    PfnRelease release = nullptr;
+    PfnMap map = nullptr;
+    PfnUnmap unmap = nullptr;
+    PfnAccess access = nullptr;
+    PfnDeviceGet device_get = nullptr;
+    PfnDevAttr dev_attr = nullptr;
+    bool ok = false;
+};
+
+const VmApi& vm_api() {
+    static VmApi api;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        auto get = [](const char* name, void** fn) {
+            cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+            return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess &&
+                   q == cudaDriverEntryPointSuccess && *fn != nullptr;
+        };
+        api.ok = get("cuMemGetAllocationGranularity", (void**)&api.gran) &&
+                 get("cuMemAddressReserve", (void**)&api.reserve) &&
+                 get("cuMemAddressFree", (void**)&api.addr_free) &&
+                 get("cuMemCreate", (void**)&api.create) &&
+                 get("cuMemRelease", (void**)&api.release) &&
+                 get("cuMemMap", (void**)&api.map) && get("cuMemUnmap", (void**)&api.unmap) &&
+                 get("cuMemSetAccess", (void**)&api.access) &&
+                 get("cuDeviceGet", (void**)&api.device_get) &&
+                 get("cuDeviceGetAttribute", (void**)&api.dev_attr);
+        (void)cudaGetLastError();
+    });
+    return api;
+}
+
+CUmemAllocationProp vm_prop(int device) {
+    CUmemAllocationProp prop = {};
+    prop.type = CU_MEM_ALLOCATION_TYPE_PINNED;
+    prop.location.type = CU_MEM_LOCATION_TYPE_DEVICE;
+    prop.location.id = device;
+    return prop;
+}
+
+// Whether this device's arrays can grow in place.
+bool vm_usable(int device) {
+    const VmApi& api = vm_api();
+    if (!api.ok) return false;
+    CUdevice dev;
+    int v = 0;
+    if (api.device_get(&dev, device) != CUDA_SUCCESS) return false;
+    if (api.dev_attr(&v, CU_DEVICE_ATTRIBUTE_VIRTUAL_MEMORY_MANAGEMENT_SUPPORTED, dev) !=
+        CUDA_SUCCESS)
+        return false;
+    return v != 0;
+}
+
+void vm_check(CUresult r, const char* what) {
+    if (r == CUDA_SUCCESS) return;
+    throw Error(r == CUDA_ERROR_OUT_OF_MEMORY ? HN_ERR_OOM : HN_ERR_CUDA,
+                std::string(what) + " failed (CUresult " + std::to_string((int)r) + ")");
+}
+
+// Map more memory onto the end of `a` until `bytes` are backed.
+void vm_grow(VmArray& a, size_t bytes) {
+    const VmApi& api = vm_api();
+    CUmemAllocationProp prop = vm_prop(a.device);
+    if (!a.base) {
+        vm_check(api.gran(&a.gran, &prop, CU_MEM_ALLOC_GRANULARITY_RECOMMENDED),
+                 "cuMemGetAllocationGranularity");
+        size_t free_b = 0, total_b = 0;
+        HN_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        // address space for the whole device: growth never needs a move
+        a.reserved = (total_b + a.gran - 1) / a.gran * a.gran;
+        vm_check(api.reserve(&a.base, a.reserved, a.gran, 0, 0), "cuMemAddressReserve");
+    }
+    if (bytes > a.reserved) throw Error(HN_ERR_OOM, "edge pool larger than device memory");
+    while (a.mapped < bytes) {
+        size_t want = bytes - a.mapped;
+        if (want < a.mapped / 4) want = a.mapped / 4;
+        size_t size = (want + a.gran - 1) / a.gran * a.gran;
+        if (size > a.reserved - a.mapped) size = a.reserved - a.mapped;
+        CUmemGenericAllocationHandle h;
+        vm_check(api.create(&h, size, &prop, 0), "cuMemCreate");
+        CUresult r = api.map(a.base + a.mapped, size, 0, h, 0);
+        if (r != CUDA_SUCCESS) {
+            api.release(h);
+            vm_check(r, "cuMemMap");
+        }
+        CUmemAccessDesc desc = {};
+        desc.location = prop.location;
+        desc.flags = CU_MEM_ACCESS_FLAGS_PROT_READWRITE;
+        r = api.access(a.base + a.mapped, size, &desc, 1);
+        a.chunks.push_back({h, size});
+        a.mapped += size;
+        vm_check(r, "cuMemSetAccess");
+    }
+}
+}  // namespace
+
+void vm_free(VmArray* a) {
+    if (!a) return;
+    const VmApi& api = vm_api();
+    size_t at = 0;
+    for (auto& c : a->chunks) {
+        api.unmap(a->base + at, c.second);
+        api.release(c.first);
+        at += c.second;
+    }
+    if (a->base) api.addr_free(a->base, a->reserved);
+    delete a;
+}
+
+// Pool (and weight pool) of at least `slots` entries.  With virtual memory
+// management the arrays grow in place; otherwise by reallocation and copy.
 void ensure_pool(hn_graph* g, unsigned long long slots) {
     if (slots <= g->pool_cap) return;
     unsigned long long ncap = slots + slots / 4 + (1ull << 20);
+    if (!g->pool && !g->vm_pool && vm_usable(g->device)) {
+        g->vm_pool = new VmArray();
+        g->vm_pool->device = g->device;
+        if (g->weighted) {
+            g->vm_wpool = new VmArray();
+            g->vm_wpool->device = g->device;
+        }
+    }
+    if (g->vm_pool) {
+        vm_grow(*g->vm_pool, ncap * sizeof(int32_t));
+        ncap = g->vm_pool->mapped / sizeof(int32_t);
+        g->pool = (int32_t*)g->vm_pool->base;
+        if (g->vm_wpool) {
+            vm_grow(*g->vm_wpool, ncap * sizeof(uint32_t));
+            g->wpool = (uint32_t*)g->vm_wpool->base;
+        }
+        g->pool_cap = ncap;
+        HN_CUDA(cudaMemcpyAsync(&g->alloc->pool_cap, &g->pool_cap, sizeof(unsigned long long),
+                                cudaMemcpyHostToDevice, g->stream));
+        return;
+    }
     int32_t* np = nullptr;
     HN_CUDA(cudaMallocAsync((void**)&np, ncap * sizeof(int32_t), g->stream));
     if (g->pool) {
@@ -328,6 +493,21 @@ void ensure_pool(hn_graph* g, unsigned long long slots) {
     g->pool_cap = ncap;
     HN_CUDA(cudaMemcpyAsync(&g->alloc->pool_cap, &g->pool_cap, sizeof(unsigned long long),
                             cudaMemcpyHostToDevice, g->stream));
+}
+
+void release_pool(hn_graph* g) {
+    if (g->vm_pool || g->vm_wpool) {
+        cudaStreamSynchronize(g->stream);   // no kernel still reads the pool
+        vm_free(g->vm_pool);
+        vm_free(g->vm_wpool);
+        g->vm_pool = g->vm_wpool = nullptr;
+    } else {
+        if (g->pool) cudaFreeAsync(g->pool, g->stream);
+        if (g->wpool) cudaFreeAsync(g->wpool, g->stream);
+    }
+    g->pool = nullptr;
+    g->wpool = nullptr;
+    g->pool_cap = 0;
 }
 
 void ensure_free_list(hn_graph* g, int c, long long count) {
@@ -413,11 +593,7 @@ void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
     for (int c = 0; c < kNumClasses; c++) g->fl_count[c] = 0;
 
     // pool: exact fit plus headroom for updates
-    if (g->pool) HN_CUDA(cudaFreeAsync(g->pool, s));
-    if (g->wpool) HN_CUDA(cudaFreeAsync(g->wpool, s));
-    g->pool = nullptr;
-    g->wpool = nullptr;
-    g->pool_cap = 0;
+    release_pool(g);
     g->weighted = d_w != nullptr;
     ensure_pool(g, used + used / 2 + 1024);
 
@@ -499,8 +675,7 @@ void free_graph_object(hn_graph* g) {
     free_ms_graph(g->ms);
     g->ms = nullptr;
     if (g->vtab) cudaFreeAsync(g->vtab, g->stream);
-    if (g->pool) cudaFreeAsync(g->pool, g->stream);
-    if (g->wpool) cudaFreeAsync(g->wpool, g->stream);
+    release_pool(g);
     if (g->stream) cudaStreamSynchronize(g->stream);
     cudaFree(g->alloc);
     cudaFreeHost(g->h_alloc);

@@ -132,6 +132,12 @@ enum Knob {
 };
 long long knob(Knob k);
 
+// A device array that grows in place: virtual address range reserved once,
+// physical memory mapped onto its end as it grows (no copy, no second
+// copy of the data during growth).  Defined in hn_graph.cu.
+struct VmArray;
+void vm_free(VmArray* a);
+
 struct BfsGraph;
 void free_bfs_graph(BfsGraph* bg);
 struct MsGraph;
@@ -176,6 +182,8 @@ struct hn_graph {
     unsigned long long pool_cap = 0;
     bool weighted = false;         // one 32-bit value per edge slot in wpool
     uint32_t* wpool = nullptr;     // edge weights, parallel to pool (weighted only)
+    hn::VmArray* vm_pool = nullptr;    // backing of pool / wpool when the device
+    hn::VmArray* vm_wpool = nullptr;   // supports virtual memory management
 
     hn::AllocState* alloc = nullptr;      // device
     hn::AllocState* h_alloc = nullptr;    // pinned host mirror
@@ -231,6 +239,9 @@ void check_device_error(hn_graph* g);
 
 // Ensure the pool holds at least `slots` slots (grows by copy).
 void ensure_pool(hn_graph* g, unsigned long long slots);
+// Free the pool and weight pool (synchronises the graph's stream first
+// when they are mapped memory).  Never throws.
+void release_pool(hn_graph* g);
 // Ensure free list c can hold `count` entries.
 void ensure_free_list(hn_graph* g, int c, long long count);
 

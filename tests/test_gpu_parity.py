@@ -490,3 +490,31 @@ def test_bfs_multi_many_sources_host_and_device():
         assert st[i].edges_scanned == scanned and st_do[i].edges_scanned == scanned
         assert st[i].visited == int((ref != O.INF).sum()) == st_do[i].visited
     np.testing.assert_array_equal(dev.cpu().numpy(), out)
+
+
+def test_pool_grows_in_place_under_many_inserts():
+    """A small graph receiving several million edges: the edge pool grows
+    (mapped in place where the device supports it) several times, and the
+    graph stays exactly the oracle's; weighted graphs grow their weights
+    alongside."""
+    g = T.er_graph(5000, 4, seed=3)
+    h = build(g)
+    wg_init = H.HornetInit(g.nV, g.nE, g.off32(), g.adj, sorted_adjacency=True)
+    wg_init.insertEdgeData(np.arange(g.nE, dtype=np.uint32))
+    hw = H.Hornet(wg_init)
+    rng = np.random.default_rng(0)
+    ref = g
+    for it in range(3):
+        bs = rng.integers(0, g.nV, 1_500_000).astype(np.int32)
+        bd = rng.integers(0, g.nV, 1_500_000).astype(np.int32)
+        n = h.insert(H.BatchUpdate(h, bs, bd))          # no dedup: every edge added
+        ref, n_ref = O.insert(ref, bs, bd, 0)
+        assert n == n_ref == len(bs)
+        hw.insert(H.BatchUpdate(hw, bs, bd, np.full(len(bs), (1 << 30) + it, np.uint32)))
+    assert_same_graph(h, ref)
+    s, d, w = hw.getCOOWeighted()
+    np.testing.assert_array_equal(d, ref.coo()[1])
+    # weights of the original edges survive the moves; inserted ones carry
+    # their batch's weight
+    np.testing.assert_array_equal(np.sort(w[w < (1 << 30)]), np.arange(g.nE, dtype=np.uint32))
+    assert set(np.unique(w[w >= (1 << 30)]).tolist()) == {1 << 30, (1 << 30) + 1, (1 << 30) + 2}
