@@ -272,14 +272,15 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
                 s_old[b] = old_off - st0;
                 s_new[b] = seg_new_off[s] - st0;
                 const int k0 = seg_kstart[s], k1 = seg_kstart[s + 1];
-                // a hub's list spans many tiles while its batch list is
-                // short: search only the batch entries that can fall between
-                // this tile's first and last old value
+                // a segment with a long batch list (a hub hit by many
+                // updates) searches only the batch entries that can fall
+                // between this tile's first and last old value; short lists
+                // are searched whole
                 const long long lo_e = st0 > t.item0 ? st0 : t.item0;
                 const long long en = t.ends[b], tend = t.item0 + n;
                 const long long hi_e = en < tend ? en : tend;
-                int blo = 0, bhi = 0;
-                if (lo_e < hi_e && k1 > k0) {
+                int blo = 0, bhi = k1 - k0;
+                if (lo_e < hi_e && k1 - k0 > 8) {   // short batch lists: searched whole
                     const int32_t a_lo = pool[old_off + (lo_e - st0)];
                     const int32_t a_hi = pool[old_off + (hi_e - 1 - st0)];
                     blo = (int)lower_bound_dev(cdst + k0, (long long)(k1 - k0), a_lo);
