@@ -602,7 +602,10 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
     # e2e: pinned host batch arrays copied in every step
     host = [(bs.cpu().pin_memory().numpy(), bd.cpu().pin_memory().numpy(), b)
             for (_, b, bs, bd) in batches]
-    bt = H.BatchUpdate(h, host[0][0][:1], host[0][1][:1])
+    # the batch's device buffers sized once for the largest batch, outside
+    # the timed region (a growing batch would reallocate inside it)
+    big = max(range(len(host)), key=lambda j: host[j][2])
+    bt = H.BatchUpdate(h, host[big][0], host[big][1])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     e_edges = 0
