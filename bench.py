@@ -106,6 +106,15 @@ class ClockSampler:
     def stop(self):
         if self.proc is None:
             return None
+        # a short timed region may end before nvidia-smi's first sample:
+        # wait (at most a second) for one line
+        for _ in range(50):
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.02)
         self.proc.terminate()
         self.proc.wait()
         rows = []
