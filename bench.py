@@ -913,7 +913,11 @@ def run_reference(args):
     K, W = args.steps, args.warmup
     O.ref_time_bfs(g, [int(x) for x in sources[:W]])
     per_step = 1
-    sec, edges = O.ref_time_bfs(g, [int(sources[i % 64]) for i in range(W, W + K * per_step)])
+    # the reference BFS is single-threaded: the host's cores run the steps'
+    # sources concurrently, one process per core (bounded)
+    cores = min(os.cpu_count() or 1, 32)
+    sec, edges, used = O.ref_time_bfs_parallel(
+        g, [int(sources[i % 64]) for i in range(W, W + K * per_step)], cores)
     value = edges / sec / 1e9
     print(json.dumps({
         "impl": "reference", "metric": "BFS GTEPS", "value": round(value, 5), "unit": "GTEPS",
@@ -923,9 +927,11 @@ def run_reference(args):
         "config": {"workload": f"static analytics: R-MAT scale {scale}, edge factor 16, "
                                f"a=.57 b=.19 c=.19, BFS TopDown from 64 seeded non-isolated sources",
                    "nV": g.nV, "nE": g.nE},
-        "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": 1,
+        "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": used,
                          "kind": "reference",
-                         "sample": f"graph::BFS (xlib/src/Graph/BFS.cpp), {per_step} source per step"},
+                         "sample": f"graph::BFS (xlib/src/Graph/BFS.cpp), {per_step} source per "
+                                   f"step, {K} steps over {used} concurrent processes; time = "
+                                   f"the slowest process's BFS phase"},
         "e2e": {"value": round(value, 5), "unit": "GTEPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }))

@@ -206,6 +206,29 @@ def ref_time_bfs(g: Csr, sources) -> Tuple[float, int]:
         return float(out[0]), int(out[1])
 
 
+def ref_time_bfs_parallel(g: Csr, sources, procs: int) -> Tuple[float, int, int]:
+    """graph::BFS::run over `sources` split across `procs` concurrent
+    ref_driver processes (the reference BFS is single-threaded; the host's
+    cores run independent sources).  Returns (seconds of the slowest
+    process's BFS phase, edges visited in total, processes used)."""
+    procs = max(1, min(procs, len(sources)))
+    parts = [list(sources[i::procs]) for i in range(procs)]
+    with tempfile.TemporaryDirectory() as d:
+        cp = os.path.join(d, "g.csr")
+        write_csr(cp, g)
+        ps = [subprocess.Popen([REF_DRIVER, "time_bfs", cp] + [str(int(x)) for x in part],
+                               stdout=subprocess.PIPE, text=True) for part in parts]
+        secs, edges = [], 0
+        for p_ in ps:
+            out, _ = p_.communicate()
+            if p_.returncode != 0:
+                raise RuntimeError("ref_driver failed")
+            a = out.split()
+            secs.append(float(a[0]))
+            edges += int(a[1])
+        return max(secs), edges, procs
+
+
 def ref_read_mtx(path: str, undirected: bool = True, by_degree: bool = False) -> Csr:
     with tempfile.TemporaryDirectory() as d:
         op = os.path.join(d, "o.csr")

@@ -18,6 +18,7 @@
 #include <chrono>
 #include <cstdint>
 #include <cstdio>
+#include <limits>
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -99,7 +100,15 @@ int main(int argc, char** argv) {
             double t0 = now_s();
             bfs.run(src);
             t += now_s() - t0;
-            edges += bfs.visited_edges();
+            // edges scanned = sum of the degrees of the reached vertices,
+            // counted here from the CSR (graph::BFS::visited_edges reads
+            // GraphStd's _out_degrees, which the CSR constructor used here
+            // does not fill)
+            {
+                const int* d = bfs.result();
+                for (int64_t v = 0; v < g.nV; v++)
+                    if (d[v] != std::numeric_limits<int>::max()) edges += g.off[v + 1] - g.off[v];
+            }
             if (!timing) {
                 const int* d = bfs.result();
                 out.insert(out.end(), d, d + g.nV);
