@@ -64,14 +64,39 @@ __device__ __forceinline__ void cc_link(int* __restrict__ parent, int u, int v) 
     }
 }
 
-// 1. link every vertex with its first kSample neighbours
+// 1. link every vertex with its first kSample neighbours.  Each thread
+// takes kVerts vertices per round and issues all their record and
+// neighbour loads before the first link (each link is a chain of dependent
+// parent reads, so the loads of one vertex alone leave the SM waiting).
+constexpr int kVerts = 4;
 __global__ void k_cc_sample(const VRec* __restrict__ vtab, const int32_t* __restrict__ pool,
                             int nV, int* __restrict__ parent) {
-    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
-         v += (long long)gridDim.x * blockDim.x) {
-        VRec r = vtab[v];
-        int k = r.deg < kSample ? r.deg : kSample;
-        for (int i = 0; i < k; i++) cc_link(parent, (int)v, pool[r.off + i]);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long v0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; v0 < nV;
+         v0 += kVerts * stride) {
+        int deg[kVerts];
+        long long off[kVerts];
+#pragma unroll
+        for (int j = 0; j < kVerts; j++) {
+            const long long v = v0 + j * stride;
+            deg[j] = 0;
+            off[j] = 0;
+            if (v < nV) {
+                const VRec r = vtab[v];
+                deg[j] = r.deg < kSample ? r.deg : kSample;
+                off[j] = r.off;
+            }
+        }
+        int nb[kVerts][kSample];
+#pragma unroll
+        for (int j = 0; j < kVerts; j++)
+#pragma unroll
+            for (int i = 0; i < kSample; i++) nb[j][i] = i < deg[j] ? __ldg(pool + off[j] + i) : -1;
+#pragma unroll
+        for (int j = 0; j < kVerts; j++)
+#pragma unroll
+            for (int i = 0; i < kSample; i++)
+                if (nb[j][i] >= 0) cc_link(parent, (int)(v0 + j * stride), nb[j][i]);
     }
 }
 
