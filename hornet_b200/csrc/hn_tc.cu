@@ -114,14 +114,27 @@ constexpr int kTcWarps = 8;
 constexpr int kWarpCap = 512;
 constexpr int kWarpTab = 2 * kWarpCap;
 constexpr int kCtaCap = 16384;
+#ifndef HN_TC_PAIR_ILP
+#define HN_TC_PAIR_ILP 4
+#endif
+constexpr int kPairIlp = HN_TC_PAIR_ILP;   // pairs in flight per lane
 
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
 }
 
+// Linear probing whose home slot is the first of a 4-slot bucket (16
+// bytes): a lookup reads the whole home bucket with one 128-bit load and is
+// decided there unless the bucket is full and does not hold w.  Slots are
+// never emptied, so a key sits before the first empty slot of its probe
+// sequence.
+__device__ __forceinline__ unsigned tab_home(int w, int bits) {
+    return tc_hash(w, bits - 2) << 2;
+}
+
 __device__ __forceinline__ void tab_insert(int* tab, int bits, int w) {
     unsigned mask = (1u << bits) - 1;
-    unsigned h = tc_hash(w, bits);
+    unsigned h = tab_home(w, bits);
     while (true) {
         int old = atomicCAS(tab + h, -1, w);
         if (old == -1 || old == w) return;
@@ -131,7 +144,8 @@ __device__ __forceinline__ void tab_insert(int* tab, int bits, int w) {
 
 // Filter bit of w for a table of 2^bits slots: the top bits+3 bits of the
 // same product, so a filter of 8 bits per slot (2^(bits-2) words) rejects
-// most absent values with one shared-memory load and no probe loop.
+// most absent values with one shared-memory load and no probe loop.  Its
+// word index is the home bucket of w.
 __device__ __forceinline__ unsigned tc_fbit(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - (bits + 3));
 }
@@ -142,15 +156,24 @@ __device__ __forceinline__ void tab_insert_f(int* tab, unsigned* filt, int bits,
     atomicOr(filt + (f >> 5), 1u << (f & 31));
 }
 
-__device__ __forceinline__ bool tab_find(const int* tab, int bits, int w) {
-    unsigned mask = (1u << bits) - 1;
-    unsigned h = tc_hash(w, bits);
-    while (true) {
-        int x = tab[h];
-        if (x == w) return true;
-        if (x == -1) return false;
-        h = (h + 1) & mask;
+// Membership of w, for lanes whose filter bit is set (`maybe`): the home
+// bucket decides unless it is full without w; then the probe continues
+// slot by slot (the table is at most half full, so it meets an empty slot).
+__device__ __forceinline__ bool tab_find(const int* tab, int bits, int w, bool maybe) {
+    const unsigned h = tab_home(w, bits);
+    int4 q = make_int4(-1, -1, -1, -1);
+    if (maybe) q = *reinterpret_cast<const int4*>(tab + h);
+    bool hit = (q.x == w) | (q.y == w) | (q.z == w) | (q.w == w);
+    const bool more = maybe & !hit & (q.x != -1) & (q.y != -1) & (q.z != -1) & (q.w != -1);
+    if (more) {
+        const unsigned mask = (1u << bits) - 1;
+        for (unsigned p = (h + 4) & mask;; p = (p + 1) & mask) {
+            const int x = tab[p];
+            if (x == w) { hit = true; break; }
+            if (x == -1) break;
+        }
     }
+    return hit;
 }
 
 // Owner credit: the warp's triangles found from u, added to counts[u] once
@@ -225,41 +248,58 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
             }
             int start = s_pref[a], end = s_pref[a + 1];
             const int32_t* base = g.fwd + s_vb[a];
-            for (int k = lane; k < T; k += 32) {
-                if (k >= end) {   // the candidate holding pair k
-                    a++;
-                    if (s_pref[a + 1] <= k) {
-                        // short lists: k skipped several candidates; search
-                        // s_pref[a..32] (s_pref[32] = T > k) instead of walking
-                        int hi = 32;
-                        while (hi - a > 1) {
-                            int mid = (a + hi) >> 1;
-                            if (s_pref[mid] <= k) a = mid; else hi = mid;
+            // kPairIlp pairs per lane per step (k, k+32, ...): their loads
+            // of w are issued together, then probed
+            for (int k0 = lane; k0 < T; k0 += 32 * kPairIlp) {
+                int wv[kPairIlp], va[kPairIlp];
+#pragma unroll
+                for (int j = 0; j < kPairIlp; j++) {
+                    const int k = k0 + 32 * j;
+                    wv[j] = -1;
+                    va[j] = a;
+                    if (k < T) {
+                        if (k >= end) {   // the candidate holding pair k
+                            a++;
+                            if (s_pref[a + 1] <= k) {
+                                // short lists: k skipped several candidates;
+                                // search s_pref[a..32] (s_pref[32] = T > k)
+                                int hi = 32;
+                                while (hi - a > 1) {
+                                    int mid = (a + hi) >> 1;
+                                    if (s_pref[mid] <= k) a = mid; else hi = mid;
+                                }
+                            }
+                            start = s_pref[a];
+                            end = s_pref[a + 1];
+                            base = g.fwd + s_vb[a];
                         }
+                        wv[j] = base[k - start];
+                        va[j] = a;
                     }
-                    start = s_pref[a];
-                    end = s_pref[a + 1];
-                    base = g.fwd + s_vb[a];
                 }
-                int w = base[k - start];
-                bool hit;
-                if (tab) {
-                    const unsigned f = tc_fbit(w, bits);
-                    hit = ((filt[f >> 5] >> (f & 31)) & 1u) && tab_find(tab, bits, w);
-                } else {
-                    int lo = 0, hi = du;
-                    while (lo < hi) {
-                        int mid = (lo + hi) >> 1;
-                        if (L[mid] < w) lo = mid + 1; else hi = mid;
+#pragma unroll
+                for (int j = 0; j < kPairIlp; j++) {
+                    const int w = wv[j];
+                    if (w < 0) continue;
+                    bool hit;
+                    if (tab) {
+                        const unsigned f = tc_fbit(w, bits);
+                        hit = tab_find(tab, bits, w, (filt[f >> 5] >> (f & 31)) & 1u);
+                    } else {
+                        int lo = 0, hi = du;
+                        while (lo < hi) {
+                            int mid = (lo + hi) >> 1;
+                            if (L[mid] < w) lo = mid + 1; else hi = mid;
+                        }
+                        hit = lo < du && L[lo] == w;
                     }
-                    hit = lo < du && L[lo] == w;
-                }
-                if (hit) {
-                    cnt++;
-                    if (MODE == 1) {
-                        atomicAdd(per_vertex + w, 1ull);
-                        atomicAdd(per_vertex + u, 1ull);
-                        atomicAdd(per_vertex + s_v[a], 1ull);
+                    if (hit) {
+                        cnt++;
+                        if (MODE == 1) {
+                            atomicAdd(per_vertex + w, 1ull);
+                            atomicAdd(per_vertex + u, 1ull);
+                            atomicAdd(per_vertex + s_v[va[j]], 1ull);
+                        }
                     }
                 }
             }
@@ -275,7 +315,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
           int32_t* __restrict__ big, int warp_cap, int chunk, int narrow_min) {
-    __shared__ int s_tab[kTcWarps][kWarpTab];
+    __shared__ __align__(16) int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
@@ -330,7 +370,7 @@ __global__ void __launch_bounds__(kTcWarps * 32)
 k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
          const int32_t* __restrict__ big, int narrow_min) {
-    extern __shared__ int s_dyn[];
+    extern __shared__ __align__(16) int s_dyn[];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
