@@ -40,7 +40,8 @@ SPACES: Dict[str, Dict[str, List[int]]] = {
     "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8],
               "msbfs.bottom_up": [0, 1]},
     "tc": {"tc.warp_cap": [64, 128, 256, 512], "tc.chunk": [4, 16, 64],
-           "tc.warp_ctas_per_sm": [4, 8, 12, 16], "tc.narrow_min": [0, 8, 32, 128]},
+           "tc.warp_ctas_per_sm": [4, 8, 12, 16], "tc.narrow_min": [0, 8, 32, 128],
+           "tc.mid_cap": [1024, 2048, 4096]},
 }
 
 DEFAULT_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")

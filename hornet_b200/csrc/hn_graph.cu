@@ -53,9 +53,11 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"bfs.host_levels", 0, 0, 1, false},
     {"tc.narrow_min", 0, 0, 1024, false},
     {"msbfs.bottom_up", 1, 0, 1, false},
+    {"tc.mid_cap", 4096, 32, 4096, false},
+    {"tc.cta_table_cap", 16384, 32, 16384, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}};
+    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

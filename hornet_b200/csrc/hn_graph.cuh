@@ -128,6 +128,8 @@ enum Knob {
     kKnobBfsHostLevels,
     kKnobTcNarrowMin,
     kKnobMsBottomUp,
+    kKnobTcMidCap,
+    kKnobTcCtaTableCap,
     kNumKnobs
 };
 long long knob(Knob k);

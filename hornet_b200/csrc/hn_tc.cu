@@ -113,11 +113,19 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
 constexpr int kTcWarps = 8;
 constexpr int kWarpCap = 512;
 constexpr int kWarpTab = 2 * kWarpCap;
-constexpr int kCtaCap = 16384;
+constexpr int kCtaCap = 16384;   // largest tc.cta_table_cap: 160 KB tables
 #ifndef HN_TC_PAIR_ILP
-#define HN_TC_PAIR_ILP 4
+#define HN_TC_PAIR_ILP 8
 #endif
 constexpr int kPairIlp = HN_TC_PAIR_ILP;   // pairs in flight per lane
+
+// Slots of a table for up to `cap` entries: the power of two >= 2*cap that a
+// vertex with d+(u) = cap asks for (and no fewer than 32).
+__host__ __device__ constexpr int tc_table_slots(int cap) {
+    int n = 32;
+    while (n < 2 * cap) n <<= 1;
+    return n;
+}
 
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
@@ -191,20 +199,26 @@ struct TcView {
 
 // One warp: every (v, w) pair of u, w in N+(v) for v in N+(u), probed
 // against N+(u) (hash table `tab`, or binary search of the sorted global
-// list L when tab == nullptr).  Candidates v are taken 32 at a time; each
-// lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
+// list L when tab == nullptr).  Candidates v are taken 32 at a time (in
+// order, or groups claimed from the CTA's counter `s_next` when several
+// warps share u); each lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
 // searches, then the group's pairs are dealt round-robin to the lanes
 // (one search over the 33-entry prefix per lane per group).
 template <int MODE>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int* tab, const unsigned* filt, int bits,
-    int narrow_min, int cand_begin,
-    int cand_step, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
+    int narrow_min, int* s_next, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
     int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
     const int lo_w = L[0], hi_w = L[du - 1];
     unsigned long long cnt = 0;
-    for (int c0 = cand_begin * 32; c0 < du; c0 += cand_step * 32) {
+    auto claim = [&](int c) {
+        if (!s_next) return c + 32;
+        int t = 0;
+        if (lane == 0) t = atomicAdd(s_next, 1);
+        return __shfl_sync(0xFFFFFFFFu, t, 0) * 32;
+    };
+    for (int c0 = claim(-32); c0 < du; c0 = claim(c0)) {
         int idx = c0 + lane;
         int dx = 0, v = 0;
         long long xb = 0;
@@ -310,11 +324,11 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kTcWarps * 32)
+__global__ void __launch_bounds__(kTcWarps * 32, 5)
 k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
-          int* __restrict__ counters /*[0] next vertex, [1] big-list size*/,
-          int32_t* __restrict__ big, int warp_cap, int chunk, int narrow_min) {
+          int* __restrict__ counters /*[0] next vertex, [1] mid, [2] huge list size*/,
+          int32_t* __restrict__ big, int warp_cap, int mid_cap, int chunk, int narrow_min) {
     __shared__ __align__(16) int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     __shared__ int s_pref[kTcWarps][33];
@@ -334,8 +348,11 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             long long ub = g.offp[u];
             int du = (int)(g.offp[u + 1] - ub);
             if (du == 0) continue;
-            if (du > warp_cap) {
-                if (lane == 0) big[atomicAdd(counters + 1, 1)] = u;
+            if (du > warp_cap) {   // mid list from the front, huge list from the back
+                if (lane == 0) {
+                    if (du <= mid_cap) big[atomicAdd(counters + 1, 1)] = u;
+                    else big[nV - 1 - atomicAdd(counters + 2, 1)] = u;
+                }
                 continue;
             }
             int bits = 32 - __clz(2 * du - 1);   // table of 2^bits >= 2*du slots
@@ -347,7 +364,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
             __syncwarp();
             const unsigned long long cu = tc_vertex_warp<MODE>(u, g.fwd + ub, du, tab, filt, bits,
-                                                               narrow_min, 0, 1, g, s_pref[warp],
+                                                               narrow_min, nullptr, g, s_pref[warp],
                                                                s_vb[warp], s_v[warp], per_vertex);
             mine += cu;
             if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
@@ -364,28 +381,37 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
     }
 }
 
-// Listed vertices (d+(u) > warp_cap): one CTA each.
+// Listed vertices (d+(u) > warp_cap): one CTA each, its warps claiming
+// groups of 32 candidates from a shared counter.  Two launches: the mid list
+// (d+(u) <= tc.mid_cap, several CTAs per SM) and the huge list (d+(u) up to
+// tc.cta_table_cap in a table, binary search of N+(u) beyond that).  A
+// table of d entries takes the power of two >= 2*d slots, so the dynamic
+// shared memory holds tc_table_slots(cap) slots and their filter.  The
+// lists share `big`: mid from the front (counters[1] entries), huge from the
+// back (counters[2] entries).
 template <int MODE>
-__global__ void __launch_bounds__(kTcWarps * 32)
-k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
+__global__ void __launch_bounds__(kTcWarps * 32, 4)
+k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
-         const int32_t* __restrict__ big, int narrow_min) {
+         const int32_t* __restrict__ big, int narrow_min, int huge, int cap) {
     extern __shared__ __align__(16) int s_dyn[];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
     __shared__ unsigned long long s_sum[kTcWarps];
+    __shared__ int s_next;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int nbig = counters[1];
+    const int nbig = counters[huge ? 2 : 1];
     unsigned long long mine = 0;
     for (int i = blockIdx.x; i < nbig; i += gridDim.x) {
-        int u = big[i];
+        int u = huge ? big[nV - 1 - i] : big[i];
         long long ub = g.offp[u];
         int du = (int)(g.offp[u + 1] - ub);
         const int* tab = nullptr;
-        unsigned* filt = (unsigned*)(s_dyn + 2 * kCtaCap);
+        unsigned* filt = (unsigned*)(s_dyn + tc_table_slots(cap));
         int bits = 0;
-        if (du <= kCtaCap) {
+        if (threadIdx.x == 0) s_next = 0;
+        if (du <= cap) {
             bits = 32 - __clz(2 * du - 1);
             if (bits < 5) bits = 5;
             for (int j = threadIdx.x; j < (1 << bits); j += blockDim.x) s_dyn[j] = -1;
@@ -397,7 +423,7 @@ k_tc_cta(TcView g, unsigned long long* __restrict__ per_vertex,
         }
         __syncthreads();
         const unsigned long long cu = tc_vertex_warp<MODE>(u, g.fwd + ub, du, tab, filt, bits,
-                                                           narrow_min, warp, kTcWarps, g,
+                                                           narrow_min, &s_next, g,
                                                            s_pref[warp], s_vb[warp], s_v[warp],
                                                            per_vertex);
         mine += cu;
@@ -444,25 +470,39 @@ void build_oriented(hn_graph* g, Oriented& o) {
 // mode 0: total only; 1: per-vertex counts (each triangle credited to its
 // three vertices); 2: owner counts (each triangle credited once, to its
 // lowest vertex in the degree orientation).
+// Dynamic shared memory of a listed-vertex table of up to `cap` entries:
+// its slots and their filter (8 bits per slot).
+constexpr size_t tc_table_bytes(int cap) {
+    return (size_t)tc_table_slots(cap) * sizeof(int) + (size_t)tc_table_slots(cap) / 4 * sizeof(unsigned);
+}
+
 template <int MODE>
 void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_counts,
-                     unsigned long long* d_total, int* counters, int32_t* big, size_t dyn) {
+                     unsigned long long* d_total, int* counters, int32_t* big) {
     cudaStream_t s = g->stream;
     const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
-    const long long gc = (long long)g->info.sms;
     const int warp_cap = (int)knob(kKnobTcWarpCap);
     const int chunk = (int)knob(kKnobTcChunk);
     const int narrow_min = (int)knob(kKnobTcNarrowMin);
+    const int mid_cap = (int)knob(kKnobTcMidCap);
+    const int cta_cap = (int)knob(kKnobTcCtaTableCap);
+    const size_t dyn_mid = tc_table_bytes(mid_cap), dyn_huge = tc_table_bytes(cta_cap);
     static bool attr_set = false;   // one attribute per instantiation
     if (!attr_set) {
         HN_CUDA(cudaFuncSetAttribute(k_tc_cta<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)dyn));
+                                     (int)tc_table_bytes(kCtaCap)));
         attr_set = true;
     }
+    int mid_per_sm = 0;
+    HN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mid_per_sm, k_tc_cta<MODE>,
+                                                          kTcWarps * 32, dyn_mid));
+    if (mid_per_sm < 1) mid_per_sm = 1;
     HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, 0, s, view, g->nV, d_counts, d_total, counters,
-              big, warp_cap, chunk, narrow_min);
-    HN_LAUNCH(k_tc_cta<MODE>, gc, kTcWarps * 32, dyn, s, view, d_counts, d_total, counters, big,
-              narrow_min);
+              big, warp_cap, mid_cap, chunk, narrow_min);
+    HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms * mid_per_sm, kTcWarps * 32, dyn_mid, s, view,
+              g->nV, d_counts, d_total, counters, big, narrow_min, 0, mid_cap);
+    HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms, kTcWarps * 32, dyn_huge, s, view, g->nV,
+              d_counts, d_total, counters, big, narrow_min, 1, cta_cap);
 }
 
 unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_counts,
@@ -470,19 +510,17 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     cudaStream_t s = g->stream;
     unsigned long long* d_total = (unsigned long long*)g->d_scalar;
     HN_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
-    int* counters = (int*)(g->d_scalar + 1);  // next vertex, big-list size
-    HN_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(int), s));
+    int* counters = (int*)(g->d_scalar + 1);  // next vertex, mid and huge list sizes
+    HN_CUDA(cudaMemsetAsync(counters, 0, 3 * sizeof(int), s));
     DevBuf<int32_t> big((size_t)g->nV + 1, s);
-    // hash table of the CTA path + its filter (8 bits per slot)
-    const size_t dyn = (size_t)2 * kCtaCap * sizeof(int) + (size_t)2 * kCtaCap / 4 * sizeof(unsigned);
     TcView view{o.offp.get(), o.fwd.get()};
     if (d_counts) HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * g->nV, s));
     if (!d_counts)
-        launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), dyn);
+        launch_counting<0>(g, view, nullptr, d_total, counters, big.get());
     else if (mode == 2)
-        launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), dyn);
+        launch_counting<2>(g, view, d_counts, d_total, counters, big.get());
     else
-        launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), dyn);
+        launch_counting<1>(g, view, d_counts, d_total, counters, big.get());
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];
 }

@@ -103,6 +103,12 @@ int hn_profile_report(char* buf, int64_t len);
  *   tc.chunk            vertices handed to a warp per atomic (1..256, 16)
  *   tc.narrow_min       candidate lists longer than this are first narrowed
  *                       to the [min, max] of N+(u) by two searches (0..1024, 0)
+ *   tc.mid_cap          listed vertices (oriented degree above tc.warp_cap)
+ *                       up to this go to the CTA kernel with small tables,
+ *                       several CTAs per SM (32..4096, 4096)
+ *   tc.cta_table_cap    table capacity of the CTA kernel for the larger
+ *                       listed vertices; above it N+(u) is binary-searched
+ *                       in global memory (32..16384, 16384)
  *   msbfs.bottom_up     1: batched BFS runs bottom-up levels while the
  *                       frontier is large (bfs.do_alpha / do_beta switch) (0..1, 1)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)

@@ -353,6 +353,9 @@ def test_tc_local(name):
     {"tc.warp_cap": 32, "tc.chunk": 1, "tc.warp_ctas_per_sm": 1},
     {"tc.warp_cap": 64, "tc.chunk": 256, "tc.warp_ctas_per_sm": 16},
     {"tc.narrow_min": 1024, "tc.warp_cap": 128},
+    # rmat10's oriented degrees reach 44: all three listed-vertex paths
+    {"tc.warp_cap": 32, "tc.mid_cap": 36, "tc.cta_table_cap": 40},
+    {"tc.warp_cap": 32, "tc.mid_cap": 32, "tc.cta_table_cap": 32, "tc.narrow_min": 8},
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
     {"bfs.warp_strided": 1},
