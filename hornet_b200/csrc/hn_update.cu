@@ -28,6 +28,7 @@
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <climits>
 
 #include "hn_graph.cuh"
 
@@ -244,8 +245,31 @@ k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
 }
 
 using Tile = LbTile<kB, 4>;
+constexpr int kStage = 512;    // batch entries of a tile staged in shared memory
 
-// Old adjacency of every changed vertex -> its new block.
+__device__ __forceinline__ int lower_bound32(const int32_t* a, int n, int32_t x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ int upper_bound32(const int32_t* a, int n, int32_t x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] <= x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Old adjacency of every changed vertex -> its new block.  The batch
+// entries the tile's segments search are one contiguous run of cdst (the
+// segments are consecutive sources and cdst is sorted by source): when the
+// run has at most kStage entries it is staged in shared memory, so the
+// per-item searches do not wait on global loads.
 template <bool INSERT>
 __global__ void __launch_bounds__(kB, 5)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
@@ -260,9 +284,15 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
     __shared__ int s_k0[Tile::TILE + 1];   // the batch list of segment b, narrowed to
     __shared__ int s_k1[Tile::TILE + 1];   // the old values this tile holds: [k0, k1)
     __shared__ int s_kb[Tile::TILE + 1];   // batch entries of the segment before k0
+    __shared__ int32_t s_cd[kStage];       // cdst[K0, K1) of this tile
+    __shared__ int s_K0, s_K1;
     const long long total = prefix[nseg];
     long long ntiles = (total + nseg + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        if (threadIdx.x == 0) {   // the previous tile ended with a barrier
+            s_K0 = INT_MAX;
+            s_K1 = INT_MIN;
+        }
         int n = lb_tile_load(t, prefix, nseg, total, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kB) {
             long long s = t.seg0 + b;
@@ -289,6 +319,10 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
                 s_k0[b] = k0 + blo;
                 s_k1[b] = k0 + bhi;
                 s_kb[b] = blo;
+                if (bhi > blo) {
+                    atomicMin(&s_K0, k0 + blo);
+                    atomicMax(&s_K1, k0 + bhi);
+                }
             }
         }
         __syncthreads();
@@ -308,23 +342,31 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
                 if (wpool) ws[k] = wpool[s_old[bs[k]] + t.item0 + i];
             }
         }
+        // stage the tile's batch run while those loads are in flight
+        const int K0 = s_K0, K1 = s_K1;
+        const bool staged = K1 > K0 && K1 - K0 <= kStage;   // uniform in the CTA
+        if (staged) {
+            for (int i = threadIdx.x; i < K1 - K0; i += kB) s_cd[i] = cdst[K0 + i];
+            __syncthreads();
+        }
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
             if (bs[k] < 0) continue;
             const int b = bs[k];
             const int x = xs[k];
             const long long e = t.item0 + threadIdx.x + k * kB;   // global item
-            const int32_t* B = cdst + s_k0[b];
-            long long nb = s_k1[b] - s_k0[b];
+            const int nb = s_k1[b] - s_k0[b];
+            // read only when nb > 0, and then [s_k0[b], s_k1[b]) lies in [K0, K1)
+            const int32_t* B = staged ? s_cd + (s_k0[b] - K0) : cdst + s_k0[b];
             if (INSERT) {
-                long long j = s_kb[b] + lower_bound_dev(B, nb, x);
+                long long j = s_kb[b] + lower_bound32(B, nb, x);
                 pool[s_new[b] + e + j] = x;
                 if (wpool) wpool[s_new[b] + e + j] = ws[k];
             } else {
                 // every batch copy of x lies inside the narrowed range
-                long long ubl = upper_bound_dev(B, nb, x);
+                long long ubl = upper_bound32(B, nb, x);
                 long long lbl = ubl;
-                if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound_dev(B, ubl, x);
+                if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound32(B, (int)ubl, x);
                 long long cnt = ubl - lbl;  // copies of x to delete
                 long long ub = s_kb[b] + ubl;
                 bool keep = true;
