@@ -164,24 +164,28 @@ __device__ __forceinline__ void tab_insert_f(int* tab, unsigned* filt, int bits,
     atomicOr(filt + (f >> 5), 1u << (f & 31));
 }
 
-// Membership of w, for lanes whose filter bit is set (`maybe`): the home
-// bucket decides unless it is full without w; then the probe continues
-// slot by slot (the table is at most half full, so it meets an empty slot).
-__device__ __forceinline__ bool tab_find(const int* tab, int bits, int w, bool maybe) {
+// Membership of w, for lanes whose filter bit is set (`maybe`), in the home
+// bucket.  `more`: the bucket is full and does not hold w, so the answer is
+// tab_rest's.
+__device__ __forceinline__ bool tab_bucket(const int* tab, int bits, int w, bool maybe,
+                                           bool& more) {
     const unsigned h = tab_home(w, bits);
     int4 q = make_int4(-1, -1, -1, -1);
     if (maybe) q = *reinterpret_cast<const int4*>(tab + h);
-    bool hit = (q.x == w) | (q.y == w) | (q.z == w) | (q.w == w);
-    const bool more = maybe & !hit & (q.x != -1) & (q.y != -1) & (q.z != -1) & (q.w != -1);
-    if (more) {
-        const unsigned mask = (1u << bits) - 1;
-        for (unsigned p = (h + 4) & mask;; p = (p + 1) & mask) {
-            const int x = tab[p];
-            if (x == w) { hit = true; break; }
-            if (x == -1) break;
-        }
-    }
+    const bool hit = (q.x == w) | (q.y == w) | (q.z == w) | (q.w == w);
+    more = maybe & !hit & (q.x != -1) & (q.y != -1) & (q.z != -1) & (q.w != -1);
     return hit;
+}
+
+// The probe after a full home bucket, slot by slot (the table is at most
+// half full, so it meets an empty slot).
+__device__ __forceinline__ bool tab_rest(const int* tab, int bits, int w) {
+    const unsigned mask = (1u << bits) - 1;
+    for (unsigned p = (tab_home(w, bits) + 4) & mask;; p = (p + 1) & mask) {
+        const int x = tab[p];
+        if (x == w) return true;
+        if (x == -1) return false;
+    }
 }
 
 // Owner credit: the warp's triangles found from u, added to counts[u] once
@@ -291,6 +295,10 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                         va[j] = a;
                     }
                 }
+                // a lane's first lookup that needs probing past its home
+                // bucket waits until after the step (one divergent probe
+                // loop per step instead of one per pair)
+                int dw = -1, da = 0;
 #pragma unroll
                 for (int j = 0; j < kPairIlp; j++) {
                     const int w = wv[j];
@@ -298,7 +306,16 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                     bool hit;
                     if (tab) {
                         const unsigned f = tc_fbit(w, bits);
-                        hit = tab_find(tab, bits, w, (filt[f >> 5] >> (f & 31)) & 1u);
+                        bool more;
+                        hit = tab_bucket(tab, bits, w, (filt[f >> 5] >> (f & 31)) & 1u, more);
+                        if (more) {
+                            if (dw < 0) {
+                                dw = w;
+                                da = va[j];
+                            } else {
+                                hit = tab_rest(tab, bits, w);
+                            }
+                        }
                     } else {
                         int lo = 0, hi = du;
                         while (lo < hi) {
@@ -314,6 +331,14 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                             atomicAdd(per_vertex + u, 1ull);
                             atomicAdd(per_vertex + s_v[va[j]], 1ull);
                         }
+                    }
+                }
+                if (dw >= 0 && tab_rest(tab, bits, dw)) {
+                    cnt++;
+                    if (MODE == 1) {
+                        atomicAdd(per_vertex + dw, 1ull);
+                        atomicAdd(per_vertex + u, 1ull);
+                        atomicAdd(per_vertex + s_v[da], 1ull);
                     }
                 }
             }
