@@ -17,6 +17,8 @@
 // table (see the comment above k_tc_warp).
 #include <cub/cub.cuh>
 
+#include <type_traits>
+
 #include "hn_graph.cuh"
 #include "hn_tc.cuh"
 
@@ -208,7 +210,7 @@ struct TcView {
 // warps share u); each lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
 // searches, then the group's pairs are dealt round-robin to the lanes
 // (one search over the 33-entry prefix per lane per group).
-template <int MODE>
+template <int MODE, bool TAB>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int* tab, const unsigned* filt, int bits,
     int narrow_min, int* s_next, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
@@ -267,15 +269,19 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
             int start = s_pref[a], end = s_pref[a + 1];
             const int32_t* base = g.fwd + s_vb[a];
             // kPairIlp pairs per lane per step (k, k+32, ...): their loads
-            // of w are issued together, then probed
-            for (int k0 = lane; k0 < T; k0 += 32 * kPairIlp) {
+            // of w are issued together, then probed.  FULL steps (every
+            // lane's kPairIlp pairs exist; uniform in the warp) skip the
+            // bounds checks; the last step of a group is partial.
+            unsigned c32 = 0;
+            auto step = [&](int k0, auto full_tag) {
+                constexpr bool FULL = decltype(full_tag)::value;
                 int wv[kPairIlp], va[kPairIlp];
 #pragma unroll
                 for (int j = 0; j < kPairIlp; j++) {
                     const int k = k0 + 32 * j;
                     wv[j] = -1;
                     va[j] = a;
-                    if (k < T) {
+                    if (FULL || k < T) {
                         if (k >= end) {   // the candidate holding pair k
                             a++;
                             if (s_pref[a + 1] <= k) {
@@ -302,9 +308,9 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
 #pragma unroll
                 for (int j = 0; j < kPairIlp; j++) {
                     const int w = wv[j];
-                    if (w < 0) continue;
+                    if (!FULL && w < 0) continue;
                     bool hit;
-                    if (tab) {
+                    if (TAB) {
                         const unsigned f = tc_fbit(w, bits);
                         bool more;
                         hit = tab_bucket(tab, bits, w, (filt[f >> 5] >> (f & 31)) & 1u, more);
@@ -324,24 +330,27 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                         }
                         hit = lo < du && L[lo] == w;
                     }
-                    if (hit) {
-                        cnt++;
-                        if (MODE == 1) {
-                            atomicAdd(per_vertex + w, 1ull);
-                            atomicAdd(per_vertex + u, 1ull);
-                            atomicAdd(per_vertex + s_v[va[j]], 1ull);
-                        }
+                    c32 += hit ? 1u : 0u;
+                    if (MODE == 1 && hit) {
+                        atomicAdd(per_vertex + w, 1ull);
+                        atomicAdd(per_vertex + u, 1ull);
+                        atomicAdd(per_vertex + s_v[va[j]], 1ull);
                     }
                 }
-                if (dw >= 0 && tab_rest(tab, bits, dw)) {
-                    cnt++;
+                if (TAB && dw >= 0 && tab_rest(tab, bits, dw)) {
+                    c32++;
                     if (MODE == 1) {
                         atomicAdd(per_vertex + dw, 1ull);
                         atomicAdd(per_vertex + u, 1ull);
                         atomicAdd(per_vertex + s_v[da], 1ull);
                     }
                 }
-            }
+            };
+            int k0 = lane;
+            for (; k0 - lane + 32 * kPairIlp <= T; k0 += 32 * kPairIlp)
+                step(k0, std::integral_constant<bool, true>());
+            if (k0 < T) step(k0, std::integral_constant<bool, false>());
+            cnt += c32;
         }
         __syncwarp();
     }
@@ -388,9 +397,9 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             __syncwarp();
             for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
             __syncwarp();
-            const unsigned long long cu = tc_vertex_warp<MODE>(u, g.fwd + ub, du, tab, filt, bits,
-                                                               narrow_min, nullptr, g, s_pref[warp],
-                                                               s_vb[warp], s_v[warp], per_vertex);
+            const unsigned long long cu = tc_vertex_warp<MODE, true>(
+                u, g.fwd + ub, du, tab, filt, bits, narrow_min, nullptr, g, s_pref[warp],
+                s_vb[warp], s_v[warp], per_vertex);
             mine += cu;
             if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
             __syncwarp();
@@ -447,10 +456,13 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             tab = s_dyn;
         }
         __syncthreads();
-        const unsigned long long cu = tc_vertex_warp<MODE>(u, g.fwd + ub, du, tab, filt, bits,
-                                                           narrow_min, &s_next, g,
-                                                           s_pref[warp], s_vb[warp], s_v[warp],
-                                                           per_vertex);
+        const unsigned long long cu =
+            tab ? tc_vertex_warp<MODE, true>(u, g.fwd + ub, du, tab, filt, bits, narrow_min,
+                                             &s_next, g, s_pref[warp], s_vb[warp], s_v[warp],
+                                             per_vertex)
+                : tc_vertex_warp<MODE, false>(u, g.fwd + ub, du, tab, filt, bits, narrow_min,
+                                              &s_next, g, s_pref[warp], s_vb[warp], s_v[warp],
+                                              per_vertex);
         mine += cu;
         if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
         __syncthreads();
