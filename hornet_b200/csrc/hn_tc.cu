@@ -175,7 +175,9 @@ __device__ __forceinline__ bool tab_bucket(const int* tab, int bits, int w, bool
     int4 q = make_int4(-1, -1, -1, -1);
     if (maybe) q = *reinterpret_cast<const int4*>(tab + h);
     const bool hit = (q.x == w) | (q.y == w) | (q.z == w) | (q.w == w);
-    more = maybe & !hit & (q.x != -1) & (q.y != -1) & (q.z != -1) & (q.w != -1);
+    // slots hold vertex ids (>= 0) or -1: the bucket is full iff the OR of
+    // its slots is non-negative
+    more = maybe & !hit & ((q.x | q.y | q.z | q.w) >= 0);
     return hit;
 }
 
@@ -266,8 +268,8 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                 int mid = (a + b) >> 1;
                 if (s_pref[mid] <= lane) a = mid; else b = mid;
             }
-            int start = s_pref[a], end = s_pref[a + 1];
-            const int32_t* base = g.fwd + s_vb[a];
+            int end = s_pref[a + 1];
+            const int32_t* base = g.fwd + (s_vb[a] - s_pref[a]);   // pair k's w: base[k]
             // kPairIlp pairs per lane per step (k, k+32, ...): their loads
             // of w are issued together, then probed.  FULL steps (every
             // lane's kPairIlp pairs exist; uniform in the warp) skip the
@@ -293,11 +295,10 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                                     if (s_pref[mid] <= k) a = mid; else hi = mid;
                                 }
                             }
-                            start = s_pref[a];
                             end = s_pref[a + 1];
-                            base = g.fwd + s_vb[a];
+                            base = g.fwd + (s_vb[a] - s_pref[a]);
                         }
-                        wv[j] = base[k - start];
+                        wv[j] = base[k];
                         va[j] = a;
                     }
                 }
