@@ -130,6 +130,7 @@ enum Knob {
     kKnobMsBottomUp,
     kKnobTcMidCap,
     kKnobTcCtaTableCap,
+    kKnobTcCandChunk,
     kNumKnobs
 };
 long long knob(Knob k);

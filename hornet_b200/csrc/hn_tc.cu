@@ -94,6 +94,66 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
         offp[u] = pos[prefix[u]];
 }
 
+// Candidate lists.  The oriented edge x -> y contributes |N+(x) ∩ N+(y)|
+// triangles whichever endpoint counts it, so it is counted by the endpoint
+// whose out-list is the longer: that list is the hash table, the shorter
+// one is probed (cost min(d+(x), d+(y)) instead of d+(y)).  C(z) lists the
+// other endpoint of every edge z counts.  Order inside C(z) is immaterial.
+__device__ __forceinline__ bool cand_flip(long long dx, long long dy) { return dy > dx; }
+
+template <bool FILL>
+__global__ void __launch_bounds__(kB)
+k_cand(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ fwd,
+       int* __restrict__ cnt /*count pass: sizes; fill pass: cursors*/,
+       const long long* __restrict__ coff, int32_t* __restrict__ cand,
+       const long long* __restrict__ splits, long long split_tiles) {
+    __shared__ Tile t;
+    __shared__ int s_c[Tile::TILE + 1];          // edges a segment keeps, this tile
+    __shared__ long long s_pos[Tile::TILE + 1];  // their first slot (fill pass)
+    const long long total = offp[nV];
+    const long long ntiles = (total + nV + Tile::TILE - 1) / Tile::TILE;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int n = lb_tile_load(t, offp, (long long)nV, total, tile, splits, split_tiles);
+        for (int b = threadIdx.x; b <= t.nends; b += kB) s_c[b] = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += kB) {
+            const int b = t.seg[i];
+            const long long dx = t.ends[b] - t.seg_start(b);
+            const int y = fwd[t.item0 + i];
+            const long long dy = offp[y + 1] - offp[y];
+            if (cand_flip(dx, dy)) {
+                if (FILL) cand[coff[y] + atomicAdd(cnt + y, 1)] = (int)(t.seg0 + b);
+                else atomicAdd(cnt + y, 1);
+            } else {
+                atomicAdd(&s_c[b], 1);   // x keeps it (fill: slots taken below)
+            }
+        }
+        __syncthreads();
+        for (int b = threadIdx.x; b <= t.nends; b += kB) {
+            const long long x = t.seg0 + b;
+            if (x < nV && s_c[b]) {
+                if (FILL) {
+                    s_pos[b] = coff[x] + atomicAdd(cnt + x, s_c[b]);
+                    s_c[b] = 0;
+                } else {
+                    atomicAdd(cnt + x, s_c[b]);
+                }
+            }
+        }
+        __syncthreads();
+        if (FILL) {
+            for (int i = threadIdx.x; i < n; i += kB) {
+                const int b = t.seg[i];
+                const long long dx = t.ends[b] - t.seg_start(b);
+                const int y = fwd[t.item0 + i];
+                const long long dy = offp[y + 1] - offp[y];
+                if (!cand_flip(dx, dy)) cand[s_pos[b] + atomicAdd(&s_c[b], 1)] = y;
+            }
+            __syncthreads();
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Vertex-centric counting.  For each vertex u, N+(u) goes into an
 // open-addressing hash table in shared memory (multiplicative hash, linear
@@ -203,18 +263,22 @@ __device__ __forceinline__ void tc_credit_owner(unsigned long long* counts, int 
 struct TcView {
     const long long* offp;   // oriented offsets
     const int32_t* fwd;      // oriented lists
+    const long long* coff;   // candidate-list offsets
+    const int32_t* cand;     // candidate lists C(z)
 };
 
-// One warp: every (v, w) pair of u, w in N+(v) for v in N+(u), probed
-// against N+(u) (hash table `tab`, or binary search of the sorted global
-// list L when tab == nullptr).  Candidates v are taken 32 at a time (in
-// order, or groups claimed from the CTA's counter `s_next` when several
-// warps share u); each lane first narrows N+(v) to [min N+(u), max N+(u)] by two binary
-// searches, then the group's pairs are dealt round-robin to the lanes
-// (one search over the 33-entry prefix per lane per group).
+// One warp: every (v, w) pair of u, w in N+(v) for v in the candidate
+// list C of u, probed against L = N+(u) (hash table `tab`, or binary search
+// of the sorted global list L when tab == nullptr).  Candidates v are taken
+// 32 at a time (in order, or groups claimed from the CTA's counter `s_next`
+// when several warps share u); each lane first narrows N+(v) to
+// [min N+(u), max N+(u)] by two binary searches, then the group's pairs are
+// dealt round-robin to the lanes (one search over the 33-entry prefix per
+// lane per group).
 template <int MODE, bool TAB>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
-    int u, const int32_t* __restrict__ L, int du, const int* tab, const unsigned* filt, int bits,
+    int u, const int32_t* __restrict__ L, int du, const int32_t* __restrict__ C, int dc,
+    const int* tab, const unsigned* filt, int bits,
     int narrow_min, int* s_next, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
     int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
@@ -226,12 +290,12 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
         if (lane == 0) t = atomicAdd(s_next, 1);
         return __shfl_sync(0xFFFFFFFFu, t, 0) * 32;
     };
-    for (int c0 = claim(-32); c0 < du; c0 = claim(c0)) {
+    for (int c0 = claim(-32); c0 < dc; c0 = claim(c0)) {
         int idx = c0 + lane;
         int dx = 0, v = 0;
         long long xb = 0;
-        if (idx < du) {
-            v = L[idx];
+        if (idx < dc) {
+            v = C[idx];
             long long b0 = g.offp[v], b1 = g.offp[v + 1];
             const int32_t* lst = g.fwd + b0;
             int n = (int)(b1 - b0);
@@ -363,7 +427,8 @@ __global__ void __launch_bounds__(kTcWarps * 32, 5)
 k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] mid, [2] huge list size*/,
-          int32_t* __restrict__ big, int warp_cap, int mid_cap, int chunk, int narrow_min) {
+          long long* __restrict__ big, long long big_cap, int warp_cap, int mid_cap,
+          int cand_chunk, int chunk, int narrow_min) {
     __shared__ __align__(16) int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     __shared__ int s_pref[kTcWarps][33];
@@ -382,11 +447,22 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
         for (int u = u0; u < u1; u++) {
             long long ub = g.offp[u];
             int du = (int)(g.offp[u + 1] - ub);
-            if (du == 0) continue;
-            if (du > warp_cap) {   // mid list from the front, huge list from the back
+            const long long cb = g.coff[u];
+            const int dc = (int)(g.coff[u + 1] - cb);
+            if (du == 0 || dc == 0) continue;
+            if (du > warp_cap || dc > cand_chunk) {
+                // listed: one work item (u, chunk) per cand_chunk candidates;
+                // mid items from the front of `big`, huge items from the back
                 if (lane == 0) {
-                    if (du <= mid_cap) big[atomicAdd(counters + 1, 1)] = u;
-                    else big[nV - 1 - atomicAdd(counters + 2, 1)] = u;
+                    const int nch = (dc + cand_chunk - 1) / cand_chunk;
+                    if (du <= mid_cap) {
+                        const int p = atomicAdd(counters + 1, nch);
+                        for (int c = 0; c < nch; c++) big[p + c] = ((long long)u << 32) | c;
+                    } else {
+                        const int p = atomicAdd(counters + 2, nch);
+                        for (int c = 0; c < nch; c++)
+                            big[big_cap - 1 - (p + c)] = ((long long)u << 32) | c;
+                    }
                 }
                 continue;
             }
@@ -399,8 +475,8 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
             __syncwarp();
             const unsigned long long cu = tc_vertex_warp<MODE, true>(
-                u, g.fwd + ub, du, tab, filt, bits, narrow_min, nullptr, g, s_pref[warp],
-                s_vb[warp], s_v[warp], per_vertex);
+                u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, bits, narrow_min, nullptr, g,
+                s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
             mine += cu;
             if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
             __syncwarp();
@@ -422,13 +498,15 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
 // tc.cta_table_cap in a table, binary search of N+(u) beyond that).  A
 // table of d entries takes the power of two >= 2*d slots, so the dynamic
 // shared memory holds tc_table_slots(cap) slots and their filter.  The
-// lists share `big`: mid from the front (counters[1] entries), huge from the
+// lists share `big` (items (u << 32) | chunk, each tc.cand_chunk candidates
+// of u): mid from the front (counters[1] entries), huge from the
 // back (counters[2] entries).
 template <int MODE>
 __global__ void __launch_bounds__(kTcWarps * 32, 4)
 k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
-         const int32_t* __restrict__ big, int narrow_min, int huge, int cap) {
+         const long long* __restrict__ big, long long big_cap, int cand_chunk, int narrow_min,
+         int huge, int cap) {
     extern __shared__ __align__(16) int s_dyn[];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
@@ -439,9 +517,14 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
     const int nbig = counters[huge ? 2 : 1];
     unsigned long long mine = 0;
     for (int i = blockIdx.x; i < nbig; i += gridDim.x) {
-        int u = huge ? big[nV - 1 - i] : big[i];
+        const long long item = huge ? big[big_cap - 1 - i] : big[i];
+        const int u = (int)(item >> 32);
+        const int ch = (int)(item & 0xFFFFFFFF);
         long long ub = g.offp[u];
         int du = (int)(g.offp[u + 1] - ub);
+        const long long cb = g.coff[u] + (long long)ch * cand_chunk;
+        const int rest = (int)(g.coff[u + 1] - cb);
+        const int dc = rest < cand_chunk ? rest : cand_chunk;
         const int* tab = nullptr;
         unsigned* filt = (unsigned*)(s_dyn + tc_table_slots(cap));
         int bits = 0;
@@ -458,12 +541,12 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
         }
         __syncthreads();
         const unsigned long long cu =
-            tab ? tc_vertex_warp<MODE, true>(u, g.fwd + ub, du, tab, filt, bits, narrow_min,
-                                             &s_next, g, s_pref[warp], s_vb[warp], s_v[warp],
-                                             per_vertex)
-                : tc_vertex_warp<MODE, false>(u, g.fwd + ub, du, tab, filt, bits, narrow_min,
-                                              &s_next, g, s_pref[warp], s_vb[warp], s_v[warp],
-                                              per_vertex);
+            tab ? tc_vertex_warp<MODE, true>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, bits,
+                                             narrow_min, &s_next, g, s_pref[warp], s_vb[warp],
+                                             s_v[warp], per_vertex)
+                : tc_vertex_warp<MODE, false>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, bits,
+                                              narrow_min, &s_next, g, s_pref[warp], s_vb[warp],
+                                              s_v[warp], per_vertex);
         mine += cu;
         if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
         __syncthreads();
@@ -505,6 +588,33 @@ void build_oriented(hn_graph* g, Oriented& o) {
               o.fwd.get(), o.offp.get(), splits.get(), (long long)splits.n - 1);
 }
 
+// C(z) for every vertex z: offsets coff (nV+1) and lists cand.
+void build_candidates(hn_graph* g, const Oriented& o, DevBuf<long long>& coff,
+                      DevBuf<int32_t>& cand) {
+    cudaStream_t s = g->stream;
+    const int nV = g->nV;
+    const long long m = g->nE;   // bound on the oriented edge count (read on the device)
+    DevBuf<int> cnt((size_t)nV + 1, s);
+    HN_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * ((size_t)nV + 1), s));
+    DevBuf<long long> splits;
+    lb_splits(g, o.offp.get(), nV, m, Tile::TILE, splits);
+    const long long grid = (long long)g->info.sms * 8;
+    coff.alloc((size_t)nV + 1, s);
+    cand.alloc((size_t)m + 4, s);
+    HN_LAUNCH(k_cand<false>, grid, kB, 0, s, o.offp.get(), nV, o.fwd.get(), cnt.get(),
+              (const long long*)nullptr, (int32_t*)nullptr, splits.get(), (long long)splits.n - 1);
+    {
+        size_t tb = 0;
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.get(), coff.get(), nV + 1, s));
+        DevBuf<char> tmp(tb, s);
+        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, cnt.get(), coff.get(), nV + 1, s));
+        count_launch();
+    }
+    HN_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * ((size_t)nV + 1), s));
+    HN_LAUNCH(k_cand<true>, grid, kB, 0, s, o.offp.get(), nV, o.fwd.get(), cnt.get(),
+              (const long long*)coff.get(), cand.get(), splits.get(), (long long)splits.n - 1);
+}
+
 // mode 0: total only; 1: per-vertex counts (each triangle credited to its
 // three vertices); 2: owner counts (each triangle credited once, to its
 // lowest vertex in the degree orientation).
@@ -516,7 +626,8 @@ constexpr size_t tc_table_bytes(int cap) {
 
 template <int MODE>
 void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_counts,
-                     unsigned long long* d_total, int* counters, int32_t* big) {
+                     unsigned long long* d_total, int* counters, long long* big,
+                     long long big_cap, int cand_chunk) {
     cudaStream_t s = g->stream;
     const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
     const int warp_cap = (int)knob(kKnobTcWarpCap);
@@ -536,11 +647,11 @@ void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_coun
                                                           kTcWarps * 32, dyn_mid));
     if (mid_per_sm < 1) mid_per_sm = 1;
     HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, 0, s, view, g->nV, d_counts, d_total, counters,
-              big, warp_cap, mid_cap, chunk, narrow_min);
+              big, big_cap, warp_cap, mid_cap, cand_chunk, chunk, narrow_min);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms * mid_per_sm, kTcWarps * 32, dyn_mid, s, view,
-              g->nV, d_counts, d_total, counters, big, narrow_min, 0, mid_cap);
+              g->nV, d_counts, d_total, counters, big, big_cap, cand_chunk, narrow_min, 0, mid_cap);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms, kTcWarps * 32, dyn_huge, s, view, g->nV,
-              d_counts, d_total, counters, big, narrow_min, 1, cta_cap);
+              d_counts, d_total, counters, big, big_cap, cand_chunk, narrow_min, 1, cta_cap);
 }
 
 unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_counts,
@@ -550,15 +661,27 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     HN_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
     int* counters = (int*)(g->d_scalar + 1);  // next vertex, mid and huge list sizes
     HN_CUDA(cudaMemsetAsync(counters, 0, 3 * sizeof(int), s));
-    DevBuf<int32_t> big((size_t)g->nV + 1, s);
-    TcView view{o.offp.get(), o.fwd.get()};
+    // work items: at most one per vertex plus one per tc.cand_chunk candidates
+    const int cand_chunk = (int)knob(kKnobTcCandChunk);
+    const long long big_cap = (long long)g->nV + g->nE / cand_chunk + 2;
+    DevBuf<long long> big((size_t)big_cap, s);
+    // owner counts credit u, the lowest vertex of each triangle found from
+    // u, so mode 2 keeps every edge with its tail: C(u) = N+(u)
+    DevBuf<long long> coff;
+    DevBuf<int32_t> cand;
+    TcView view{o.offp.get(), o.fwd.get(), o.offp.get(), o.fwd.get()};
+    if (mode != 2 || !d_counts) {
+        build_candidates(g, o, coff, cand);
+        view.coff = coff.get();
+        view.cand = cand.get();
+    }
     if (d_counts) HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * g->nV, s));
     if (!d_counts)
-        launch_counting<0>(g, view, nullptr, d_total, counters, big.get());
+        launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), big_cap, cand_chunk);
     else if (mode == 2)
-        launch_counting<2>(g, view, d_counts, d_total, counters, big.get());
+        launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), big_cap, cand_chunk);
     else
-        launch_counting<1>(g, view, d_counts, d_total, counters, big.get());
+        launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), big_cap, cand_chunk);
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];
 }
