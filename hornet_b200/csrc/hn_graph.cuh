@@ -130,7 +130,8 @@ enum Knob {
     kKnobMsBottomUp,
     kKnobTcMidCap,
     kKnobTcCtaTableCap,
-    kKnobTcCandChunk,
+    kKnobTcItemWork,
+    kKnobTcWarpWork,
     kNumKnobs
 };
 long long knob(Knob k);

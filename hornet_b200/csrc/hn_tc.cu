@@ -189,6 +189,16 @@ __host__ __device__ constexpr int tc_table_slots(int cap) {
     return n;
 }
 
+// Candidates of one work item of a listed vertex with d+(u) = du: about
+// item_work pairs (every list it probes is at most du long), a multiple of
+// 32, at least 32.
+__device__ __forceinline__ int item_cands(int du, long long item_work) {
+    long long c = item_work / du;
+    if (c > (1 << 20)) c = 1 << 20;
+    c &= ~31LL;
+    return c < 32 ? 32 : (int)c;
+}
+
 __device__ __forceinline__ unsigned tc_hash(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - bits);
 }
@@ -428,7 +438,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] mid, [2] huge list size*/,
           long long* __restrict__ big, long long big_cap, int warp_cap, int mid_cap,
-          int cand_chunk, int chunk, int narrow_min) {
+          long long warp_work, long long item_work, int chunk, int narrow_min) {
     __shared__ __align__(16) int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     __shared__ int s_pref[kTcWarps][33];
@@ -450,11 +460,13 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             const long long cb = g.coff[u];
             const int dc = (int)(g.coff[u + 1] - cb);
             if (du == 0 || dc == 0) continue;
-            if (du > warp_cap || dc > cand_chunk) {
-                // listed: one work item (u, chunk) per cand_chunk candidates;
+            // every probed list of u is at most du long: dc * du bounds u's pairs
+            if (du > warp_cap || (long long)dc * du > warp_work) {
+                // listed: one work item (u, chunk) per item_cands candidates;
                 // mid items from the front of `big`, huge items from the back
                 if (lane == 0) {
-                    const int nch = (dc + cand_chunk - 1) / cand_chunk;
+                    const int ipc = item_cands(du, item_work);
+                    const int nch = (dc + ipc - 1) / ipc;
                     if (du <= mid_cap) {
                         const int p = atomicAdd(counters + 1, nch);
                         for (int c = 0; c < nch; c++) big[p + c] = ((long long)u << 32) | c;
@@ -498,14 +510,14 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
 // tc.cta_table_cap in a table, binary search of N+(u) beyond that).  A
 // table of d entries takes the power of two >= 2*d slots, so the dynamic
 // shared memory holds tc_table_slots(cap) slots and their filter.  The
-// lists share `big` (items (u << 32) | chunk, each tc.cand_chunk candidates
-// of u): mid from the front (counters[1] entries), huge from the
+// lists share `big` (items (u << 32) | chunk, each item_cands(d+(u))
+// candidates of u): mid from the front (counters[1] entries), huge from the
 // back (counters[2] entries).
 template <int MODE>
 __global__ void __launch_bounds__(kTcWarps * 32, 4)
 k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
          unsigned long long* __restrict__ total_out, const int* __restrict__ counters,
-         const long long* __restrict__ big, long long big_cap, int cand_chunk, int narrow_min,
+         const long long* __restrict__ big, long long big_cap, long long item_work, int narrow_min,
          int huge, int cap) {
     extern __shared__ __align__(16) int s_dyn[];
     __shared__ int s_pref[kTcWarps][33];
@@ -522,9 +534,10 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
         const int ch = (int)(item & 0xFFFFFFFF);
         long long ub = g.offp[u];
         int du = (int)(g.offp[u + 1] - ub);
-        const long long cb = g.coff[u] + (long long)ch * cand_chunk;
+        const int ipc = item_cands(du, item_work);
+        const long long cb = g.coff[u] + (long long)ch * ipc;
         const int rest = (int)(g.coff[u + 1] - cb);
-        const int dc = rest < cand_chunk ? rest : cand_chunk;
+        const int dc = rest < ipc ? rest : ipc;
         const int* tab = nullptr;
         unsigned* filt = (unsigned*)(s_dyn + tc_table_slots(cap));
         int bits = 0;
@@ -627,12 +640,13 @@ constexpr size_t tc_table_bytes(int cap) {
 template <int MODE>
 void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_counts,
                      unsigned long long* d_total, int* counters, long long* big,
-                     long long big_cap, int cand_chunk) {
+                     long long big_cap) {
     cudaStream_t s = g->stream;
     const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
     const int warp_cap = (int)knob(kKnobTcWarpCap);
     const int chunk = (int)knob(kKnobTcChunk);
     const int narrow_min = (int)knob(kKnobTcNarrowMin);
+    const long long warp_work = knob(kKnobTcWarpWork), item_work = knob(kKnobTcItemWork);
     const int mid_cap = (int)knob(kKnobTcMidCap);
     const int cta_cap = (int)knob(kKnobTcCtaTableCap);
     const size_t dyn_mid = tc_table_bytes(mid_cap), dyn_huge = tc_table_bytes(cta_cap);
@@ -647,11 +661,11 @@ void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_coun
                                                           kTcWarps * 32, dyn_mid));
     if (mid_per_sm < 1) mid_per_sm = 1;
     HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, 0, s, view, g->nV, d_counts, d_total, counters,
-              big, big_cap, warp_cap, mid_cap, cand_chunk, chunk, narrow_min);
+              big, big_cap, warp_cap, mid_cap, warp_work, item_work, chunk, narrow_min);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms * mid_per_sm, kTcWarps * 32, dyn_mid, s, view,
-              g->nV, d_counts, d_total, counters, big, big_cap, cand_chunk, narrow_min, 0, mid_cap);
+              g->nV, d_counts, d_total, counters, big, big_cap, item_work, narrow_min, 0, mid_cap);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms, kTcWarps * 32, dyn_huge, s, view, g->nV,
-              d_counts, d_total, counters, big, big_cap, cand_chunk, narrow_min, 1, cta_cap);
+              d_counts, d_total, counters, big, big_cap, item_work, narrow_min, 1, cta_cap);
 }
 
 unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_counts,
@@ -661,9 +675,8 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     HN_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
     int* counters = (int*)(g->d_scalar + 1);  // next vertex, mid and huge list sizes
     HN_CUDA(cudaMemsetAsync(counters, 0, 3 * sizeof(int), s));
-    // work items: at most one per vertex plus one per tc.cand_chunk candidates
-    const int cand_chunk = (int)knob(kKnobTcCandChunk);
-    const long long big_cap = (long long)g->nV + g->nE / cand_chunk + 2;
+    // work items: at most one per vertex plus one per 32 candidates
+    const long long big_cap = (long long)g->nV + g->nE / 32 + 2;
     DevBuf<long long> big((size_t)big_cap, s);
     // owner counts credit u, the lowest vertex of each triangle found from
     // u, so mode 2 keeps every edge with its tail: C(u) = N+(u)
@@ -677,11 +690,11 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     }
     if (d_counts) HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * g->nV, s));
     if (!d_counts)
-        launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), big_cap, cand_chunk);
+        launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), big_cap);
     else if (mode == 2)
-        launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), big_cap, cand_chunk);
+        launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), big_cap);
     else
-        launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), big_cap, cand_chunk);
+        launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), big_cap);
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];
 }

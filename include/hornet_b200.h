@@ -109,9 +109,11 @@ int hn_profile_report(char* buf, int64_t len);
  *   tc.cta_table_cap    table capacity of the CTA kernel for the larger
  *                       listed vertices; above it N+(u) is binary-searched
  *                       in global memory (32..16384, 16384)
- *   tc.cand_chunk       candidates of one CTA work item: vertices with more
- *                       candidates (or a table above tc.warp_cap) are split
- *                       into items of this many (32..2^20, 4096)
+ *   tc.warp_work        bound on a vertex's pairs (candidates x d+(u)) for
+ *                       the warp-per-vertex kernel; above it, or with d+(u)
+ *                       above tc.warp_cap, the vertex goes to CTA work
+ *                       items (1024..2^30, 65536)
+ *   tc.item_work        pairs bound of one CTA work item (1024..2^30, 262144)
  *   msbfs.bottom_up     1: batched BFS runs bottom-up levels while the
  *                       frontier is large (bfs.do_alpha / do_beta switch) (0..1, 1)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)

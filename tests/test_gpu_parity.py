@@ -356,8 +356,8 @@ def test_tc_local(name):
     # rmat10's oriented degrees reach 44: all three listed-vertex paths
     {"tc.warp_cap": 32, "tc.mid_cap": 36, "tc.cta_table_cap": 40},
     {"tc.warp_cap": 32, "tc.mid_cap": 32, "tc.cta_table_cap": 32, "tc.narrow_min": 8},
-    {"tc.cand_chunk": 32, "tc.warp_cap": 64},
-    {"tc.cand_chunk": 33, "tc.mid_cap": 36, "tc.warp_cap": 32},
+    {"tc.warp_work": 1024, "tc.item_work": 1024, "tc.warp_cap": 64},
+    {"tc.warp_work": 1024, "tc.item_work": 1500, "tc.mid_cap": 36, "tc.warp_cap": 32},
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
     {"bfs.warp_strided": 1},
