@@ -444,7 +444,8 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
     keep = (d[src] < d[adj]) | ((d[src] == d[adj]) & (src < adj))
     dplus = np.bincount(src[keep], minlength=nV).astype(np.int64)
     tc_bytes = 8 * m_plus + 4 * int((dplus[src[keep]] + dplus[adj[keep]]).sum())
-    troof = roofline_entry(H, ["k_orient", "k_tc_", "k_degrees"], lambda: tc_bytes, peak, peak_kind, rep,
+    troof = roofline_entry(H, ["k_orient", "k_cand", "k_tc_", "k_degrees"], lambda: tc_bytes, peak,
+                           peak_kind, rep,
                            f"R-MAT scale {scale} TC")
     also["tc"] = {"metric": "TC edges/s", "value": round(m_plus / t, 1), "unit": "edges/s",
                   "triangles": int(tc.countTriangles()), "ms": round(t * 1e3, 3),
