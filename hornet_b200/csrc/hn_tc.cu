@@ -107,50 +107,66 @@ k_cand(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ f
        int* __restrict__ cnt /*count pass: sizes; fill pass: cursors*/,
        const long long* __restrict__ coff, int32_t* __restrict__ cand,
        const long long* __restrict__ splits, long long split_tiles) {
+    constexpr int IPT = Tile::TILE / kB;   // items per thread, blocked
+    using Scan = cub::BlockScan<int, kB>;
     __shared__ Tile t;
-    __shared__ int s_c[Tile::TILE + 1];          // edges a segment keeps, this tile
-    __shared__ long long s_pos[Tile::TILE + 1];  // their first slot (fill pass)
+    __shared__ typename Scan::TempStorage scan_tmp;
+    __shared__ int s_rank[Tile::TILE + 1];       // kept edges of the tile before item i
+    __shared__ long long s_pos[Tile::TILE + 1];  // first slot of segment b's kept edges
     const long long total = offp[nV];
     const long long ntiles = (total + nV + Tile::TILE - 1) / Tile::TILE;
     for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
         int n = lb_tile_load(t, offp, (long long)nV, total, tile, splits, split_tiles);
-        for (int b = threadIdx.x; b <= t.nends; b += kB) s_c[b] = 0;
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += kB) {
-            const int b = t.seg[i];
-            const long long dx = t.ends[b] - t.seg_start(b);
-            const int y = fwd[t.item0 + i];
-            const long long dy = offp[y + 1] - offp[y];
-            if (cand_flip(dx, dy)) {
-                if (FILL) cand[coff[y] + atomicAdd(cnt + y, 1)] = (int)(t.seg0 + b);
-                else atomicAdd(cnt + y, 1);
-            } else {
-                atomicAdd(&s_c[b], 1);   // x keeps it (fill: slots taken below)
-            }
-        }
-        __syncthreads();
-        for (int b = threadIdx.x; b <= t.nends; b += kB) {
-            const long long x = t.seg0 + b;
-            if (x < nV && s_c[b]) {
-                if (FILL) {
-                    s_pos[b] = coff[x] + atomicAdd(cnt + x, s_c[b]);
-                    s_c[b] = 0;
-                } else {
-                    atomicAdd(cnt + x, s_c[b]);
-                }
-            }
-        }
-        __syncthreads();
-        if (FILL) {
-            for (int i = threadIdx.x; i < n; i += kB) {
+        int ys[IPT], keep[IPT], rank[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = threadIdx.x * IPT + k;
+            keep[k] = 0;
+            ys[k] = -1;
+            if (i < n) {
                 const int b = t.seg[i];
                 const long long dx = t.ends[b] - t.seg_start(b);
                 const int y = fwd[t.item0 + i];
                 const long long dy = offp[y + 1] - offp[y];
-                if (!cand_flip(dx, dy)) cand[s_pos[b] + atomicAdd(&s_c[b], 1)] = y;
+                ys[k] = y;
+                keep[k] = cand_flip(dx, dy) ? 0 : 1;
             }
-            __syncthreads();
         }
+        int kept_total;
+        Scan(scan_tmp).ExclusiveSum(keep, rank, kept_total);
+#pragma unroll
+        for (int k = 0; k < IPT; k++) s_rank[threadIdx.x * IPT + k] = rank[k];
+        if (threadIdx.x == 0) s_rank[Tile::TILE] = kept_total;
+        __syncthreads();
+        // per segment: its kept edges are the ones ranked [lo, hi) of the tile
+        for (int b = threadIdx.x; b <= t.nends; b += kB) {
+            const long long x = t.seg0 + b;
+            if (x < nV) {
+                const long long s0 = t.seg_start(b), s1 = t.ends[b];
+                const int lo = (int)((s0 > t.item0 ? s0 : t.item0) - t.item0);
+                const long long e1 = t.item0 + n;
+                const int hi = (int)((s1 < e1 ? s1 : e1) - t.item0);
+                const int kept = lo < hi ? (hi < n ? s_rank[hi] : kept_total) - s_rank[lo] : 0;
+                if (kept) {
+                    if (FILL) s_pos[b] = coff[x] + atomicAdd(cnt + x, kept) - s_rank[lo];
+                    else atomicAdd(cnt + x, kept);
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = threadIdx.x * IPT + k;
+            if (ys[k] < 0) continue;
+            const int b = t.seg[i];
+            if (keep[k]) {
+                if (FILL) cand[s_pos[b] + rank[k]] = ys[k];
+            } else {
+                if (FILL) cand[coff[ys[k]] + atomicAdd(cnt + ys[k], 1)] = (int)(t.seg0 + b);
+                else atomicAdd(cnt + ys[k], 1);
+            }
+        }
+        __syncthreads();
     }
 }
 
