@@ -23,6 +23,7 @@
 #include <cub/cub.cuh>
 
 #include "hn_graph.cuh"
+#include "hn_tc.cuh"
 
 namespace hn {
 namespace {
@@ -55,78 +56,20 @@ __global__ void k_kt_canon(const long long* __restrict__ off, const int32_t* __r
     }
 }
 
-// support of each canonical edge = |N(u) ∩ N(v)|
-// Support of every canonical edge (u < v): |N(u) ∩ N(v)|.  Edges whose
-// shorter list exceeds 32 entries are listed for k_kt_support_heavy (a warp
-// each), as in the peel.
-__global__ void k_kt_support(const long long* __restrict__ off, const int32_t* __restrict__ adj,
-                             const int32_t* __restrict__ src, long long m,
-                             int32_t* __restrict__ sup, unsigned char* __restrict__ alive,
-                             int* __restrict__ nalive, int32_t* __restrict__ heavy,
-                             int* __restrict__ nheavy) {
+// Canonical edges (u < v) start alive (their supports come from the
+// triangle enumeration: every triangle, found once, credits its three edges).
+__global__ void k_kt_init(const int32_t* __restrict__ adj, const int32_t* __restrict__ src,
+                          long long m, unsigned char* __restrict__ alive,
+                          int* __restrict__ nalive) {
     int mine = 0;
-    for (long long e0 = blockIdx.x * (long long)blockDim.x; e0 < m;
-         e0 += (long long)gridDim.x * blockDim.x) {
-        const long long e = e0 + threadIdx.x;
-        bool big = false;
-        if (e < m) {
-            int u = src[e], v = adj[e];
-            if (u >= v) {
-                alive[e] = 0;
-            } else {
-                const int32_t* A = adj + off[u];
-                long long la = off[u + 1] - off[u];
-                const int32_t* B = adj + off[v];
-                long long lb = off[v + 1] - off[v];
-                if (la > lb) { const int32_t* T = A; A = B; B = T; long long t = la; la = lb; lb = t; }
-                if (la > 32) {
-                    big = true;
-                    sup[e] = 0;
-                } else {
-                    int cnt = 0;
-                    long long lo = 0;
-                    for (long long i = 0; i < la && lo < lb; i++) {
-                        long long p = lo + lower_bound_dev(B + lo, lb - lo, A[i]);
-                        if (p < lb && B[p] == A[i]) { cnt++; lo = p + 1; } else lo = p;
-                    }
-                    sup[e] = cnt;
-                }
-                alive[e] = 1;
-                mine++;
-            }
-        }
-        int slot = warp_append(nheavy, big);
-        if (big) heavy[slot] = (int)e;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < m;
+         e += (long long)gridDim.x * blockDim.x) {
+        const bool canon = src[e] < adj[e];
+        alive[e] = canon ? 1 : 0;
+        mine += canon ? 1 : 0;
     }
     for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(nalive, mine);
-}
-
-__global__ void k_kt_support_heavy(const long long* __restrict__ off,
-                                   const int32_t* __restrict__ adj,
-                                   const int32_t* __restrict__ src,
-                                   const int32_t* __restrict__ heavy,
-                                   const int* __restrict__ nheavy, int32_t* __restrict__ sup) {
-    const int lane = threadIdx.x & 31;
-    const long long nh = *nheavy;
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long h = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh;
-         h += warps) {
-        const int e = heavy[h];
-        const int u = src[e], v = adj[e];
-        const int32_t* A = adj + off[u];
-        long long la = off[u + 1] - off[u];
-        const int32_t* B = adj + off[v];
-        long long lb = off[v + 1] - off[v];
-        if (la > lb) { const int32_t* T = A; A = B; B = T; long long t = la; la = lb; lb = t; }
-        int cnt = 0;
-        for (long long i = lane; i < la; i += 32) {
-            const long long p = lower_bound_dev(B, lb, A[i]);
-            cnt += (p < lb && B[p] == A[i]) ? 1 : 0;
-        }
-        for (int o = 16; o; o >>= 1) cnt += __shfl_down_sync(0xFFFFFFFFu, cnt, o);
-        if (lane == 0) sup[e] = cnt;
-    }
 }
 
 // Positions of the current lists whose (canonical) edge is still alive.
@@ -351,11 +294,18 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         throw Error(HN_ERR_INVALID, "k-truss needs a simple symmetric graph");
     HN_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
     HN_CUDA(cudaMemsetAsync(inF.get(), 0, (size_t)m, s));
-    DevBuf<int32_t> H((size_t)m, s);   // heavy edges (support, then each peel round)
-    HN_LAUNCH(k_kt_support, grid_for(g, m, kB), kB, 0, s, off.get(), adj.get(), src.get(), m,
-              sup.get(), alive.get(), cnt, H.get(), cnt + 3);
-    HN_LAUNCH(k_kt_support_heavy, grid_for(g, m, 256), 256, 0, s, off.get(), adj.get(),
-              src.get(), (const int32_t*)H.get(), (const int*)(cnt + 3), sup.get());
+    DevBuf<int32_t> H((size_t)m, s);   // heavy frontier edges of each peel round
+    {
+        // supports: each triangle of the degree-oriented graph credits its
+        // three canonical edges once (uses the graph's scalars, so it runs
+        // before the counters below are set)
+        HN_CUDA(cudaMemsetAsync(sup.get(), 0, sizeof(int32_t) * (size_t)m, s));
+        Oriented o;
+        build_oriented(g, o, canon.get());
+        edge_support(g, o, sup.get());
+    }
+    HN_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(int), s));
+    HN_LAUNCH(k_kt_init, grid_for(g, m, kB), kB, 0, s, adj.get(), src.get(), m, alive.get(), cnt);
     // truss numbers start at 2 (0x02020202 per int is not 2; fill by kernel-free memset of 0
     // then write on retirement: every edge is retired exactly once)
     read_scalars(g, 1);

@@ -69,7 +69,8 @@ __global__ void __launch_bounds__(kB)
 k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restrict__ vtab,
               const int32_t* __restrict__ pool, const int32_t* __restrict__ pos,
               int32_t* __restrict__ fwd, long long* __restrict__ offp,
-              const long long* __restrict__ splits, long long split_tiles) {
+              const long long* __restrict__ splits, long long split_tiles,
+              const int32_t* __restrict__ canon, int32_t* __restrict__ feid) {
     __shared__ Tile t;
     __shared__ long long s_base[Tile::TILE + 1];
     const long long total = prefix[nV];
@@ -84,7 +85,10 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
         for (int i = threadIdx.x; i < n; i += kB) {
             long long e = t.item0 + i;
             int p = pos[e];
-            if (pos[e + 1] != p) fwd[p] = pool[s_base[t.seg[i]] + e];
+            if (pos[e + 1] != p) {
+                fwd[p] = pool[s_base[t.seg[i]] + e];
+                if (feid) feid[p] = canon[e];   // edge id of the kept edge
+            }
         }
         __syncthreads();
     }
@@ -106,7 +110,8 @@ __global__ void __launch_bounds__(kB)
 k_cand(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ fwd,
        int* __restrict__ cnt /*count pass: sizes; fill pass: cursors*/,
        const long long* __restrict__ coff, int32_t* __restrict__ cand,
-       const long long* __restrict__ splits, long long split_tiles) {
+       const long long* __restrict__ splits, long long split_tiles,
+       const int32_t* __restrict__ feid, int32_t* __restrict__ ceid) {
     constexpr int IPT = Tile::TILE / kB;   // items per thread, blocked
     using Scan = cub::BlockScan<int, kB>;
     __shared__ Tile t;
@@ -159,12 +164,16 @@ k_cand(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ f
             const int i = threadIdx.x * IPT + k;
             if (ys[k] < 0) continue;
             const int b = t.seg[i];
+            long long q = -1;
             if (keep[k]) {
-                if (FILL) cand[s_pos[b] + rank[k]] = ys[k];
+                if (FILL) q = s_pos[b] + rank[k];
+                if (FILL) cand[q] = ys[k];
             } else {
-                if (FILL) cand[coff[ys[k]] + atomicAdd(cnt + ys[k], 1)] = (int)(t.seg0 + b);
+                if (FILL) q = coff[ys[k]] + atomicAdd(cnt + ys[k], 1);
+                if (FILL) cand[q] = (int)(t.seg0 + b);
                 else atomicAdd(cnt + ys[k], 1);
             }
+            if (FILL && ceid) ceid[q] = feid[t.item0 + i];
         }
         __syncthreads();
     }
@@ -228,12 +237,13 @@ __device__ __forceinline__ unsigned tab_home(int w, int bits) {
     return tc_hash(w, bits - 2) << 2;
 }
 
-__device__ __forceinline__ void tab_insert(int* tab, int bits, int w) {
+// Inserts w; returns its slot.
+__device__ __forceinline__ unsigned tab_insert(int* tab, int bits, int w) {
     unsigned mask = (1u << bits) - 1;
     unsigned h = tab_home(w, bits);
     while (true) {
         int old = atomicCAS(tab + h, -1, w);
-        if (old == -1 || old == w) return;
+        if (old == -1 || old == w) return h;
         h = (h + 1) & mask;
     }
 }
@@ -246,21 +256,23 @@ __device__ __forceinline__ unsigned tc_fbit(int w, int bits) {
     return ((unsigned)w * 2654435761u) >> (32 - (bits + 3));
 }
 
-__device__ __forceinline__ void tab_insert_f(int* tab, unsigned* filt, int bits, int w) {
-    tab_insert(tab, bits, w);
+__device__ __forceinline__ unsigned tab_insert_f(int* tab, unsigned* filt, int bits, int w) {
+    const unsigned h = tab_insert(tab, bits, w);
     const unsigned f = tc_fbit(w, bits);
     atomicOr(filt + (f >> 5), 1u << (f & 31));
+    return h;
 }
 
 // Membership of w, for lanes whose filter bit is set (`maybe`), in the home
 // bucket.  `more`: the bucket is full and does not hold w, so the answer is
-// tab_rest's.
+// tab_rest's.  `slot`: where w is, on a hit.
 __device__ __forceinline__ bool tab_bucket(const int* tab, int bits, int w, bool maybe,
-                                           bool& more) {
+                                           bool& more, unsigned& slot) {
     const unsigned h = tab_home(w, bits);
     int4 q = make_int4(-1, -1, -1, -1);
     if (maybe) q = *reinterpret_cast<const int4*>(tab + h);
     const bool hit = (q.x == w) | (q.y == w) | (q.z == w) | (q.w == w);
+    slot = h + (q.x == w ? 0 : q.y == w ? 1 : q.z == w ? 2 : 3);
     // slots hold vertex ids (>= 0) or -1: the bucket is full iff the OR of
     // its slots is non-negative
     more = maybe & !hit & ((q.x | q.y | q.z | q.w) >= 0);
@@ -268,13 +280,13 @@ __device__ __forceinline__ bool tab_bucket(const int* tab, int bits, int w, bool
 }
 
 // The probe after a full home bucket, slot by slot (the table is at most
-// half full, so it meets an empty slot).
-__device__ __forceinline__ bool tab_rest(const int* tab, int bits, int w) {
+// half full, so it meets an empty slot): w's slot, or -1.
+__device__ __forceinline__ int tab_rest(const int* tab, int bits, int w) {
     const unsigned mask = (1u << bits) - 1;
     for (unsigned p = (tab_home(w, bits) + 4) & mask;; p = (p + 1) & mask) {
         const int x = tab[p];
-        if (x == w) return true;
-        if (x == -1) return false;
+        if (x == w) return (int)p;
+        if (x == -1) return -1;
     }
 }
 
@@ -291,7 +303,18 @@ struct TcView {
     const int32_t* fwd;      // oriented lists
     const long long* coff;   // candidate-list offsets
     const int32_t* cand;     // candidate lists C(z)
+    // edge-support mode (MODE 3) only:
+    const int32_t* feid;     // edge id of each fwd entry
+    const int32_t* ceid;     // edge id of each candidate entry
+    int* esup;               // per-edge triangle counts
 };
+
+// One triangle {u, v, w} found from u: credit its three edges (MODE 3).
+__device__ __forceinline__ void tc_credit_edges(int* esup, int e_uv, int e_vw, int e_uw) {
+    atomicAdd(esup + e_uv, 1);
+    atomicAdd(esup + e_vw, 1);
+    atomicAdd(esup + e_uw, 1);
+}
 
 // One warp: every (v, w) pair of u, w in N+(v) for v in the candidate
 // list C of u, probed against L = N+(u) (hash table `tab`, or binary search
@@ -304,7 +327,7 @@ struct TcView {
 template <int MODE, bool TAB>
 __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int32_t* __restrict__ C, int dc,
-    const int* tab, const unsigned* filt, int bits,
+    const int* tab, const unsigned* filt, const int* teid, int bits,
     int narrow_min, int* s_next, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
     int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
@@ -349,7 +372,9 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
         s_pref[lane + 1] = incl;
         if (lane == 0) s_pref[0] = 0;
         s_vb[lane] = xb;
-        s_v[lane] = v;
+        // MODE 3 keeps the candidate's edge id (u, v) instead of v
+        if (MODE == 3) s_v[lane] = idx < dc ? g.ceid[(C - g.cand) + idx] : 0;
+        else s_v[lane] = v;
         __syncwarp();
         const int T = s_pref[32];
         if (lane < T) {
@@ -395,24 +420,32 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                 // a lane's first lookup that needs probing past its home
                 // bucket waits until after the step (one divergent probe
                 // loop per step instead of one per pair)
-                int dw = -1, da = 0;
+                int dw = -1, da = 0, dk = 0;
+                // MODE 3: the edge (v, w) of pair k of candidate slot c
+                auto e_vw = [&](int c, int k) { return g.feid[s_vb[c] - s_pref[c] + k]; };
 #pragma unroll
                 for (int j = 0; j < kPairIlp; j++) {
                     const int w = wv[j];
                     if (!FULL && w < 0) continue;
                     bool hit;
+                    int e_uw = 0;   // MODE 3: edge (u, w)
                     if (TAB) {
                         const unsigned f = tc_fbit(w, bits);
                         bool more;
-                        hit = tab_bucket(tab, bits, w, (filt[f >> 5] >> (f & 31)) & 1u, more);
+                        unsigned slot;
+                        hit = tab_bucket(tab, bits, w, (filt[f >> 5] >> (f & 31)) & 1u, more, slot);
                         if (more) {
                             if (dw < 0) {
                                 dw = w;
                                 da = va[j];
+                                dk = k0 + 32 * j;
                             } else {
-                                hit = tab_rest(tab, bits, w);
+                                const int sl = tab_rest(tab, bits, w);
+                                hit = sl >= 0;
+                                slot = (unsigned)sl;
                             }
                         }
+                        if (MODE == 3 && hit) e_uw = teid[slot];
                     } else {
                         int lo = 0, hi = du;
                         while (lo < hi) {
@@ -420,6 +453,7 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                             if (L[mid] < w) lo = mid + 1; else hi = mid;
                         }
                         hit = lo < du && L[lo] == w;
+                        if (MODE == 3 && hit) e_uw = g.feid[(L - g.fwd) + lo];
                     }
                     c32 += hit ? 1u : 0u;
                     if (MODE == 1 && hit) {
@@ -427,13 +461,19 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                         atomicAdd(per_vertex + u, 1ull);
                         atomicAdd(per_vertex + s_v[va[j]], 1ull);
                     }
+                    if (MODE == 3 && hit)
+                        tc_credit_edges(g.esup, s_v[va[j]], e_vw(va[j], k0 + 32 * j), e_uw);
                 }
-                if (TAB && dw >= 0 && tab_rest(tab, bits, dw)) {
-                    c32++;
-                    if (MODE == 1) {
-                        atomicAdd(per_vertex + dw, 1ull);
-                        atomicAdd(per_vertex + u, 1ull);
-                        atomicAdd(per_vertex + s_v[da], 1ull);
+                if (TAB && dw >= 0) {
+                    const int sl = tab_rest(tab, bits, dw);
+                    if (sl >= 0) {
+                        c32++;
+                        if (MODE == 1) {
+                            atomicAdd(per_vertex + dw, 1ull);
+                            atomicAdd(per_vertex + u, 1ull);
+                            atomicAdd(per_vertex + s_v[da], 1ull);
+                        }
+                        if (MODE == 3) tc_credit_edges(g.esup, s_v[da], e_vw(da, dk), teid[sl]);
                     }
                 }
             };
@@ -457,6 +497,8 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           long long warp_work, long long item_work, int chunk, int narrow_min) {
     __shared__ __align__(16) int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
+    // MODE 3: edge id (u, w) of each table slot, kWarpTab per warp (dynamic)
+    extern __shared__ int s_teid[];
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
@@ -500,10 +542,14 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             for (int i = lane; i < (1 << bits); i += 32) tab[i] = -1;
             for (int i = lane; i < (1 << (bits - 2)); i += 32) filt[i] = 0u;
             __syncwarp();
-            for (int i = lane; i < du; i += 32) tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
+            int* teid = MODE == 3 ? s_teid + warp * kWarpTab : nullptr;
+            for (int i = lane; i < du; i += 32) {
+                const unsigned h = tab_insert_f(tab, filt, bits, g.fwd[ub + i]);
+                if (MODE == 3) teid[h] = g.feid[ub + i];
+            }
             __syncwarp();
             const unsigned long long cu = tc_vertex_warp<MODE, true>(
-                u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, bits, narrow_min, nullptr, g,
+                u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, teid, bits, narrow_min, nullptr, g,
                 s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
             mine += cu;
             if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
@@ -556,6 +602,7 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
         const int dc = rest < ipc ? rest : ipc;
         const int* tab = nullptr;
         unsigned* filt = (unsigned*)(s_dyn + tc_table_slots(cap));
+        int* teid = MODE == 3 ? (int*)(filt + tc_table_slots(cap) / 4) : nullptr;
         int bits = 0;
         if (threadIdx.x == 0) s_next = 0;
         if (du <= cap) {
@@ -564,18 +611,20 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             for (int j = threadIdx.x; j < (1 << bits); j += blockDim.x) s_dyn[j] = -1;
             for (int j = threadIdx.x; j < (1 << (bits - 2)); j += blockDim.x) filt[j] = 0u;
             __syncthreads();
-            for (int j = threadIdx.x; j < du; j += blockDim.x)
-                tab_insert_f(s_dyn, filt, bits, g.fwd[ub + j]);
+            for (int j = threadIdx.x; j < du; j += blockDim.x) {
+                const unsigned h = tab_insert_f(s_dyn, filt, bits, g.fwd[ub + j]);
+                if (MODE == 3) teid[h] = g.feid[ub + j];
+            }
             tab = s_dyn;
         }
         __syncthreads();
         const unsigned long long cu =
-            tab ? tc_vertex_warp<MODE, true>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, bits,
-                                             narrow_min, &s_next, g, s_pref[warp], s_vb[warp],
-                                             s_v[warp], per_vertex)
-                : tc_vertex_warp<MODE, false>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, bits,
-                                              narrow_min, &s_next, g, s_pref[warp], s_vb[warp],
-                                              s_v[warp], per_vertex);
+            tab ? tc_vertex_warp<MODE, true>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, teid,
+                                             bits, narrow_min, &s_next, g, s_pref[warp],
+                                             s_vb[warp], s_v[warp], per_vertex)
+                : tc_vertex_warp<MODE, false>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, teid,
+                                              bits, narrow_min, &s_next, g, s_pref[warp],
+                                              s_vb[warp], s_v[warp], per_vertex);
         mine += cu;
         if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
         __syncthreads();
@@ -592,7 +641,7 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
 
 }  // namespace
 
-void build_oriented(hn_graph* g, Oriented& o) {
+void build_oriented(hn_graph* g, Oriented& o, const int32_t* canon) {
     cudaStream_t s = g->stream;
     const int nV = g->nV;
     const long long m = g->nE;
@@ -613,13 +662,15 @@ void build_oriented(hn_graph* g, Oriented& o) {
     }
     o.offp.alloc((size_t)nV + 1, s);
     o.fwd.alloc((size_t)(m + 4), s);
+    if (canon) o.feid.alloc((size_t)(m + 4), s);
     HN_LAUNCH(k_orient_fill, grid, kB, 0, s, o.prefix.get(), nV, g->vtab, g->pool, pos.get(),
-              o.fwd.get(), o.offp.get(), splits.get(), (long long)splits.n - 1);
+              o.fwd.get(), o.offp.get(), splits.get(), (long long)splits.n - 1, canon,
+              canon ? o.feid.get() : (int32_t*)nullptr);
 }
 
 // C(z) for every vertex z: offsets coff (nV+1) and lists cand.
 void build_candidates(hn_graph* g, const Oriented& o, DevBuf<long long>& coff,
-                      DevBuf<int32_t>& cand) {
+                      DevBuf<int32_t>& cand, DevBuf<int32_t>* ceid) {
     cudaStream_t s = g->stream;
     const int nV = g->nV;
     const long long m = g->nE;   // bound on the oriented edge count (read on the device)
@@ -631,7 +682,8 @@ void build_candidates(hn_graph* g, const Oriented& o, DevBuf<long long>& coff,
     coff.alloc((size_t)nV + 1, s);
     cand.alloc((size_t)m + 4, s);
     HN_LAUNCH(k_cand<false>, grid, kB, 0, s, o.offp.get(), nV, o.fwd.get(), cnt.get(),
-              (const long long*)nullptr, (int32_t*)nullptr, splits.get(), (long long)splits.n - 1);
+              (const long long*)nullptr, (int32_t*)nullptr, splits.get(), (long long)splits.n - 1,
+              (const int32_t*)nullptr, (int32_t*)nullptr);
     {
         size_t tb = 0;
         HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.get(), coff.get(), nV + 1, s));
@@ -640,18 +692,23 @@ void build_candidates(hn_graph* g, const Oriented& o, DevBuf<long long>& coff,
         count_launch();
     }
     HN_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * ((size_t)nV + 1), s));
+    if (ceid) ceid->alloc((size_t)m + 4, s);
     HN_LAUNCH(k_cand<true>, grid, kB, 0, s, o.offp.get(), nV, o.fwd.get(), cnt.get(),
-              (const long long*)coff.get(), cand.get(), splits.get(), (long long)splits.n - 1);
+              (const long long*)coff.get(), cand.get(), splits.get(), (long long)splits.n - 1,
+              ceid ? (const int32_t*)o.feid.get() : (const int32_t*)nullptr,
+              ceid ? ceid->get() : (int32_t*)nullptr);
 }
 
 // mode 0: total only; 1: per-vertex counts (each triangle credited to its
 // three vertices); 2: owner counts (each triangle credited once, to its
 // lowest vertex in the degree orientation).
 // Dynamic shared memory of a listed-vertex table of up to `cap` entries:
-// its slots and their filter (8 bits per slot).
-constexpr size_t tc_table_bytes(int cap) {
-    return (size_t)tc_table_slots(cap) * sizeof(int) + (size_t)tc_table_slots(cap) / 4 * sizeof(unsigned);
+// its slots, their filter (8 bits per slot) and, for edge support, the edge
+// id of each slot.
+constexpr size_t tc_table_bytes(int cap, bool eid = false) {
+    return (size_t)tc_table_slots(cap) * (sizeof(int) + 1 + (eid ? sizeof(int) : 0));
 }
+constexpr int kCtaCapEid = 8192;   // largest table with edge ids (147 KB)
 
 template <int MODE>
 void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_counts,
@@ -663,29 +720,37 @@ void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_coun
     const int chunk = (int)knob(kKnobTcChunk);
     const int narrow_min = (int)knob(kKnobTcNarrowMin);
     const long long warp_work = knob(kKnobTcWarpWork), item_work = knob(kKnobTcItemWork);
+    constexpr bool eid = MODE == 3;
+    const int cap_max = eid ? kCtaCapEid : kCtaCap;
     const int mid_cap = (int)knob(kKnobTcMidCap);
-    const int cta_cap = (int)knob(kKnobTcCtaTableCap);
-    const size_t dyn_mid = tc_table_bytes(mid_cap), dyn_huge = tc_table_bytes(cta_cap);
+    const int cta_cap = (int)std::min<long long>(knob(kKnobTcCtaTableCap), cap_max);
+    const size_t dyn_mid = tc_table_bytes(mid_cap, eid), dyn_huge = tc_table_bytes(cta_cap, eid);
+    const size_t dyn_warp = eid ? (size_t)kTcWarps * kWarpTab * sizeof(int) : 0;
     static bool attr_set = false;   // one attribute per instantiation
     if (!attr_set) {
         HN_CUDA(cudaFuncSetAttribute(k_tc_cta<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)tc_table_bytes(kCtaCap)));
+                                     (int)tc_table_bytes(cap_max, eid)));
+        HN_CUDA(cudaFuncSetAttribute(k_tc_warp<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)dyn_warp));
         attr_set = true;
     }
     int mid_per_sm = 0;
     HN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mid_per_sm, k_tc_cta<MODE>,
                                                           kTcWarps * 32, dyn_mid));
     if (mid_per_sm < 1) mid_per_sm = 1;
-    HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, 0, s, view, g->nV, d_counts, d_total, counters,
-              big, big_cap, warp_cap, mid_cap, warp_work, item_work, chunk, narrow_min);
+    HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, dyn_warp, s, view, g->nV, d_counts, d_total,
+              counters, big, big_cap, warp_cap, mid_cap, warp_work, item_work, chunk, narrow_min);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms * mid_per_sm, kTcWarps * 32, dyn_mid, s, view,
               g->nV, d_counts, d_total, counters, big, big_cap, item_work, narrow_min, 0, mid_cap);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms, kTcWarps * 32, dyn_huge, s, view, g->nV,
               d_counts, d_total, counters, big, big_cap, item_work, narrow_min, 1, cta_cap);
 }
 
-unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_counts,
-                                   int mode) {
+namespace {
+
+// mode 0: total; 1: per-vertex counts; 2: owner counts; 3: edge supports.
+unsigned long long run_counting(hn_graph* g, const Oriented& o, int mode,
+                                unsigned long long* d_counts, int* esup) {
     cudaStream_t s = g->stream;
     unsigned long long* d_total = (unsigned long long*)g->d_scalar;
     HN_CUDA(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), s));
@@ -697,22 +762,39 @@ unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long
     // owner counts credit u, the lowest vertex of each triangle found from
     // u, so mode 2 keeps every edge with its tail: C(u) = N+(u)
     DevBuf<long long> coff;
-    DevBuf<int32_t> cand;
-    TcView view{o.offp.get(), o.fwd.get(), o.offp.get(), o.fwd.get()};
-    if (mode != 2 || !d_counts) {
-        build_candidates(g, o, coff, cand);
+    DevBuf<int32_t> cand, ceid;
+    TcView view{o.offp.get(), o.fwd.get(), o.offp.get(), o.fwd.get(), nullptr, nullptr, nullptr};
+    if (mode != 2) {
+        build_candidates(g, o, coff, cand, mode == 3 ? &ceid : nullptr);
         view.coff = coff.get();
         view.cand = cand.get();
     }
+    if (mode == 3) {
+        view.feid = o.feid.get();
+        view.ceid = ceid.get();
+        view.esup = esup;
+    }
     if (d_counts) HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * g->nV, s));
-    if (!d_counts)
-        launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), big_cap);
-    else if (mode == 2)
-        launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), big_cap);
-    else
-        launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), big_cap);
+    switch (mode) {
+        case 0: launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), big_cap); break;
+        case 1: launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), big_cap); break;
+        case 2: launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), big_cap); break;
+        default: launch_counting<3>(g, view, nullptr, d_total, counters, big.get(), big_cap);
+    }
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];
+}
+
+}  // namespace
+
+unsigned long long count_triangles(hn_graph* g, const Oriented& o, unsigned long long* d_counts,
+                                   int mode) {
+    return run_counting(g, o, d_counts ? mode : 0, d_counts, nullptr);
+}
+
+unsigned long long edge_support(hn_graph* g, const Oriented& o, int32_t* sup) {
+    HN_REQUIRE(o.feid.get() != nullptr, "edge support needs an orientation built with edge ids");
+    return run_counting(g, o, 3, nullptr, sup);
 }
 
 }  // namespace hn
