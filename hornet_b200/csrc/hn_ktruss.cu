@@ -22,6 +22,9 @@
 // lives on the (u < v) position.
 #include <cub/cub.cuh>
 
+#include <algorithm>
+#include <climits>
+
 #include "hn_graph.cuh"
 #include "hn_tc.cuh"
 
@@ -148,7 +151,7 @@ __device__ __forceinline__ void kt_triangle(int e, int e1, int e2, int K,
 }
 
 // Frontier edges whose shorter list has at most 32 entries: a thread each.
-// Longer ones go to a list for k_kt_peel_heavy (a warp each): the dense
+// Longer ones go to a list for k_kt_peel_heavy (a CTA each): the dense
 // core's hub-hub edges would otherwise run one long intersection per thread.
 __global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __restrict__ adj,
                           const int32_t* __restrict__ src, const int32_t* __restrict__ canon,
@@ -199,11 +202,10 @@ __global__ void k_kt_peel_heavy(const long long* __restrict__ off,
                                 int K, const unsigned char* __restrict__ alive,
                                 const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
                                 int32_t* __restrict__ NF, int* __restrict__ nNF) {
-    const int lane = threadIdx.x & 31;
+    // a CTA per heavy edge: its shorter list is searched by all threads,
+    // so a round whose frontier is a few hub-hub edges still spreads them
     const long long nh = *nheavy;
-    const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long h = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); h < nh;
-         h += warps) {
+    for (long long h = blockIdx.x; h < nh; h += gridDim.x) {
         const int e = heavy[h];
         const int u = src[e], v = eadj[e];
         const long long au = off[u], la = off[u + 1] - au;
@@ -211,7 +213,7 @@ __global__ void k_kt_peel_heavy(const long long* __restrict__ off,
         const bool swapped = la > lb;
         const long long pa = swapped ? bv : au, pb = swapped ? au : bv;
         const long long na = swapped ? lb : la, nb = swapped ? la : lb;
-        for (long long i = lane; i < na; i += 32) {
+        for (long long i = threadIdx.x; i < na; i += blockDim.x) {
             const int w = adj[pa + i];
             const long long p = lower_bound_dev(adj + pb, nb, w);
             if (p < nb && adj[pb + p] == w)
@@ -401,7 +403,7 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
                       (const int32_t*)ladj, src.get(), (const int32_t*)lcanon,
                       (const int32_t*)adj.get(), F.get(), nf, K, alive.get(), inF.get(), sup.get(),
                       NF.get(), nNF, H.get(), nheavy);
-            HN_LAUNCH(k_kt_peel_heavy, grid_for(g, (long long)nf * 32, 256), 256, 0, s,
+            HN_LAUNCH(k_kt_peel_heavy, std::min<long long>(nf, (long long)g->info.sms * 8), 256, 0, s,
                       (const long long*)loff, (const int32_t*)ladj, src.get(),
                       (const int32_t*)lcanon, (const int32_t*)adj.get(), (const int32_t*)H.get(),
                       (const int*)nheavy, K, alive.get(), inF.get(), sup.get(), NF.get(), nNF);
