@@ -244,7 +244,12 @@ k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
     }
 }
 
-using Tile = LbTile<kB, 4>;
+// Scatter tiles: 256 threads x 4 items, five CTAs per SM (the shared-memory
+// limit of a tile).  128 x 8, 128 x 4 (ten per SM) and 256 x 2 (eight per
+// SM) measured 13-52 % slower on the 10M-edge batch.
+constexpr int kSB = 256;
+constexpr int kScatterCtas = 5;
+using Tile = LbTile<kSB, 4>;
 constexpr int kStage = 512;    // batch entries of a tile staged in shared memory
 
 __device__ __forceinline__ int lower_bound32(const int32_t* a, int n, int32_t x) {
@@ -271,7 +276,7 @@ __device__ __forceinline__ int upper_bound32(const int32_t* a, int n, int32_t x)
 // run has at most kStage entries it is staged in shared memory, so the
 // per-item searches do not wait on global loads.
 template <bool INSERT>
-__global__ void __launch_bounds__(kB, 5)
+__global__ void __launch_bounds__(kSB, kScatterCtas)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
@@ -294,7 +299,7 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             s_K1 = INT_MIN;
         }
         int n = lb_tile_load(t, prefix, nseg, total, tile, splits, split_tiles);
-        for (int b = threadIdx.x; b <= t.nends; b += kB) {
+        for (int b = threadIdx.x; b <= t.nends; b += kSB) {
             long long s = t.seg0 + b;
             if (s < nseg) {
                 const long long st0 = t.seg_start(b);
@@ -328,12 +333,12 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
         __syncthreads();
         // all of this thread's old-list loads first (the pool is both read
         // and written here, so a plain loop would wait for each store)
-        constexpr int IPT = Tile::TILE / kB;
+        constexpr int IPT = Tile::TILE / kSB;
         int xs[IPT], bs[IPT];
         uint32_t ws[IPT];
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
-            const int i = threadIdx.x + k * kB;
+            const int i = threadIdx.x + k * kSB;
             bs[k] = -1;
             ws[k] = 0;
             if (i < n) {
@@ -346,7 +351,7 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
         const int K0 = s_K0, K1 = s_K1;
         const bool staged = K1 > K0 && K1 - K0 <= kStage;   // uniform in the CTA
         if (staged) {
-            for (int i = threadIdx.x; i < K1 - K0; i += kB) s_cd[i] = cdst[K0 + i];
+            for (int i = threadIdx.x; i < K1 - K0; i += kSB) s_cd[i] = cdst[K0 + i];
             __syncthreads();
         }
 #pragma unroll
@@ -354,7 +359,7 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             if (bs[k] < 0) continue;
             const int b = bs[k];
             const int x = xs[k];
-            const long long e = t.item0 + threadIdx.x + k * kB;   // global item
+            const long long e = t.item0 + threadIdx.x + k * kSB;   // global item
             const int nb = s_k1[b] - s_k0[b];
             // read only when nb > 0, and then [s_k0[b], s_k1[b]) lies in [K0, K1)
             const int32_t* B = staged ? s_cd + (s_k0[b] - K0) : cdst + s_k0[b];
@@ -693,18 +698,18 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     // tiles are read from the device prefix; the grid is persistent
     // five CTAs per SM (the shared-memory limit of the tile): each tile waits
     // on a short chain of dependent loads, so more resident tiles hide it
-    const long long grid_sc = (long long)g->info.sms * 5;
+    const long long grid_sc = (long long)g->info.sms * kScatterCtas;
     DevBuf<long long> splits;
     lb_splits(g, seg_work.get(), nseg, g->nE, Tile::TILE, splits);
     if (insert) {
-        HN_LAUNCH(k_scatter_old<true>, grid_sc, kB, 0, s, seg_work.get(), nseg,
+        HN_LAUNCH(k_scatter_old<true>, grid_sc, kSB, 0, s, seg_work.get(), nseg,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
                   g->vtab, g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
         HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), totals,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool,
                   (const uint32_t*)cw.get(), g->wpool);
     } else {
-        HN_LAUNCH(k_scatter_old<false>, grid_sc, kB, 0, s, seg_work.get(),
+        HN_LAUNCH(k_scatter_old<false>, grid_sc, kSB, 0, s, seg_work.get(),
                   nseg, seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
                   g->vtab, g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
     }
