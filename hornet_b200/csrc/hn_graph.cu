@@ -57,9 +57,10 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"tc.cta_table_cap", 16384, 32, 16384, false},
     {"tc.item_work", 1 << 18, 1024, 1 << 30, false},
     {"tc.warp_work", 1 << 16, 1024, 1 << 30, false},
+    {"tc.flip", 1, 0, 1, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}};
+    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}, {1}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

@@ -132,6 +132,7 @@ enum Knob {
     kKnobTcCtaTableCap,
     kKnobTcItemWork,
     kKnobTcWarpWork,
+    kKnobTcFlip,
     kNumKnobs
 };
 long long knob(Knob k);

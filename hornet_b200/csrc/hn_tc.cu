@@ -102,7 +102,8 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
 // triangles whichever endpoint counts it, so it is counted by the endpoint
 // whose out-list is the longer: that list is the hash table, the shorter
 // one is probed (cost min(d+(x), d+(y)) instead of d+(y)).  C(z) lists the
-// other endpoint of every edge z counts.  Order inside C(z) is immaterial.
+// other endpoint of every edge z counts, stored as ~x when z is the head of
+// x -> z (owner counts credit the tail x).  Order inside C(z) is immaterial.
 __device__ __forceinline__ bool cand_flip(long long dx, long long dy) { return dy > dx; }
 
 template <bool FILL>
@@ -170,7 +171,7 @@ k_cand(const long long* __restrict__ offp, int nV, const int32_t* __restrict__ f
                 if (FILL) cand[q] = ys[k];
             } else {
                 if (FILL) q = coff[ys[k]] + atomicAdd(cnt + ys[k], 1);
-                if (FILL) cand[q] = (int)(t.seg0 + b);
+                if (FILL) cand[q] = ~(int)(t.seg0 + b);   // flipped: ~tail
                 else atomicAdd(cnt + ys[k], 1);
             }
             if (FILL && ceid) ceid[q] = feid[t.item0 + i];
@@ -329,10 +330,10 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
     int u, const int32_t* __restrict__ L, int du, const int32_t* __restrict__ C, int dc,
     const int* tab, const unsigned* filt, const int* teid, int bits,
     int narrow_min, int* s_next, const TcView& g, int* s_pref /*33*/, long long* s_vb /*32*/,
-    int* s_v /*32*/, unsigned long long* __restrict__ per_vertex) {
+    int* s_v /*32*/, unsigned* s_fc /*32*/, unsigned long long* __restrict__ per_vertex) {
     const int lane = threadIdx.x & 31;
     const int lo_w = L[0], hi_w = L[du - 1];
-    unsigned long long cnt = 0;
+    unsigned long long cnt = 0, cnt_u = 0;   // all hits; MODE 2: hits owned by u
     auto claim = [&](int c) {
         if (!s_next) return c + 32;
         int t = 0;
@@ -342,9 +343,12 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
     for (int c0 = claim(-32); c0 < dc; c0 = claim(c0)) {
         int idx = c0 + lane;
         int dx = 0, v = 0;
+        bool flp = false;   // u is the head of v -> u
         long long xb = 0;
         if (idx < dc) {
             v = C[idx];
+            flp = v < 0;
+            if (flp) v = ~v;
             long long b0 = g.offp[v], b1 = g.offp[v + 1];
             const int32_t* lst = g.fwd + b0;
             int n = (int)(b1 - b0);
@@ -373,8 +377,12 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
         if (lane == 0) s_pref[0] = 0;
         s_vb[lane] = xb;
         // MODE 3 keeps the candidate's edge id (u, v) instead of v
+        // MODE 3 keeps the candidate's edge id; MODE 2 the owner of its
+        // triangles when that is v (flipped), else -1 (owner u)
         if (MODE == 3) s_v[lane] = idx < dc ? g.ceid[(C - g.cand) + idx] : 0;
+        else if (MODE == 2) s_v[lane] = idx < dc && flp ? v : -1;
         else s_v[lane] = v;
+        if (MODE == 2) s_fc[lane] = 0;
         __syncwarp();
         const int T = s_pref[32];
         if (lane < T) {
@@ -389,7 +397,7 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
             // of w are issued together, then probed.  FULL steps (every
             // lane's kPairIlp pairs exist; uniform in the warp) skip the
             // bounds checks; the last step of a group is partial.
-            unsigned c32 = 0;
+            unsigned c32 = 0, c32u = 0;   // hits of this group; MODE 2: those owned by u
             auto step = [&](int k0, auto full_tag) {
                 constexpr bool FULL = decltype(full_tag)::value;
                 int wv[kPairIlp], va[kPairIlp];
@@ -463,6 +471,10 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                     }
                     if (MODE == 3 && hit)
                         tc_credit_edges(g.esup, s_v[va[j]], e_vw(va[j], k0 + 32 * j), e_uw);
+                    if (MODE == 2 && hit) {
+                        if (s_v[va[j]] >= 0) atomicAdd(s_fc + va[j], 1u);
+                        else c32u++;
+                    }
                 }
                 if (TAB && dw >= 0) {
                     const int sl = tab_rest(tab, bits, dw);
@@ -474,6 +486,10 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                             atomicAdd(per_vertex + s_v[da], 1ull);
                         }
                         if (MODE == 3) tc_credit_edges(g.esup, s_v[da], e_vw(da, dk), teid[sl]);
+                        if (MODE == 2) {
+                            if (s_v[da] >= 0) atomicAdd(s_fc + da, 1u);
+                            else c32u++;
+                        }
                     }
                 }
             };
@@ -482,14 +498,22 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
                 step(k0, std::integral_constant<bool, true>());
             if (k0 < T) step(k0, std::integral_constant<bool, false>());
             cnt += c32;
+            cnt_u += c32u;
         }
         __syncwarp();
+        if (MODE == 2) {   // flipped candidates own their triangles
+            if (s_v[lane] >= 0 && s_fc[lane]) atomicAdd(per_vertex + s_v[lane], (unsigned long long)s_fc[lane]);
+            __syncwarp();
+        }
     }
+    if (MODE == 2) tc_credit_owner(per_vertex, u, cnt_u);
     return cnt;
 }
 
+// Five CTAs per SM for the plain count (48 registers, no spills); the
+// modes that credit vertices or edges carry more state and get 64.
 template <int MODE>
-__global__ void __launch_bounds__(kTcWarps * 32, 5)
+__global__ void __launch_bounds__(kTcWarps * 32, MODE == 0 ? 5 : 4)
 k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] mid, [2] huge list size*/,
@@ -502,6 +526,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
+    __shared__ unsigned s_fc[kTcWarps][32];   // MODE 2: hits owned by each candidate
     __shared__ unsigned long long s_sum[kTcWarps];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int* tab = s_tab[warp];
@@ -550,9 +575,8 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             __syncwarp();
             const unsigned long long cu = tc_vertex_warp<MODE, true>(
                 u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, teid, bits, narrow_min, nullptr, g,
-                s_pref[warp], s_vb[warp], s_v[warp], per_vertex);
+                s_pref[warp], s_vb[warp], s_v[warp], s_fc[warp], per_vertex);
             mine += cu;
-            if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
             __syncwarp();
         }
     }
@@ -585,6 +609,7 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
     __shared__ int s_pref[kTcWarps][33];
     __shared__ long long s_vb[kTcWarps][32];
     __shared__ int s_v[kTcWarps][32];
+    __shared__ unsigned s_fc[kTcWarps][32];   // MODE 2: hits owned by each candidate
     __shared__ unsigned long long s_sum[kTcWarps];
     __shared__ int s_next;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -621,12 +646,11 @@ k_tc_cta(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
         const unsigned long long cu =
             tab ? tc_vertex_warp<MODE, true>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, teid,
                                              bits, narrow_min, &s_next, g, s_pref[warp],
-                                             s_vb[warp], s_v[warp], per_vertex)
+                                             s_vb[warp], s_v[warp], s_fc[warp], per_vertex)
                 : tc_vertex_warp<MODE, false>(u, g.fwd + ub, du, g.cand + cb, dc, tab, filt, teid,
                                               bits, narrow_min, &s_next, g, s_pref[warp],
-                                              s_vb[warp], s_v[warp], per_vertex);
+                                              s_vb[warp], s_v[warp], s_fc[warp], per_vertex);
         mine += cu;
-        if (MODE == 2) tc_credit_owner(per_vertex, u, cu);
         __syncthreads();
     }
     for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
@@ -759,12 +783,15 @@ unsigned long long run_counting(hn_graph* g, const Oriented& o, int mode,
     // work items: at most one per vertex plus one per 32 candidates
     const long long big_cap = (long long)g->nV + g->nE / 32 + 2;
     DevBuf<long long> big((size_t)big_cap, s);
-    // owner counts credit u, the lowest vertex of each triangle found from
-    // u, so mode 2 keeps every edge with its tail: C(u) = N+(u)
+    // candidate lists: each oriented edge with the endpoint of the longer
+    // out-list (owner counts credit the edge's tail, the lowest vertex of
+    // the triangles it finds, which a flipped entry names)
+    // (tc.flip = 0: every edge stays with its tail, C(u) = N+(u); edge
+    // supports always use the lists)
     DevBuf<long long> coff;
     DevBuf<int32_t> cand, ceid;
     TcView view{o.offp.get(), o.fwd.get(), o.offp.get(), o.fwd.get(), nullptr, nullptr, nullptr};
-    if (mode != 2) {
+    if (mode == 3 || knob(kKnobTcFlip)) {
         build_candidates(g, o, coff, cand, mode == 3 ? &ceid : nullptr);
         view.coff = coff.get();
         view.cand = cand.get();

@@ -114,6 +114,9 @@ int hn_profile_report(char* buf, int64_t len);
  *                       above tc.warp_cap, the vertex goes to CTA work
  *                       items (1024..2^30, 65536)
  *   tc.item_work        pairs bound of one CTA work item (1024..2^30, 262144)
+ *   tc.flip             1: each oriented edge is counted by the endpoint
+ *                       with the longer out-list (the shorter list is
+ *                       probed); 0: by its tail (0..1, 1)
  *   msbfs.bottom_up     1: batched BFS runs bottom-up levels while the
  *                       frontier is large (bfs.do_alpha / do_beta switch) (0..1, 1)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)

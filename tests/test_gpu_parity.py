@@ -357,6 +357,7 @@ def test_tc_local(name):
     {"tc.warp_cap": 32, "tc.mid_cap": 36, "tc.cta_table_cap": 40},
     {"tc.warp_cap": 32, "tc.mid_cap": 32, "tc.cta_table_cap": 32, "tc.narrow_min": 8},
     {"tc.warp_work": 1024, "tc.item_work": 1024, "tc.warp_cap": 64},
+    {"tc.flip": 0, "tc.warp_work": 1024, "tc.item_work": 1024},
     {"tc.warp_work": 1024, "tc.item_work": 1500, "tc.mid_cap": 36, "tc.warp_cap": 32},
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
@@ -441,10 +442,20 @@ def test_ktruss_keep_runForKDynamic(K):
     assert off[-1] == int(keep.sum()) and h2.nE() == g.nE
 
 
+@pytest.mark.parametrize("flip", [1, 0])
 @pytest.mark.parametrize("name", ["rmat10", "er2000"])
-def test_tc_owner_counts(name):
+def test_tc_owner_counts(name, flip):
     """Owner counts: each triangle credited once, to its lowest vertex in the
-    degree orientation (oracle: |N+(u) ∩ N+(v)| summed over v in N+(u))."""
+    degree orientation (oracle: |N+(u) ∩ N+(v)| summed over v in N+(u)),
+    whichever endpoint of an oriented edge counts it (tc.flip)."""
+    H.tune_set("tc.flip", flip)
+    try:
+        _check_owner_counts(name)
+    finally:
+        H.tune_reset()
+
+
+def _check_owner_counts(name):
     g = GRAPHS[name]()
     h = build(g)
     o = O.orient_by_degree(g)
