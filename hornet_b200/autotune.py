@@ -42,7 +42,8 @@ SPACES: Dict[str, Dict[str, List[int]]] = {
     "tc": {"tc.warp_cap": [64, 128, 256, 512], "tc.chunk": [4, 16, 64],
            "tc.warp_ctas_per_sm": [4, 8, 12, 16], "tc.narrow_min": [0, 8, 32, 128],
            "tc.mid_cap": [1024, 2048, 4096], "tc.warp_work": [16384, 65536, 262144],
-           "tc.item_work": [65536, 262144, 1048576], "tc.flip": [0, 1]},
+           "tc.item_work": [65536, 262144, 1048576], "tc.flip": [0, 1],
+           "tc.thread_du": [0, 8, 16, 32], "tc.thread_dc": [16, 32, 128]},
 }
 
 DEFAULT_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")

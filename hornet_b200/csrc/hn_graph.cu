@@ -58,9 +58,11 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"tc.item_work", 1 << 18, 1024, 1 << 30, false},
     {"tc.warp_work", 1 << 16, 1024, 1 << 30, false},
     {"tc.flip", 1, 0, 1, false},
+    {"tc.thread_du", 16, 0, 64, false},
+    {"tc.thread_dc", 32, 1, 1024, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}, {1}};
+    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}, {1}, {16}, {32}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

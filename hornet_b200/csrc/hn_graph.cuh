@@ -133,6 +133,8 @@ enum Knob {
     kKnobTcItemWork,
     kKnobTcWarpWork,
     kKnobTcFlip,
+    kKnobTcThreadDu,
+    kKnobTcThreadDc,
     kNumKnobs
 };
 long long knob(Knob k);

@@ -510,6 +510,73 @@ __device__ __forceinline__ unsigned long long tc_vertex_warp(
     return cnt;
 }
 
+// Small vertices (d+(u) <= small_du, at most small_dc candidates; used with
+// the smaller-side assignment, so every probed list is at most d+(u) long):
+// a thread each, merging N+(u) with each candidate's list.  No table, no
+// warp-wide steps: the per-vertex overhead that dominates tiny vertices in
+// the warp kernel is gone.
+template <int MODE>
+__global__ void __launch_bounds__(256)
+k_tc_thread(TcView g, int nV, int small_du, int small_dc,
+            unsigned long long* __restrict__ per_vertex,
+            unsigned long long* __restrict__ total_out) {
+    __shared__ unsigned long long s_sum[8];
+    unsigned long long mine = 0;
+    for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < nV;
+         x += (long long)gridDim.x * blockDim.x) {
+        const int u = (int)x;
+        const long long ub = g.offp[u];
+        const int du = (int)(g.offp[u + 1] - ub);
+        const long long cb = g.coff[u];
+        const int dc = (int)(g.coff[u + 1] - cb);
+        if (du == 0 || dc == 0 || du > small_du || dc > small_dc) continue;
+        const int32_t* A = g.fwd + ub;
+        unsigned cu = 0;   // MODE 2: hits owned by u
+        for (int c = 0; c < dc; c++) {
+            int v = g.cand[cb + c];
+            const bool flp = v < 0;
+            if (flp) v = ~v;
+            const long long vb = g.offp[v];
+            const int dv = (int)(g.offp[v + 1] - vb);
+            const int32_t* Bv = g.fwd + vb;
+            unsigned hits = 0;
+            for (int i = 0, j = 0; i < du && j < dv;) {
+                const int a = A[i], b = Bv[j];
+                if (a == b) {
+                    hits++;
+                    if (MODE == 1) {
+                        atomicAdd(per_vertex + a, 1ull);
+                        atomicAdd(per_vertex + u, 1ull);
+                        atomicAdd(per_vertex + v, 1ull);
+                    }
+                    if (MODE == 3)
+                        tc_credit_edges(g.esup, g.ceid[cb + c], g.feid[vb + j], g.feid[ub + i]);
+                    i++;
+                    j++;
+                } else if (a < b) {
+                    i++;
+                } else {
+                    j++;
+                }
+            }
+            if (MODE == 2) {
+                if (flp) { if (hits) atomicAdd(per_vertex + v, (unsigned long long)hits); }
+                else cu += hits;
+            }
+            mine += hits;
+        }
+        if (MODE == 2 && cu) atomicAdd(per_vertex + u, (unsigned long long)cu);
+    }
+    for (int o = 16; o; o >>= 1) mine += __shfl_down_sync(0xFFFFFFFFu, mine, o);
+    if ((threadIdx.x & 31) == 0) s_sum[threadIdx.x >> 5] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < 8; w++) t += s_sum[w];
+        if (t) atomicAdd(total_out, t);
+    }
+}
+
 // Five CTAs per SM for the plain count (48 registers, no spills); the
 // modes that credit vertices or edges carry more state and get 64.
 template <int MODE>
@@ -518,7 +585,8 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
           unsigned long long* __restrict__ total_out,
           int* __restrict__ counters /*[0] next vertex, [1] mid, [2] huge list size*/,
           long long* __restrict__ big, long long big_cap, int warp_cap, int mid_cap,
-          long long warp_work, long long item_work, int chunk, int narrow_min) {
+          long long warp_work, long long item_work, int chunk, int narrow_min, int small_du,
+          int small_dc) {
     __shared__ __align__(16) int s_tab[kTcWarps][kWarpTab];
     __shared__ unsigned s_filt[kTcWarps][kWarpTab / 4];
     // MODE 3: edge id (u, w) of each table slot, kWarpTab per warp (dynamic)
@@ -543,6 +611,7 @@ k_tc_warp(TcView g, int nV, unsigned long long* __restrict__ per_vertex,
             const long long cb = g.coff[u];
             const int dc = (int)(g.coff[u + 1] - cb);
             if (du == 0 || dc == 0) continue;
+            if (du <= small_du && dc <= small_dc) continue;   // k_tc_thread's
             // every probed list of u is at most du long: dc * du bounds u's pairs
             if (du > warp_cap || (long long)dc * du > warp_work) {
                 // listed: one work item (u, chunk) per item_cands candidates;
@@ -737,7 +806,7 @@ constexpr int kCtaCapEid = 8192;   // largest table with edge ids (147 KB)
 template <int MODE>
 void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_counts,
                      unsigned long long* d_total, int* counters, long long* big,
-                     long long big_cap) {
+                     long long big_cap, bool flipped) {
     cudaStream_t s = g->stream;
     const long long gw = (long long)g->info.sms * knob(kKnobTcWarpCtasPerSm);
     const int warp_cap = (int)knob(kKnobTcWarpCap);
@@ -762,8 +831,16 @@ void launch_counting(hn_graph* g, const TcView& view, unsigned long long* d_coun
     HN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&mid_per_sm, k_tc_cta<MODE>,
                                                           kTcWarps * 32, dyn_mid));
     if (mid_per_sm < 1) mid_per_sm = 1;
+    // small vertices by thread (only with the smaller-side assignment, which
+    // bounds every probed list by d+(u))
+    const int small_du = flipped ? (int)knob(kKnobTcThreadDu) : 0;
+    const int small_dc = (int)knob(kKnobTcThreadDc);
+    if (small_du > 0)
+        HN_LAUNCH(k_tc_thread<MODE>, (long long)g->info.sms * 8, 256, 0, s, view, g->nV, small_du,
+                  small_dc, d_counts, d_total);
     HN_LAUNCH(k_tc_warp<MODE>, gw, kTcWarps * 32, dyn_warp, s, view, g->nV, d_counts, d_total,
-              counters, big, big_cap, warp_cap, mid_cap, warp_work, item_work, chunk, narrow_min);
+              counters, big, big_cap, warp_cap, mid_cap, warp_work, item_work, chunk, narrow_min,
+              small_du, small_dc);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms * mid_per_sm, kTcWarps * 32, dyn_mid, s, view,
               g->nV, d_counts, d_total, counters, big, big_cap, item_work, narrow_min, 0, mid_cap);
     HN_LAUNCH(k_tc_cta<MODE>, (long long)g->info.sms, kTcWarps * 32, dyn_huge, s, view, g->nV,
@@ -791,7 +868,8 @@ unsigned long long run_counting(hn_graph* g, const Oriented& o, int mode,
     DevBuf<long long> coff;
     DevBuf<int32_t> cand, ceid;
     TcView view{o.offp.get(), o.fwd.get(), o.offp.get(), o.fwd.get(), nullptr, nullptr, nullptr};
-    if (mode == 3 || knob(kKnobTcFlip)) {
+    const bool flipped = mode == 3 || knob(kKnobTcFlip);
+    if (flipped) {
         build_candidates(g, o, coff, cand, mode == 3 ? &ceid : nullptr);
         view.coff = coff.get();
         view.cand = cand.get();
@@ -802,11 +880,12 @@ unsigned long long run_counting(hn_graph* g, const Oriented& o, int mode,
         view.esup = esup;
     }
     if (d_counts) HN_CUDA(cudaMemsetAsync(d_counts, 0, sizeof(unsigned long long) * g->nV, s));
+    long long* bp = big.get();
     switch (mode) {
-        case 0: launch_counting<0>(g, view, nullptr, d_total, counters, big.get(), big_cap); break;
-        case 1: launch_counting<1>(g, view, d_counts, d_total, counters, big.get(), big_cap); break;
-        case 2: launch_counting<2>(g, view, d_counts, d_total, counters, big.get(), big_cap); break;
-        default: launch_counting<3>(g, view, nullptr, d_total, counters, big.get(), big_cap);
+        case 0: launch_counting<0>(g, view, nullptr, d_total, counters, bp, big_cap, flipped); break;
+        case 1: launch_counting<1>(g, view, d_counts, d_total, counters, bp, big_cap, flipped); break;
+        case 2: launch_counting<2>(g, view, d_counts, d_total, counters, bp, big_cap, flipped); break;
+        default: launch_counting<3>(g, view, nullptr, d_total, counters, bp, big_cap, flipped);
     }
     read_scalars(g, 1);
     return (unsigned long long)g->h_scalar[0];

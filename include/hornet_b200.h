@@ -117,6 +117,10 @@ int hn_profile_report(char* buf, int64_t len);
  *   tc.flip             1: each oriented edge is counted by the endpoint
  *                       with the longer out-list (the shorter list is
  *                       probed); 0: by its tail (0..1, 1)
+ *   tc.thread_du        with tc.flip: vertices with d+(u) up to this and at
+ *   tc.thread_dc        most tc.thread_dc candidates run a thread each,
+ *                       merging sorted lists (0 turns it off) (0..64, 16;
+ *                       1..1024, 32)
  *   msbfs.bottom_up     1: batched BFS runs bottom-up levels while the
  *                       frontier is large (bfs.do_alpha / do_beta switch) (0..1, 1)
  *   tc.warp_ctas_per_sm CTAs per SM of the warp-per-vertex kernel (1..16, 8)

@@ -358,6 +358,9 @@ def test_tc_local(name):
     {"tc.warp_cap": 32, "tc.mid_cap": 32, "tc.cta_table_cap": 32, "tc.narrow_min": 8},
     {"tc.warp_work": 1024, "tc.item_work": 1024, "tc.warp_cap": 64},
     {"tc.flip": 0, "tc.warp_work": 1024, "tc.item_work": 1024},
+    {"tc.thread_du": 64, "tc.thread_dc": 1024},
+    {"tc.thread_du": 0},
+    {"tc.thread_du": 4, "tc.thread_dc": 3},
     {"tc.warp_work": 1024, "tc.item_work": 1500, "tc.mid_cap": 36, "tc.warp_cap": 32},
     {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
     {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
