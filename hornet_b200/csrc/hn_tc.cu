@@ -53,12 +53,27 @@ k_orient_flags(const long long* __restrict__ prefix, int nV, const VRec* __restr
             }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += kB) {
-            long long e = t.item0 + i;
-            int b = t.seg[i];
-            int u = (int)(t.seg0 + b);
-            int v = pool[s_base[b] + e];
-            flag[e] = oriented_before(s_deg[b], u, vtab[v].deg, v) ? 1 : 0;
+        // all of a thread's loads first: neighbours, then their degrees
+        constexpr int IPT = Tile::TILE / kB;
+        int bs[IPT], vs[IPT], dv[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = threadIdx.x + k * kB;
+            bs[k] = -1;
+            if (i < n) {
+                bs[k] = t.seg[i];
+                vs[k] = pool[s_base[bs[k]] + t.item0 + i];
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < IPT; k++)
+            if (bs[k] >= 0) dv[k] = vtab[vs[k]].deg;
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            if (bs[k] < 0) continue;
+            const int b = bs[k];
+            const int u = (int)(t.seg0 + b);
+            flag[t.item0 + threadIdx.x + k * kB] = oriented_before(s_deg[b], u, dv[k], vs[k]) ? 1 : 0;
         }
         __syncthreads();
     }
@@ -82,13 +97,25 @@ k_orient_fill(const long long* __restrict__ prefix, int nV, const VRec* __restri
             if (u < nV) s_base[b] = vtab[u].off - t.seg_start(b);
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < n; i += kB) {
-            long long e = t.item0 + i;
-            int p = pos[e];
-            if (pos[e + 1] != p) {
-                fwd[p] = pool[s_base[t.seg[i]] + e];
-                if (feid) feid[p] = canon[e];   // edge id of the kept edge
+        constexpr int IPT = Tile::TILE / kB;
+        int ps[IPT], keep[IPT], vs[IPT];
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            const int i = threadIdx.x + k * kB;
+            keep[k] = 0;
+            if (i < n) {
+                const long long e = t.item0 + i;
+                ps[k] = pos[e];
+                keep[k] = pos[e + 1] != ps[k];
+                vs[k] = pool[s_base[t.seg[i]] + e];
             }
+        }
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            if (!keep[k]) continue;
+            const long long e = t.item0 + threadIdx.x + k * kB;
+            fwd[ps[k]] = vs[k];
+            if (feid) feid[ps[k]] = canon[e];   // edge id of the kept edge
         }
         __syncthreads();
     }
