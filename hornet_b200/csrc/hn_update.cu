@@ -172,7 +172,8 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
 __global__ void __launch_bounds__(kB)
 k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
        const long long* __restrict__ totals, bool insert, const VRec* __restrict__ vtab,
-       long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap, AllocState* st) {
+       long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap,
+       long long* __restrict__ seg_old_off, AllocState* st) {
     __shared__ int s_need[kNumClasses], s_push[kNumClasses];
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_need[c] = s_push[c] = 0;
     __syncthreads();
@@ -192,6 +193,7 @@ k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart
         }
         seg_ncap[s] = ncap;
         seg_work[s] = k > 0 ? r.deg : 0;
+        seg_old_off[s] = r.off;   // the scatter reads it without the seg_u -> vtab chain
     }
     __syncthreads();
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) {
@@ -280,7 +282,7 @@ __global__ void __launch_bounds__(kSB, kScatterCtas)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
-              const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
+              const long long* __restrict__ seg_old_off, int32_t* __restrict__ pool,
               const long long* __restrict__ splits, long long split_tiles,
               uint32_t* __restrict__ wpool) {
     __shared__ Tile t;
@@ -303,7 +305,7 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             long long s = t.seg0 + b;
             if (s < nseg) {
                 const long long st0 = t.seg_start(b);
-                const long long old_off = vtab[seg_u[s]].off;
+                const long long old_off = seg_old_off[s];
                 s_old[b] = old_off - st0;
                 s_new[b] = seg_new_off[s] - st0;
                 const int k0 = seg_kstart[s], k1 = seg_kstart[s + 1];
@@ -625,7 +627,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         count_launch();
     }
     DevBuf<int32_t> cdst(n, s), cseg(n, s), seg_u(n, s), seg_kstart(n + 1, s), seg_ncap(n, s);
-    DevBuf<long long> seg_work(n + 1, s), seg_new_off(n, s);
+    DevBuf<long long> seg_work(n + 1, s), seg_new_off(n, s), seg_old_off(n, s);
     long long* totals = g->d_scalar;
     DevBuf<uint32_t> cw;
     if (carry_w) cw.alloc(n, s);
@@ -637,7 +639,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     scan.release();
     // 4. plan
     HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
-              insert, g->vtab, seg_work.get(), seg_ncap.get(), st);
+              insert, g->vtab, seg_work.get(), seg_ncap.get(), seg_old_off.get(), st);
     // 5. host plan (the one synchronisation of the batch)
     cudaEvent_t plan_ev = nullptr;   // profiled: the stream's idle time across the plan
     if (g_profiling) profile_begin(s, &plan_ev);
@@ -704,14 +706,14 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     if (insert) {
         HN_LAUNCH(k_scatter_old<true>, grid_sc, kSB, 0, s, seg_work.get(), nseg,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
+                  seg_old_off.get(), g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
         HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), totals,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool,
                   (const uint32_t*)cw.get(), g->wpool);
     } else {
         HN_LAUNCH(k_scatter_old<false>, grid_sc, kSB, 0, s, seg_work.get(),
                   nseg, seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  g->vtab, g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
+                  seg_old_off.get(), g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
     }
     // 8. commit
     HN_LAUNCH(k_commit, grid_for(g, nseg, kB, 4), kB, 0, s, seg_u.get(), seg_kstart.get(),
