@@ -26,6 +26,7 @@ import json
 import os
 import statistics
 import subprocess
+import tempfile
 import sys
 import time
 
@@ -89,7 +90,7 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.path = os.path.join(tempfile.gettempdir(), f"hn_clocks_{os.getpid()}.csv")
 
     def start(self):
         os.makedirs(os.path.dirname(self.path), exist_ok=True)

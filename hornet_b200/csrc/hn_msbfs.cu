@@ -2,9 +2,8 @@
 // multi-source BFS after Then et al., "The More the Merrier: Efficient
 // Multi-Source Graph Traversal", VLDB 2015).
 //
-// The batching pattern of the north star for the hot path: many BFS sources
-// (and, on a disjoint union, many small graphs) in one persistent launch
-// captured in a CUDA graph.  Each vertex carries three 64-bit masks:
+// Batching: many BFS sources (and, on a disjoint union, many small graphs)
+// in one persistent launch captured in a CUDA graph.  Each vertex carries three 64-bit masks:
 //   seen[v]  slots that have reached v,
 //   front[v] slots for which v is on the current frontier,
 //   nxt[v]   slots that reach v at this level (OR-accumulated).
