@@ -53,3 +53,23 @@ def test_save_and_apply(tmp_path):
     assert A.apply_saved("B200", sig, p) == {"tc.warp_cap": 256, "tc.chunk": 4}
     assert H.tune_get("tc.warp_cap") == 256
     assert A.apply_saved("other", sig, p) is None
+
+
+def test_search_spaces_and_saved_knobs_are_registered():
+    """Every value the autotuner may try, and every knob saved in the
+    shipped tuned file, is accepted by the library's registry."""
+    import json
+    names = set(H.tune_names())
+    for space in A.SPACES.values():
+        for knob, values in space.items():
+            assert knob in names, knob
+            for v in values:
+                H.tune_set(knob, v)
+                assert H.tune_get(knob) == v
+    with open(A.DEFAULT_PATH) as f:
+        db = json.load(f)
+    for dev in db.values():
+        for rec in dev.values():
+            for knob, v in rec["knobs"].items():
+                H.tune_set(knob, v)
+                assert H.tune_get(knob) == v
