@@ -34,7 +34,7 @@ import numpy as np
 from . import tune_get, tune_names, tune_reset, tune_set
 
 SPACES: Dict[str, Dict[str, List[int]]] = {
-    "bfs": {"bfs.ctas_per_sm": [4, 6, 8, 12, 16], "bfs.dynamic_chunks": [0, 1],
+    "bfs": {"bfs.ctas_per_sm": [4, 6, 8, 9, 12, 16], "bfs.dynamic_chunks": [0, 1],
             "bfs.warp_strided": [0, 1]},
     "bfs_do": {"bfs.do_alpha": [4, 8, 14, 24, 48], "bfs.do_beta": [8, 24, 64, 256]},
     "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8],

@@ -256,7 +256,7 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
 // Breadth-First Search", SC 2012).  Both produce the next frontier queue, so
 // the direction may change at any level; distances are the same either way.
 template <bool DO>
-__global__ void __launch_bounds__(kBfsBlock, 8)
+__global__ void __launch_bounds__(kBfsBlock, 9)
 k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
     __shared__ BfsSmem sm;
     const int level = st->level;

@@ -40,7 +40,7 @@ struct KnobDef {
     bool pow2;   // value must be a power of two
 };
 const KnobDef kKnobs[kNumKnobs] = {
-    {"bfs.ctas_per_sm", 8, 1, 16, false},
+    {"bfs.ctas_per_sm", 9, 1, 16, false},
     {"bfs.do_alpha", 14, 1, 1 << 20, false},
     {"bfs.do_beta", 24, 1, 1 << 20, false},
     {"msbfs.block", 256, 128, 512, true},
@@ -62,7 +62,7 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"tc.thread_dc", 32, 1, 1024, false},
 };
 std::atomic<long long> g_knob[kNumKnobs] = {
-    {8}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}, {1}, {16}, {32}};
+    {9}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}, {1}, {16}, {32}};
 
 int knob_index(const char* name) {
     if (!name) return -1;

@@ -92,7 +92,7 @@ int hn_profile_report(char* buf, int64_t len);
  * effect on the next call).  An autotuner sets them; the defaults are the
  * built-in values.  Knobs:
  *   bfs.ctas_per_sm     CTAs per SM of the BFS level kernel, 128 threads
- *                       each (1..16, 8)
+ *                       each (1..16, 9)
  *   bfs.do_alpha        direction-optimising switch to bottom-up when the
  *                       frontier's edges exceed unexplored edges / alpha (14)
  *   bfs.do_beta         back to top-down below nV / beta frontier vertices (24)
