@@ -4,6 +4,8 @@ graph::WCC) and the reference's example graphs.
 
     python tests/golden/make_golden.py [/path/to/hornet/source]
 
+The source path defaults to the environment variable HORNET_REFERENCE.
+
 Run in a container that has the reference sources; the fixtures are
 committed so the tests never need them.  Each fixture holds:
   off, adj          undirected CSR as GraphStd builds it (mirror, drop self
@@ -24,7 +26,7 @@ sys.path.insert(0, ROOT)
 
 from oracle import oracle as O  # noqa: E402
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HORNET_REFERENCE", "")
 
 
 def fixture(name: str, path: str, nsrc: int = 4) -> None:
@@ -38,9 +40,26 @@ def fixture(name: str, path: str, nsrc: int = 4) -> None:
     print(f"{name}: nV={g.nV} nE={g.nE} oriented={og.nE}")
 
 
+def fixture_bin(name: str, path: str) -> None:
+    """The reference's own GraphStd binary file: its SHA-256 and the CSR it
+    holds (header: 6 bytes, nV, nE, 16 more bytes; then off[nV+1], adj[nE])."""
+    import hashlib
+    raw = open(path, "rb").read()
+    nV = int.from_bytes(raw[6:10], "little")
+    nE = int.from_bytes(raw[10:14], "little")
+    body = np.frombuffer(raw[30:], np.int32)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), off=body[: nV + 1].copy(),
+                        adj=body[nV + 1: nV + 1 + nE].copy(),
+                        sha256=np.frombuffer(hashlib.sha256(raw).digest(), np.uint8),
+                        size=np.int64(len(raw)))
+    print(f"{name}: nV={nV} nE={nE} bytes={len(raw)}")
+
+
 def main() -> None:
+    assert REF, "give the reference source path (argument or HORNET_REFERENCE)"
     assert O.ref_available(), "build oracle/_ref first: make -C oracle ref"
     ex = os.path.join(REF, "example")
+    fixture_bin("G_bin", os.path.join(ex, "G.bin"))
     fixture("G", os.path.join(ex, "G.mtx"))
     fixture("G_cc2", os.path.join(ex, "G_cc2.mtx"))
     fixture("rome99", os.path.join(ex, "rome99.gr"))

@@ -1,6 +1,9 @@
 """CPU: GraphStd binary (.bin) and Matrix Market formats, pinned against the
-reference: byte-identical to the reference's own example/G.bin, and read
-back by the reference's GraphStd reader (oracle/_ref) when it was built."""
+reference: byte-identical to the reference's own example/G.bin (its SHA-256
+and CSR are the fixture tests/golden/G_bin.npz, made by
+tests/golden/make_golden.py), and read back by the reference's GraphStd
+reader (oracle/_ref) when it was built."""
+import hashlib
 import os
 import tempfile
 
@@ -12,7 +15,6 @@ from oracle import oracle as O
 from tests import helpers as T
 
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
-REF_G_BIN = "/root/reference/example/G.bin"
 
 
 def test_bin_roundtrip():
@@ -25,21 +27,19 @@ def test_bin_roundtrip():
     np.testing.assert_array_equal(adj, g.adj)
 
 
-@pytest.mark.skipif(not os.path.exists(REF_G_BIN), reason="reference example not present")
 def test_bin_matches_reference_example_bytes():
     """example/G.mtx read as DIRECTED by GraphStd and written with
     writeBinary is example/G.bin; the same CSR written here gives the same
-    bytes."""
-    ref = open(REF_G_BIN, "rb").read()
-    nV = int.from_bytes(ref[6:10], "little")
-    nE = int.from_bytes(ref[10:14], "little")
-    body = np.frombuffer(ref[30:], np.int32)
-    off, adj = body[: nV + 1], body[nV + 1: nV + 1 + nE]
+    bytes (same length and SHA-256), and reads back as the same CSR."""
+    z = np.load(os.path.join(GOLD, "G_bin.npz"))
+    off, adj = z["off"], z["adj"]
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "G.bin")
         H.write_bin(p, off, adj)
-        assert open(p, "rb").read() == ref
-        o2, a2 = H.read_bin(REF_G_BIN)
+        raw = open(p, "rb").read()
+        assert len(raw) == int(z["size"])
+        assert hashlib.sha256(raw).digest() == z["sha256"].tobytes()
+        o2, a2 = H.read_bin(p)
     np.testing.assert_array_equal(o2, off)
     np.testing.assert_array_equal(a2, adj)
 

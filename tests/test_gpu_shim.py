@@ -18,7 +18,10 @@ EXE = os.path.join(ROOT, "hornet_b200", "_lib", "hn_shim_test")
 
 
 def test_shim_reference_style_program():
-    assert os.path.exists(EXE), "build the shim test: make -C tests/shim"
+    # the executable is a build product (not tracked): make it when missing
+    # or older than the library
+    subprocess.run(["make", "-C", os.path.join(ROOT, "tests", "shim")], check=True)
+    assert os.path.exists(EXE)
     g = T.rmat_graph(10, 8, seed=31)
     rng = np.random.default_rng(9)
     bs = rng.integers(0, g.nV, 2000).astype(np.int32)
