@@ -361,7 +361,7 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
         prof_vis += v
     rep = H.profile_report()
     H.profile_enable(False)
-    roof = roofline_entry(H, "k_bfs_level<false>", lambda: 8 * prof_edges + 20 * prof_vis, peak,
+    roof = roofline_entry(H, ["k_bfs_level<false>", "k_bfs_wlevel<false>"], lambda: 8 * prof_edges + 20 * prof_vis, peak,
                           peak_kind, rep, f"R-MAT scale {scale} BFS, {min(K, 16)} sources")
 
     also = {}

@@ -7,8 +7,9 @@ The knobs are load-balancing bin thresholds and launch shapes:
   tc.warp_ctas_per_sm — grid of the warp kernel;
 * msbfs.block — block size of the batched BFS (128/256/512 threads, the
   same 2048-edge chunks); msbfs.ctas_per_sm — its grid;
-* bfs.ctas_per_sm — grid of the BFS level kernel; bfs.dynamic_chunks —
-  frontier chunks taken from a counter instead of round-robin;
+* bfs.kernel — the warp-chunk (1) or CTA-chunk (0) BFS level kernel;
+  bfs.warp_ctas_per_sm / bfs.ctas_per_sm — their grids; bfs.dynamic_chunks —
+  frontier chunks taken from a counter instead of round-robin (CTA kernel);
   bfs.do_alpha / do_beta — the direction-optimising switch thresholds.
 
 `tune` runs coordinate descent over a knob space: every candidate value of a
@@ -34,7 +35,8 @@ import numpy as np
 from . import tune_get, tune_names, tune_reset, tune_set
 
 SPACES: Dict[str, Dict[str, List[int]]] = {
-    "bfs": {"bfs.ctas_per_sm": [4, 6, 8, 9, 12, 16], "bfs.dynamic_chunks": [0, 1],
+    "bfs": {"bfs.kernel": [1, 0], "bfs.warp_ctas_per_sm": [2, 3, 4, 6, 8],
+            "bfs.ctas_per_sm": [4, 6, 8, 9, 12, 16], "bfs.dynamic_chunks": [0, 1],
             "bfs.warp_strided": [0, 1]},
     "bfs_do": {"bfs.do_alpha": [4, 8, 14, 24, 48], "bfs.do_beta": [8, 24, 64, 256]},
     "msbfs": {"msbfs.block": [128, 256, 512], "msbfs.ctas_per_sm": [2, 4, 6, 8],

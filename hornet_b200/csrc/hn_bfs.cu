@@ -7,33 +7,41 @@
 // least three host synchronisations per level.
 //
 // Here a whole BFS is ONE CUDA-graph launch: an init kernel, then a
-// conditional WHILE node whose body is a single persistent expand kernel.
+// conditional WHILE node whose body is a single persistent level kernel.
 //   * Frontier entries are (vertex, adjacency base, edge offset).  The edge
 //     offset is the exclusive prefix of the frontier's degrees; it comes out
-//     of the enqueue itself: one 64-bit atomicAdd of (degree << 32 | 1) per
-//     warp hands out the queue slot (low word) and the edge offset (high
+//     of the enqueue itself: one 64-bit atomicAdd of (degree sum << 32 |
+//     count) hands out the queue slots (low word) and the edge offsets (high
 //     word) together, so offsets are ordered like slots and no scan runs.
-//   * The frontier's edge space is cut into chunks of kChunk edges.  The
+//   * The frontier's edge space is cut into chunks of 2^cshift edges.  The
 //     vertex that covers the first edge of each chunk records itself in
-//     chunk_seg[] when it is enqueued, so the expand kernel finds a chunk's
-//     vertex window with two loads — no search in global memory.  Only
-//     vertices with at least one edge are queued, so a chunk spans at most
-//     kChunk + 1 queue entries.
+//     chunk[] when it is enqueued, so a chunk finds its vertex window with
+//     two loads -- no search in global memory.  Only vertices with at least
+//     one edge are queued, so a chunk of E edges spans at most E + 1 queue
+//     entries.
 //   * Visited-bitmap probes go through L1 (ld.ca): on power-law graphs most
 //     edges point at a few hubs, and L2-only probes of their bitmap words
 //     turn into a hot spot on a few L2 slices.  A stale L1 copy can only
 //     miss bits set during this level (bits never clear), which costs an
-//     extra atomicOr and never a wrong claim.
-//   * A CTA stages the window's (edge offset, adjacency base) pairs in
-//     shared memory; each thread takes kIpt consecutive edges, finds its
-//     first vertex by a shared-memory binary search, then issues all kIpt
-//     neighbour loads and all kIpt visited-bitmap probes back to back (high
-//     memory-level parallelism), and claims new vertices with atomicOr on
-//     the bitmap (nV/8 bytes, L2-resident): each vertex is enqueued and its
-//     distance written exactly once.
+//     extra atomicOr and never a wrong claim.  New vertices are claimed with
+//     atomicOr on the bitmap (nV/8 bytes, L2-resident), so each vertex is
+//     enqueued and its distance written exactly once.
 //   * The last CTA of a level (ticket counter) seals the next frontier and
 //     sets the WHILE condition with cudaGraphSetConditional; the loop also
 //     stops after nV levels, so it always terminates.
+//
+// Two level kernels share this frontier format (knob bfs.kernel):
+//   * k_bfs_wlevel (default): every WARP runs on its own.  It takes 256-edge
+//     chunks round-robin, reads its window, loads its 8 x 32 neighbours
+//     lane-strided (each load instruction reads 32 consecutive edges),
+//     probes and claims, and appends the claims to a warp-private list in
+//     shared memory.  The list is enqueued 32 vertices at a time with one
+//     atomic per 32 claims.  There is no CTA barrier inside a level, so the
+//     resident warps are independent chains of loads.  Windows of at most
+//     32 vertices stay in registers: a lane finds the vertex of each of its
+//     edges with one OR-reduction, one ballot and one shuffle.
+//   * k_bfs_level: a CTA of 128 threads per 1024-edge chunk, with the window
+//     staged in shared memory and a CTA-wide enqueue (one atomic per chunk).
 // Distances equal the reference's: level-synchronous, INF = INT32_MAX.
 //
 // hn_bfs_do runs the same graph with a level kernel that may switch to
@@ -46,7 +54,14 @@ namespace hn {
 
 constexpr int kBfsBlock = 128;
 constexpr int kIpt = 8;                          // edges per thread per chunk
-constexpr int kChunk = kBfsBlock * kIpt;         // edges per chunk
+constexpr int kChunk = kBfsBlock * kIpt;         // edges per CTA chunk (k_bfs_level)
+constexpr int kChunkShiftCta = 10;               // log2(kChunk)
+constexpr int kWBlock = 256;                     // k_bfs_wlevel: threads per CTA
+constexpr int kWIpt = 8;                         // edges per lane per warp chunk
+constexpr int kWChunk = 32 * kWIpt;              // edges per warp chunk
+constexpr int kChunkShiftWarp = 8;               // log2(kWChunk)
+constexpr int kWList = kWChunk + 32;             // claim list capacity per warp
+static_assert(kChunk == 1 << kChunkShiftCta && kWChunk == 1 << kChunkShiftWarp, "chunk sizes");
 
 struct BfsState {
     unsigned long long cnt[3];   // frontier counters: (edge total << 32) | size
@@ -75,7 +90,7 @@ struct BfsState {
     int warp_strided;            // 1: a warp's edges are lane-strided (coalesced loads)
     int cont;                    // 1 while another level follows (host-driven loop)
     int host_driven;             // 1: no conditional node (levels launched by the host)
-    int pad3;
+    int cshift;                  // log2 of the chunk size of chunk[]
 };
 
 struct BfsGraph {
@@ -91,6 +106,7 @@ struct BfsGraph {
     cudaGraph_t graph[2] = {nullptr, nullptr};      // [0] top-down, [1] direction-optimising
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     unsigned grid = 0;                              // level-kernel CTAs baked in
+    int kernel = -1;                                // bfs.kernel baked in
     // multi-source calls: pinned per-source states (the next source's state
     // is staged while the previous BFS runs), a copy stream and events so a
     // host-bound distance array is copied out while the next BFS runs
@@ -103,11 +119,12 @@ struct BfsGraph {
 
 namespace {
 
-// Record queue slot `pos` as the owner of every chunk whose first edge lies
-// in [off, off + d).
-__device__ __forceinline__ void mark_chunks(int32_t* chunk, unsigned off, unsigned d, int pos) {
-    unsigned c0 = (off + kChunk - 1) / kChunk;
-    unsigned c1 = (off + d - 1) / kChunk;
+// Record queue slot `pos` as the owner of every chunk (2^cs edges) whose
+// first edge lies in [off, off + d).
+__device__ __forceinline__ void mark_chunks(int32_t* chunk, unsigned off, unsigned d, int pos,
+                                            int cs) {
+    unsigned c0 = (off + (1u << cs) - 1) >> cs;
+    unsigned c1 = (off + d - 1) >> cs;
     for (unsigned c = c0; c <= c1; c++) chunk[c] = pos;
 }
 
@@ -126,7 +143,7 @@ __global__ void k_bfs3_init(BfsState* st) {
     unsigned d = (unsigned)r.deg;
     // chunk marks of a high-degree source are spread over the grid
     if (d > 0) {
-        unsigned nc = (d - 1) / kChunk + 1;
+        unsigned nc = ((d - 1) >> st->cshift) + 1;
         for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < nc;
              c += (long long)gridDim.x * blockDim.x)
             st->chunk[0][c] = 0;
@@ -172,7 +189,7 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
                                             const VRec* __restrict__ vtab, int32_t* dist,
                                             unsigned long long* cout, int32_t* nqv,
                                             long long* nqbase, unsigned* nqoff, int32_t* nchunk,
-                                            int& found) {
+                                            int cs, int& found) {
     const int lane = threadIdx.x & 31;
     if (threadIdx.x == 0) sm.nclaimed = 0;
     __syncthreads();
@@ -241,12 +258,313 @@ __device__ __forceinline__ void bfs_enqueue(BfsSmem& sm, const int (&w)[kIpt],
             nqv[pos] = v;
             nqbase[pos] = r.off;
             nqoff[pos] = off;
-            mark_chunks(nchunk, off, (unsigned)r.deg, pos);
+            mark_chunks(nchunk, off, (unsigned)r.deg, pos, cs);
             pos++;
             off += (unsigned)r.deg;
         }
     }
     __syncthreads();
+}
+
+// End of a level, called by every thread of every CTA: the visited count
+// (one atomic per warp), then the last CTA seals the next frontier, picks the
+// next direction and decides whether to loop.
+template <bool DO>
+__device__ __forceinline__ void bfs_level_end(BfsState* st, cudaGraphConditionalHandle cond,
+                                              int found, int level, int nq, unsigned total,
+                                              unsigned long long* cout, unsigned* nqoff) {
+    const int lane = threadIdx.x & 31;
+    for (int o = 16; o; o >>= 1) found += __shfl_down_sync(0xFFFFFFFFu, found, o);
+    if (lane == 0 && found) atomicAdd((unsigned long long*)&st->visited, (unsigned long long)found);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        unsigned tk = atomicAdd(&st->ticket, 1u);
+        if (tk == gridDim.x - 1) {
+            __threadfence();
+            unsigned long long cn = atomicAdd(cout, 0ull);
+            unsigned nn = (unsigned)(cn & 0xFFFFFFFFull);
+            unsigned long long mf = cn >> 32;
+            nqoff[nn] = (unsigned)mf;
+            st->ticket = 0;
+            st->next_chunk = 0;
+            st->scanned += total;
+            st->level = level + 1;
+            if (DO) {
+                // Beamer's switch: to bottom-up when the next frontier's edges
+                // exceed 1/alpha of the unexplored edges (alpha = 14 by
+                // default), back to top-down when the frontier falls below
+                // nV/beta vertices (beta = 24) and is shrinking
+                st->edges_visited += (long long)mf;
+                long long mu = st->m_total - st->edges_visited;
+                if (st->mode == 0) {
+                    if ((long long)mf * st->alpha > mu) st->mode = 1;
+                } else {
+                    if ((long long)nn * st->beta < st->nV && nn < (unsigned)nq) st->mode = 0;
+                }
+            }
+            const unsigned more = (nn > 0 && level < st->nV) ? 1u : 0u;
+            st->cont = (int)more;
+            if (!st->host_driven) cudaGraphSetConditional(cond, more);
+        }
+    }
+}
+
+// Warp-private shared memory of k_bfs_wlevel.
+struct WarpSmem {
+    long long base[kWChunk + 1];   // window: pool index = base + edge (large windows)
+    unsigned start[kWChunk + 2];   // window edge offsets (+ end)
+    int list[kWList];              // claimed vertices not yet enqueued
+};
+
+// Enqueue the warp's claimed vertices 32 at a time (all of them when `all`,
+// else only whole groups of 32; the rest moves to the front of the list and
+// the new list length is returned).  Per group: the vertex records are read,
+// distances written, then one 64-bit atomicAdd reserves the group's queue
+// slots and edge range.  A vertex that spans many chunks has its chunk marks
+// written by the whole warp.  Called by all 32 lanes with the same n.
+__device__ __forceinline__ int warp_flush(int* __restrict__ list, int n, bool all, int level,
+                                          const VRec* __restrict__ vtab, int32_t* dist,
+                                          unsigned long long* cout, int32_t* nqv,
+                                          long long* nqbase, unsigned* nqoff, int32_t* nchunk,
+                                          int& found) {
+    const int lane = threadIdx.x & 31;
+    const unsigned kFull = 0xFFFFFFFFu;
+    int done = 0;
+    while (all ? done < n : n - done >= 32) {
+        const int i = done + lane;
+        const bool have = i < n;
+        const int v = have ? list[i] : 0;
+        VRec r = {0, 0, 0};
+        if (have) {
+            r = vtab[v];
+            dist[v] = level;
+            found++;
+        }
+        const unsigned d = (unsigned)r.deg;
+        const unsigned long long mine = d ? (((unsigned long long)d << 32) | 1ull) : 0ull;
+        unsigned long long incl = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long x = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += x;
+        }
+        unsigned long long base = 0;
+        if (lane == 31 && incl) base = atomicAdd(cout, incl);
+        base = __shfl_sync(kFull, base, 31);
+        const unsigned long long at = base + incl - mine;
+        const int pos = (int)(at & 0xFFFFFFFFull);
+        const unsigned off = (unsigned)(at >> 32);
+        unsigned c0 = 0, c1 = 0;
+        bool big = false;
+        if (d) {
+            nqv[pos] = v;
+            nqbase[pos] = r.off;
+            nqoff[pos] = off;
+            c0 = (off + kWChunk - 1) >> kChunkShiftWarp;
+            c1 = (off + d - 1) >> kChunkShiftWarp;
+            big = c1 >= c0 + 8;
+            if (!big)
+                for (unsigned c = c0; c <= c1; c++) nchunk[c] = pos;
+        }
+        unsigned bigm = __ballot_sync(kFull, big);
+        while (bigm) {
+            const int src = __ffs(bigm) - 1;
+            bigm &= bigm - 1;
+            const unsigned b0 = __shfl_sync(kFull, c0, src);
+            const unsigned b1 = __shfl_sync(kFull, c1, src);
+            const int bp = __shfl_sync(kFull, pos, src);
+            for (unsigned c = b0 + lane; c <= b1; c += 32) nchunk[c] = bp;
+        }
+        done += 32;
+    }
+    if (all || done == 0) return all ? 0 : n;
+    const int rem = n - done;
+    __syncwarp();
+    const int x = lane < rem ? list[done + lane] : 0;
+    __syncwarp();
+    if (lane < rem) list[lane] = x;
+    __syncwarp();
+    return rem;
+}
+
+// Append the lanes' claimed vertices (bit k of `claim` set: w[k] claimed) to
+// the warp list and flush whole groups of 32.
+__device__ __forceinline__ void warp_claims(WarpSmem& sm, int& nlist, const int (&w)[kWIpt],
+                                            unsigned claim, int level,
+                                            const VRec* __restrict__ vtab, int32_t* dist,
+                                            unsigned long long* cout, int32_t* nqv,
+                                            long long* nqbase, unsigned* nqoff, int32_t* nchunk,
+                                            int& found) {
+    const int lane = threadIdx.x & 31;
+    const unsigned kFull = 0xFFFFFFFFu;
+    const int mine = __popc(claim);
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int x = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += x;
+    }
+    const int tot = __shfl_sync(kFull, incl, 31);
+    if (tot == 0) return;
+    int at = nlist + incl - mine;
+#pragma unroll
+    for (int k = 0; k < kWIpt; k++)
+        if (claim >> k & 1u) sm.list[at++] = w[k];
+    nlist += tot;
+    __syncwarp();
+    if (nlist >= 32)
+        nlist = warp_flush(sm.list, nlist, false, level, vtab, dist, cout, nqv, nqbase, nqoff,
+                           nchunk, found);
+}
+
+// One BFS level, warp-independent form (bfs.kernel = 1).  Top-down: warps
+// take 256-edge chunks round-robin.  Bottom-up (DO and st->mode == 1): warps
+// take 256 vertices; every unvisited one scans its sorted neighbours for one
+// at distance level-1 and stops at the first (Beamer, Asanovic & Patterson,
+// "Direction-Optimizing Breadth-First Search", SC 2012).  Both append their
+// claims to the warp's list; there is no CTA barrier before the level end.
+template <bool DO>
+__global__ void __launch_bounds__(kWBlock, 4)
+k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
+    __shared__ WarpSmem wsm[kWBlock / 32];
+    const unsigned kFull = 0xFFFFFFFFu;
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    WarpSmem& sm = wsm[warp];
+    const int level = st->level;
+    const int it = level - 1;
+    const unsigned long long cin = st->cnt[it % 3];
+    unsigned long long* cout = &st->cnt[(it + 1) % 3];
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->cnt[(it + 2) % 3] = 0;
+    const int nq = (int)(cin & 0xFFFFFFFFull);
+    const unsigned total = (unsigned)(cin >> 32);
+    const int cur = it & 1, nxt = cur ^ 1;
+    int32_t* nqv = st->q[nxt];
+    long long* nqbase = st->qbase[nxt];
+    unsigned* nqoff = st->qoff[nxt];
+    int32_t* nchunk = st->chunk[nxt];
+    const VRec* __restrict__ vtab = st->vtab;
+    const int32_t* __restrict__ pool = st->pool;
+    unsigned* bm = st->bitmap;
+    int32_t* dist = st->dist;
+    const int mode = DO ? st->mode : 0;
+    const unsigned gw = blockIdx.x * (kWBlock / 32) + warp;
+    const unsigned nwarps = gridDim.x * (kWBlock / 32);
+    int found = 0;
+    int nlist = 0;
+
+    if (mode == 0) {
+        const long long* __restrict__ qbase = st->qbase[cur];
+        const unsigned* __restrict__ qoff = st->qoff[cur];
+        const int32_t* __restrict__ chunk = st->chunk[cur];
+        const unsigned nchunks = (total + kWChunk - 1) >> kChunkShiftWarp;
+        for (unsigned c = gw; c < nchunks; c += nwarps) {
+            const unsigned e0 = c << kChunkShiftWarp;
+            const unsigned e1 = e0 + kWChunk < total ? e0 + kWChunk : total;
+            const int s0 = chunk[c];
+            const int s1 = c + 1 < nchunks ? chunk[c + 1] : nq - 1;   // inclusive
+            const int nw = s1 - s0 + 1;
+            int w[kWIpt];
+            if (nw <= 32) {
+                // window in registers: lane j holds entry s0 + j.  The vertex
+                // of edge e is the last entry starting at or before e:
+                // entries started before the row (ballot) plus starts inside
+                // the row up to this lane (OR-reduced bit positions)
+                unsigned sj = 0xFFFFFFFFu;
+                long long bj = 0;
+                if (lane < nw) {
+                    sj = qoff[s0 + lane];
+                    bj = qbase[s0 + lane] - (long long)sj;
+                }
+#pragma unroll
+                for (int k = 0; k < kWIpt; k++) {
+                    const unsigned rs = e0 + 32u * k;
+                    const unsigned rel = sj - rs;   // wraps for entries before the row
+                    const unsigned bits = __reduce_or_sync(kFull, lane < nw && sj >= rs && rel < 32u
+                                                                      ? 1u << rel : 0u);
+                    const int before = __popc(__ballot_sync(kFull, lane < nw && sj < rs));
+                    const int j = before - 1 + __popc(bits & (kFull >> (31 - lane)));
+                    const long long b = __shfl_sync(kFull, bj, j & 31);
+                    const unsigned e = rs + lane;
+                    w[k] = e < e1 ? __ldg(pool + b + e) : -1;
+                }
+            } else {
+                // larger window: staged in the warp's shared memory, one
+                // search per lane over 8 consecutive edges
+                for (int j = lane; j <= nw; j += 32) {
+                    const unsigned so = qoff[s0 + j];   // qoff[nq] is the sealed total
+                    sm.start[j] = so;
+                    if (j < nw) sm.base[j] = qbase[s0 + j] - (long long)so;
+                }
+                __syncwarp();
+                const unsigned a = e0 + lane * kWIpt;
+                int lo = 0, hi = nw;                    // last j with start[j] <= a
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (sm.start[mid] <= a) lo = mid; else hi = mid;
+                }
+                int j = lo;
+#pragma unroll
+                for (int k = 0; k < kWIpt; k++) {
+                    const unsigned e = a + k;
+                    w[k] = -1;
+                    if (e < e1) {
+                        while (sm.start[j + 1] <= e) j++;
+                        w[k] = __ldg(pool + sm.base[j] + e);
+                    }
+                }
+                __syncwarp();
+            }
+            unsigned word[kWIpt];
+#pragma unroll
+            for (int k = 0; k < kWIpt; k++)
+                word[k] = w[k] >= 0 ? __ldca(bm + (w[k] >> 5)) : 0xFFFFFFFFu;
+            unsigned claim = 0;
+#pragma unroll
+            for (int k = 0; k < kWIpt; k++) {
+                if (w[k] >= 0 && !(word[k] & (1u << (w[k] & 31)))) {
+                    const unsigned bit = 1u << (w[k] & 31);
+                    if (!(atomicOr(bm + (w[k] >> 5), bit) & bit)) claim |= 1u << k;
+                }
+            }
+            warp_claims(sm, nlist, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
+                        found);
+        }
+    } else {
+        // bottom-up over all vertices, 256 per warp, lane-strided
+        const int nV = st->nV;
+        const unsigned nvc = ((unsigned)nV + kWChunk - 1) >> kChunkShiftWarp;
+        for (unsigned c = gw; c < nvc; c += nwarps) {
+            int w[kWIpt];
+            int dv[kWIpt];
+#pragma unroll
+            for (int k = 0; k < kWIpt; k++) {
+                const long long v = ((long long)c << kChunkShiftWarp) + 32 * k + lane;
+                w[k] = v < nV ? (int)v : -1;
+                dv[k] = w[k] >= 0 ? __ldcg(dist + v) : 0;
+            }
+            unsigned claim = 0;
+#pragma unroll
+            for (int k = 0; k < kWIpt; k++) {
+                if (w[k] >= 0 && dv[k] == kInf) {
+                    const VRec r = vtab[w[k]];
+                    const int32_t* nb = pool + r.off;
+                    for (int i = 0; i < r.deg; i++) {
+                        if (__ldca(dist + nb[i]) == level - 1) { claim |= 1u << k; break; }
+                    }
+                    if (claim >> k & 1u) atomicOr(bm + (w[k] >> 5), 1u << (w[k] & 31));
+                }
+            }
+            warp_claims(sm, nlist, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
+                        found);
+        }
+    }
+    if (nlist > 0)
+        warp_flush(sm.list, nlist, true, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
+                   found);
+    (void)kFull;
+    bfs_level_end<DO>(st, cond, found, level, nq, total, cout, nqoff);
 }
 
 // One BFS level.  TopDown (always, or while st->mode == 0 when DO): the
@@ -275,7 +593,6 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
     const int32_t* pool = st->pool;
     unsigned* bm = st->bitmap;
     int32_t* dist = st->dist;
-    const int lane = threadIdx.x & 31;
     const int mode = DO ? st->mode : 0;
     int found = 0;
 
@@ -378,7 +695,8 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
                     }
                 }
             }
-            bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk, found);
+            bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
+                        kChunkShiftCta, found);
             // bfs_enqueue ends with a barrier, so every thread has read sm.next
             if (threadIdx.x == 0) sm.next = dyn ? atomicAdd(&st->next_chunk, 1u) : c + gridDim.x;
             __syncthreads();
@@ -410,51 +728,28 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
                     if (claim[k]) atomicOr(bm + (w[k] >> 5), 1u << (w[k] & 31));
                 }
             }
-            bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk, found);
+            bfs_enqueue(sm, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
+                        kChunkShiftCta, found);
         }
     }
-    // visited count: one atomic per warp
-    for (int o = 16; o; o >>= 1) found += __shfl_down_sync(0xFFFFFFFFu, found, o);
-    if (lane == 0 && found) atomicAdd((unsigned long long*)&st->visited, (unsigned long long)found);
-    // the last CTA seals the next frontier, picks the next direction and
-    // decides whether to loop
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        unsigned tk = atomicAdd(&st->ticket, 1u);
-        if (tk == gridDim.x - 1) {
-            __threadfence();
-            unsigned long long cn = atomicAdd(cout, 0ull);
-            unsigned nn = (unsigned)(cn & 0xFFFFFFFFull);
-            unsigned long long mf = cn >> 32;
-            nqoff[nn] = (unsigned)mf;
-            st->ticket = 0;
-            st->next_chunk = 0;
-            st->scanned += total;
-            st->level = level + 1;
-            if (DO) {
-                // Beamer's switch: to bottom-up when the next frontier's edges
-                // exceed 1/alpha of the unexplored edges (alpha = 14 by
-                // default), back to top-down when the frontier falls below
-                // nV/beta vertices (beta = 24) and is shrinking
-                st->edges_visited += (long long)mf;
-                long long mu = st->m_total - st->edges_visited;
-                if (st->mode == 0) {
-                    if ((long long)mf * st->alpha > mu) st->mode = 1;
-                } else {
-                    if ((long long)nn * st->beta < st->nV && nn < (unsigned)nq) st->mode = 0;
-                }
-            }
-            const unsigned more = (nn > 0 && level < st->nV) ? 1u : 0u;
-            st->cont = (int)more;
-            if (!st->host_driven) cudaGraphSetConditional(cond, more);
-        }
-    }
+    bfs_level_end<DO>(st, cond, found, level, nq, total, cout, nqoff);
+}
+
+// The level kernel for bfs.kernel = `kernel` (top-down or direction-optimising).
+void* level_kernel(int kernel, bool dir_opt) {
+    if (kernel)
+        return dir_opt ? (void*)k_bfs_wlevel<true> : (void*)k_bfs_wlevel<false>;
+    return dir_opt ? (void*)k_bfs_level<true> : (void*)k_bfs_level<false>;
+}
+
+const char* level_kernel_name(int kernel, bool dir_opt) {
+    if (kernel) return dir_opt ? "k_bfs_wlevel<true>" : "k_bfs_wlevel<false>";
+    return dir_opt ? "k_bfs_level<true>" : "k_bfs_level<false>";
 }
 
 void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
     const int nV = g->nV;
-    const long long nchunk_cap = g->nE / kChunk + 4;
+    const long long nchunk_cap = g->nE / kWChunk + 4;   // the finer of the two granularities
     HN_CUDA(cudaMalloc((void**)&bg.state, sizeof(BfsState)));
     HN_CUDA(cudaMallocHost((void**)&bg.h_state, sizeof(BfsState)));
     HN_CUDA(cudaMalloc((void**)&bg.qbuf, sizeof(int32_t) * 2 * ((size_t)nV + 1)));
@@ -490,9 +785,9 @@ void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
         {
             void* args[] = {&bg.state, &handle};
             cudaKernelNodeParams p = {};
-            p.func = variant ? (void*)k_bfs_level<true> : (void*)k_bfs_level<false>;
+            p.func = level_kernel(bg.kernel, variant != 0);
             p.gridDim = dim3(bg.grid);
-            p.blockDim = dim3(kBfsBlock);
+            p.blockDim = dim3(bg.kernel ? kWBlock : kBfsBlock);
             p.kernelParams = args;
             HN_CUDA(cudaGraphAddKernelNode(&body_node, body, nullptr, 0, &p));
         }
@@ -529,10 +824,12 @@ namespace {
 
 BfsGraph& bfs_graph_of(hn_graph* g) {
     // rebuilt when the vertex count changes, the edge count outgrows the
-    // chunk table or the bfs.ctas_per_sm knob changes the level grid
-    const unsigned grid = (unsigned)(g->info.sms * knob(kKnobBfsCtasPerSm));
-    if (g->bfs && (g->bfs->nV != g->nV || g->nE / kChunk + 4 > g->bfs->nchunk_cap ||
-                   g->bfs->grid != grid)) {
+    // chunk table or a knob changes the level kernel or its grid
+    const int kernel = (int)knob(kKnobBfsKernel);
+    const unsigned grid = (unsigned)(g->info.sms *
+                                     knob(kernel ? kKnobBfsWarpCtasPerSm : kKnobBfsCtasPerSm));
+    if (g->bfs && (g->bfs->nV != g->nV || g->nE / kWChunk + 4 > g->bfs->nchunk_cap ||
+                   g->bfs->grid != grid || g->bfs->kernel != kernel)) {
         HN_CUDA(cudaStreamSynchronize(g->stream));
         free_bfs_graph(g->bfs);
         g->bfs = nullptr;
@@ -540,6 +837,7 @@ BfsGraph& bfs_graph_of(hn_graph* g) {
     if (!g->bfs) {
         g->bfs = new BfsGraph();
         g->bfs->grid = grid;
+        g->bfs->kernel = kernel;
         try {
             build_bfs_graph(g, *g->bfs);
         } catch (...) {
@@ -558,7 +856,8 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
     for (int i = 0; i < k; i++)
         if (sources[i] < 0 || sources[i] >= nV)
             throw Error(HN_ERR_INVALID, "BFS source outside [0, nV)");
-    if (g->nE >= 0xFFFFFFFFll) throw Error(HN_ERR_CAPACITY, "BFS needs nE < 2^32");
+    // edge offsets are 32-bit, and a chunk's end (offset + 256) must not wrap
+    if (g->nE > 0xFFFFFE00ll) throw Error(HN_ERR_CAPACITY, "BFS needs nE < 2^32 - 512");
     BfsGraph& bg = bfs_graph_of(g);
     if (!bg.h_ring) {
         HN_CUDA(cudaMallocHost((void**)&bg.h_ring, sizeof(BfsState) * BfsGraph::kRing));
@@ -609,6 +908,7 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
         h.warp_strided = (int)knob(kKnobBfsWarpStrided);
         h.host_driven = host_driven ? 1 : 0;
         h.next_chunk = 0;
+        h.cshift = bg.kernel ? kChunkShiftWarp : kChunkShiftCta;
         HN_CUDA(cudaMemcpyAsync(bg.state, &h, sizeof(BfsState), cudaMemcpyHostToDevice, s));
         // profiling records the whole graph (one init + one expand per
         // level) under the name of its dominant kernel
@@ -621,11 +921,11 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
             HN_CUDA(cudaGetLastError());
             count_launch();
             for (int lv = 0; lv <= nV; lv++) {
-                if (direction_optimizing)
-                    k_bfs_level<true><<<bg.grid, kBfsBlock, 0, s>>>(bg.state, 0);
-                else
-                    k_bfs_level<false><<<bg.grid, kBfsBlock, 0, s>>>(bg.state, 0);
-                HN_CUDA(cudaGetLastError());
+                cudaGraphConditionalHandle none = 0;
+                void* args[] = {&bg.state, &none};
+                HN_CUDA(cudaLaunchKernel(level_kernel(bg.kernel, direction_optimizing),
+                                         dim3(bg.grid), dim3(bg.kernel ? kWBlock : kBfsBlock),
+                                         args, 0, s));
                 count_launch();
                 HN_CUDA(cudaMemcpyAsync(&bg.h_state->cont, &bg.state->cont, sizeof(int),
                                         cudaMemcpyDeviceToHost, s));
@@ -636,8 +936,7 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
             HN_CUDA(cudaGraphLaunch(bg.exec[direction_optimizing ? 1 : 0], s));
             count_launch(2);
         }
-        if (ev0)
-            profile_end(direction_optimizing ? "k_bfs_level<true>" : "k_bfs_level<false>", s, ev0);
+        if (ev0) profile_end(level_kernel_name(bg.kernel, direction_optimizing), s, ev0);
         // the finished state back into this source's ring slot (ordered
         // before the next source's state upload on the same stream)
         HN_CUDA(cudaMemcpyAsync(&h, bg.state, sizeof(BfsState), cudaMemcpyDeviceToHost, s));

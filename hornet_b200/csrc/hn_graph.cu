@@ -60,9 +60,17 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"tc.flip", 1, 0, 1, false},
     {"tc.thread_du", 16, 0, 64, false},
     {"tc.thread_dc", 32, 1, 1024, false},
+    {"bfs.kernel", 1, 0, 1, false},
+    {"bfs.warp_ctas_per_sm", 4, 1, 8, false},
 };
-std::atomic<long long> g_knob[kNumKnobs] = {
-    {9}, {14}, {24}, {256}, {4}, {512}, {16}, {8}, {0}, {0}, {0}, {0}, {1}, {4096}, {16384}, {1 << 18}, {1 << 16}, {1}, {16}, {32}};
+std::atomic<long long> g_knob[kNumKnobs];
+// every knob starts at its default (static initialisation, in definition
+// order after kKnobs)
+struct KnobDefaults {
+    KnobDefaults() {
+        for (int i = 0; i < kNumKnobs; i++) g_knob[i].store(kKnobs[i].def, std::memory_order_relaxed);
+    }
+} g_knob_defaults;
 
 int knob_index(const char* name) {
     if (!name) return -1;

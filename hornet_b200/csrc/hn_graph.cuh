@@ -135,6 +135,8 @@ enum Knob {
     kKnobTcFlip,
     kKnobTcThreadDu,
     kKnobTcThreadDc,
+    kKnobBfsKernel,
+    kKnobBfsWarpCtasPerSm,
     kNumKnobs
 };
 long long knob(Knob k);

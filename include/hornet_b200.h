@@ -132,6 +132,12 @@ int hn_profile_report(char* buf, int64_t len);
  *   bfs.host_levels     1: launch the BFS levels one by one from the host
  *                       (for per-level profiling) instead of the CUDA
  *                       graph's device-side loop (0..1, 0)
+ *   bfs.kernel          BFS level kernel: 1 = independent warps on 256-edge
+ *                       chunks, 0 = 128-thread CTAs on 1024-edge chunks
+ *                       (bfs.ctas_per_sm, bfs.dynamic_chunks and
+ *                       bfs.warp_strided apply to it) (0..1, 1)
+ *   bfs.warp_ctas_per_sm  CTAs per SM of the warp-chunk level kernel, 256
+ *                       threads each (1..8, 4)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);

@@ -73,3 +73,17 @@ def test_search_spaces_and_saved_knobs_are_registered():
             for knob, v in rec["knobs"].items():
                 H.tune_set(knob, v)
                 assert H.tune_get(knob) == v
+
+
+def test_knobs_start_at_their_defaults():
+    """In a fresh process every knob already holds its default before any
+    hn_tune_reset (the values are not a second hand-kept list)."""
+    import subprocess
+    import sys
+    code = ("import hornet_b200 as H\n"
+            "before = {n: H.tune_get(n) for n in H.tune_names()}\n"
+            "H.tune_reset()\n"
+            "after = {n: H.tune_get(n) for n in H.tune_names()}\n"
+            "assert before == after, (before, after)\n")
+    root = __import__("os").path.dirname(__import__("os").path.dirname(__file__))
+    subprocess.run([sys.executable, "-c", code], check=True, cwd=root)

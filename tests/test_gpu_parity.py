@@ -204,6 +204,63 @@ def test_bfs_direction_optimizing(name):
         assert do_stats[i].levels == td_stats[i].levels
 
 
+def _shape_graph(kind):
+    """Graphs that reach every branch of the level kernels: a star whose hub
+    spans many 256- and 1024-edge chunks, a long path (one vertex per
+    level), many vertices of degree 1-2 (windows of more than 32 vertices
+    per chunk) and hubs joined by paths."""
+    rng = np.random.default_rng(17)
+    if kind == "star":
+        n = 20001
+        s = np.zeros(n - 1, np.int32)
+        d = np.arange(1, n, dtype=np.int32)
+    elif kind == "path":
+        n = 3000
+        s = np.arange(n - 1, dtype=np.int32)
+        d = s + 1
+    elif kind == "sparse":
+        n = 50000
+        s = rng.integers(0, n, n // 2).astype(np.int32)
+        d = rng.integers(0, n, n // 2).astype(np.int32)
+        s = np.concatenate([s, np.arange(n - 1, dtype=np.int32)])
+        d = np.concatenate([d, np.arange(1, n, dtype=np.int32)])
+    else:   # "hubs": four stars of 6000 leaves whose hubs are joined by a path
+        n = 4 * 6001 + 100
+        ss, dd = [], []
+        for h in range(4):
+            hub = h * 6001
+            ss.append(np.full(6000, hub, np.int32))
+            dd.append(np.arange(hub + 1, hub + 6001, dtype=np.int32))
+        chain = np.array([0, 24004, 6001, 24010, 12002, 24020, 18003], np.int32)
+        ss.append(chain[:-1])
+        dd.append(chain[1:])
+        s, d = np.concatenate(ss), np.concatenate(dd)
+    return O.build_csr_undirected(n, s, d)
+
+
+@pytest.mark.parametrize("kernel", [1, 0])
+@pytest.mark.parametrize("kind", ["star", "path", "sparse", "hubs"])
+def test_bfs_graph_shapes_both_kernels(kind, kernel):
+    """Both level kernels (warp chunks and CTA chunks), top-down and
+    direction-optimising, equal the oracle on graphs that stress the chunk
+    table: hubs spanning many chunks, one vertex per level, and windows of
+    many low-degree vertices."""
+    g = _shape_graph(kind)
+    h = build(g)
+    srcs = [0, g.nV - 1, g.nV // 2]
+    try:
+        H.tune_set("bfs.kernel", kernel)
+        td, st = H.BfsTopDown(h).run_multi(srcs)
+        do, _ = H.BfsTopDown(h).run_multi(srcs, direction_optimizing=True)
+    finally:
+        H.tune_reset()
+    for i, s in enumerate(srcs):
+        ref, scanned = O.bfs(g, s)
+        np.testing.assert_array_equal(td[i], ref)
+        np.testing.assert_array_equal(do[i], ref)
+        assert st[i].edges_scanned == scanned
+
+
 def test_bfs_isolated_source():
     s = np.array([1, 2], np.int32)
     d = np.array([2, 3], np.int32)
@@ -362,12 +419,15 @@ def test_tc_local(name):
     {"tc.thread_du": 0},
     {"tc.thread_du": 4, "tc.thread_dc": 3},
     {"tc.warp_work": 1024, "tc.item_work": 1500, "tc.mid_cap": 36, "tc.warp_cap": 32},
-    {"bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
-    {"bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
-    {"bfs.warp_strided": 1},
-    {"bfs.host_levels": 1, "bfs.warp_strided": 1},
-    {"bfs.warp_strided": 1, "bfs.dynamic_chunks": 1, "bfs.ctas_per_sm": 8},
-    {"bfs.ctas_per_sm": 8, "bfs.do_alpha": 1 << 20, "bfs.do_beta": 1 << 20},
+    {"bfs.kernel": 0, "bfs.ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
+    {"bfs.kernel": 0, "bfs.ctas_per_sm": 3, "bfs.dynamic_chunks": 1},
+    {"bfs.kernel": 0, "bfs.warp_strided": 1},
+    {"bfs.kernel": 0, "bfs.host_levels": 1, "bfs.warp_strided": 1},
+    {"bfs.kernel": 0, "bfs.warp_strided": 1, "bfs.dynamic_chunks": 1, "bfs.ctas_per_sm": 8},
+    {"bfs.kernel": 0, "bfs.ctas_per_sm": 8, "bfs.do_alpha": 1 << 20, "bfs.do_beta": 1 << 20},
+    {"bfs.warp_ctas_per_sm": 1, "bfs.do_alpha": 1, "bfs.do_beta": 1},
+    {"bfs.warp_ctas_per_sm": 8, "bfs.host_levels": 1},
+    {"bfs.warp_ctas_per_sm": 2, "bfs.do_alpha": 1 << 20, "bfs.do_beta": 1 << 20},
 ])
 def test_tuning_knobs_keep_results(knobs):
     """The knob extremes the autotuner can set change only the speed: TC
