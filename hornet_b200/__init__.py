@@ -102,6 +102,7 @@ _SIGNATURES = {
     "hn_bfs": [_P, _I32, _P, _INT, _P],
     "hn_bfs_multi": [_P, _P, _I32, _P, _INT, _P],
     "hn_bfs_do": [_P, _P, _I32, _P, _INT, _P],
+    "hn_bfs_level_trace": [_P, _I32, _P, _P, _P],
     "hn_bfs_batch": [_P, _P, _P, _I32, _I32, _P, _INT, _P],
     "hn_tc": [_P, _P, _INT, _P],
     "hn_tc_local": [_P, _P, _I32, _P, _INT],
@@ -528,6 +529,16 @@ class BfsTopDown(StaticAlgorithm):
         _check(fn(self.hornet.handle, srcs.ctypes.data_as(_P), len(srcs), p, mem, stats))
         return out, [stats[i] for i in range(len(srcs))]
 
+
+    def level_trace(self, max_levels: int = 32):
+        """Per-level device time (us) and frontier edges of the latest BFS
+        source run on this graph (instrumentation, hn_bfs_level_trace)."""
+        us = np.zeros(max_levels, np.float64)
+        ed = np.zeros(max_levels, np.int64)
+        n = ctypes.c_int32(0)
+        _check(lib().hn_bfs_level_trace(self.hornet.handle, max_levels, us.ctypes.data_as(_P),
+                                        ed.ctypes.data_as(_P), ctypes.byref(n)))
+        return us[: n.value], ed[: n.value]
 
     def run_batch(self, sources, slots=None, nslots=None, out=None):
         """Batched BFS (hn_bfs_batch): up to 64 slots in one traversal.

@@ -63,6 +63,14 @@ constexpr int kChunkShiftWarp = 8;               // log2(kWChunk)
 constexpr int kWList = kWChunk + 32;             // claim list capacity per warp
 static_assert(kChunk == 1 << kChunkShiftCta && kWChunk == 1 << kChunkShiftWarp, "chunk sizes");
 
+constexpr int kTraceLevels = 32;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 struct BfsState {
     unsigned long long cnt[3];   // frontier counters: (edge total << 32) | size
     int level;                   // distance given to vertices found now
@@ -91,6 +99,11 @@ struct BfsState {
     int cont;                    // 1 while another level follows (host-driven loop)
     int host_driven;             // 1: no conditional node (levels launched by the host)
     int cshift;                  // log2 of the chunk size of chunk[]
+    // level trace: global timer (ns) at the start and at the end of each of
+    // the first kTraceLevels levels, and the frontier edges each one scanned
+    unsigned long long t_start;
+    unsigned long long t_end[kTraceLevels];
+    unsigned long long lvl_edges[kTraceLevels];
 };
 
 struct BfsGraph {
@@ -107,6 +120,7 @@ struct BfsGraph {
     cudaGraphExec_t exec[2] = {nullptr, nullptr};
     unsigned grid = 0;                              // level-kernel CTAs baked in
     int kernel = -1;                                // bfs.kernel baked in
+    int per_sm = 0;                                 // CTAs per SM baked in
     // multi-source calls: pinned per-source states (the next source's state
     // is staged while the previous BFS runs), a copy stream and events so a
     // host-bound distance array is copied out while the next BFS runs
@@ -115,6 +129,8 @@ struct BfsGraph {
     cudaStream_t copy = nullptr;
     cudaEvent_t done[2] = {nullptr, nullptr};       // BFS into buffer b finished
     cudaEvent_t copied[2] = {nullptr, nullptr};     // buffer b copied to the host
+    BfsState last = {};                             // final state of the latest BFS
+    bool have_last = false;
 };
 
 namespace {
@@ -162,6 +178,7 @@ __global__ void k_bfs3_init(BfsState* st) {
         st->scanned = 0;
         st->mode = 0;
         st->edges_visited = d;
+        st->t_start = global_ns();
     }
 }
 
@@ -289,6 +306,10 @@ __device__ __forceinline__ void bfs_level_end(BfsState* st, cudaGraphConditional
             st->ticket = 0;
             st->next_chunk = 0;
             st->scanned += total;
+            if (level <= kTraceLevels) {
+                st->t_end[level - 1] = global_ns();
+                st->lvl_edges[level - 1] = total;
+            }
             st->level = level + 1;
             if (DO) {
                 // Beamer's switch: to bottom-up when the next frontier's edges
@@ -312,92 +333,134 @@ __device__ __forceinline__ void bfs_level_end(BfsState* st, cudaGraphConditional
 
 // Warp-private shared memory of k_bfs_wlevel.
 struct WarpSmem {
-    long long base[kWChunk + 1];   // window: pool index = base + edge (large windows)
-    unsigned start[kWChunk + 2];   // window edge offsets (+ end)
+    long long base[kWList];        // window: pool index = base + edge (large windows);
+                                   // flush: adjacency base of each listed vertex
+    unsigned start[kWList];        // window edge offsets (+ end); flush: degrees
     int list[kWList];              // claimed vertices not yet enqueued
 };
 
-// Enqueue the warp's claimed vertices 32 at a time (all of them when `all`,
-// else only whole groups of 32; the rest moves to the front of the list and
-// the new list length is returned).  Per group: the vertex records are read,
-// distances written, then one 64-bit atomicAdd reserves the group's queue
-// slots and edge range.  A vertex that spans many chunks has its chunk marks
+// Where a level's claims go (per CTA, in shared memory: the enqueue is rare
+// next to the edge loop, so these do not hold registers there).
+struct LevelOut {
+    const VRec* vtab;
+    int32_t* dist;
+    unsigned long long* cout;
+    int32_t* nqv;
+    long long* nqbase;
+    unsigned* nqoff;
+    int32_t* nchunk;
+    int level;
+};
+
+// Enqueue all n vertices of the warp's claim list in one pass: every lane
+// reads the records of up to ceil(n / 32) listed vertices (loads issued
+// together) into the warp's shared memory and writes their distances, then
+// one warp scan and ONE 64-bit atomicAdd reserve the queue slots and the
+// edge range of all of them, and each lane writes its consecutive share of
+// queue entries.  A vertex that spans many chunks has its chunk marks
 // written by the whole warp.  Called by all 32 lanes with the same n.
-__device__ __forceinline__ int warp_flush(int* __restrict__ list, int n, bool all, int level,
-                                          const VRec* __restrict__ vtab, int32_t* dist,
-                                          unsigned long long* cout, int32_t* nqv,
-                                          long long* nqbase, unsigned* nqoff, int32_t* nchunk,
-                                          int& found) {
+__device__ __forceinline__ void warp_flush(WarpSmem& sm, int n, const LevelOut& lo, int& found) {
     const int lane = threadIdx.x & 31;
+    const VRec* __restrict__ vtab = lo.vtab;
+    int32_t* dist = lo.dist;
+    const int level = lo.level;
     const unsigned kFull = 0xFFFFFFFFu;
-    int done = 0;
-    while (all ? done < n : n - done >= 32) {
-        const int i = done + lane;
-        const bool have = i < n;
-        const int v = have ? list[i] : 0;
-        VRec r = {0, 0, 0};
-        if (have) {
-            r = vtab[v];
-            dist[v] = level;
-            found++;
-        }
-        const unsigned d = (unsigned)r.deg;
-        const unsigned long long mine = d ? (((unsigned long long)d << 32) | 1ull) : 0ull;
-        unsigned long long incl = mine;
+    // records of the listed vertices, four loads in flight per lane
+    for (int i0 = 0; i0 < n; i0 += 128) {
+        VRec r[4];
+        int v[4];
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            unsigned long long x = __shfl_up_sync(kFull, incl, o);
-            if (lane >= o) incl += x;
+        for (int u = 0; u < 4; u++) {
+            const int i = i0 + u * 32 + lane;
+            v[u] = i < n ? sm.list[i] : -1;
+            if (v[u] >= 0) r[u] = vtab[v[u]];
         }
-        unsigned long long base = 0;
-        if (lane == 31 && incl) base = atomicAdd(cout, incl);
-        base = __shfl_sync(kFull, base, 31);
-        const unsigned long long at = base + incl - mine;
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = i0 + u * 32 + lane;
+            if (v[u] >= 0) {
+                dist[v[u]] = level;
+                found++;
+                sm.base[i] = r[u].off;
+                sm.start[i] = (unsigned)r[u].deg;
+            }
+        }
+    }
+    __syncwarp();
+    // lane L owns list entries [L * per, L * per + per)
+    const int per = (n + 31) >> 5;
+    const int i0 = lane * per;
+    const int i1 = i0 + per < n ? i0 + per : n;
+    unsigned long long mine = 0;   // (degree sum << 32) | vertices with edges
+    for (int i = i0; i < i1; i++) {
+        const unsigned d = sm.start[i];
+        if (d) mine += ((unsigned long long)d << 32) | 1ull;
+    }
+    unsigned long long incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned long long x = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += x;
+    }
+    unsigned long long base = 0;
+    if (lane == 31 && incl) base = atomicAdd(lo.cout, incl);
+    base = __shfl_sync(kFull, base, 31);
+    unsigned long long at = base + incl - mine;
+    bool has_big = false;
+    int32_t* nqv = lo.nqv;
+    long long* nqbase = lo.nqbase;
+    unsigned* nqoff = lo.nqoff;
+    int32_t* nchunk = lo.nchunk;
+    for (int i = i0; i < i1; i++) {
+        const unsigned d = sm.start[i];
+        if (!d) continue;
         const int pos = (int)(at & 0xFFFFFFFFull);
         const unsigned off = (unsigned)(at >> 32);
-        unsigned c0 = 0, c1 = 0;
-        bool big = false;
-        if (d) {
-            nqv[pos] = v;
-            nqbase[pos] = r.off;
-            nqoff[pos] = off;
-            c0 = (off + kWChunk - 1) >> kChunkShiftWarp;
-            c1 = (off + d - 1) >> kChunkShiftWarp;
-            big = c1 >= c0 + 8;
-            if (!big)
-                for (unsigned c = c0; c <= c1; c++) nchunk[c] = pos;
+        nqv[pos] = sm.list[i];
+        nqbase[pos] = sm.base[i];
+        nqoff[pos] = off;
+        const unsigned c0 = (off + kWChunk - 1) >> kChunkShiftWarp;
+        const unsigned c1 = (off + d - 1) >> kChunkShiftWarp;
+        if (c1 < c0 + 8) {
+            for (unsigned c = c0; c <= c1; c++) nchunk[c] = pos;
+        } else {
+            // marked below by the whole warp: keep its (slot, offset)
+            sm.base[i] = (long long)at;
+            sm.start[i] = d | 0x80000000u;
+            has_big = true;
         }
-        unsigned bigm = __ballot_sync(kFull, big);
-        while (bigm) {
-            const int src = __ffs(bigm) - 1;
-            bigm &= bigm - 1;
-            const unsigned b0 = __shfl_sync(kFull, c0, src);
-            const unsigned b1 = __shfl_sync(kFull, c1, src);
-            const int bp = __shfl_sync(kFull, pos, src);
-            for (unsigned c = b0 + lane; c <= b1; c += 32) nchunk[c] = bp;
-        }
-        done += 32;
+        at += ((unsigned long long)d << 32) | 1ull;
     }
-    if (all || done == 0) return all ? 0 : n;
-    const int rem = n - done;
+    // vertices spanning many chunks: their chunk marks written by the warp
+    unsigned bigm = __ballot_sync(kFull, has_big);
     __syncwarp();
-    const int x = lane < rem ? list[done + lane] : 0;
+    while (bigm) {
+        const int src = __ffs(bigm) - 1;
+        bigm &= bigm - 1;
+        const int j0 = src * per;
+        const int j1 = j0 + per < n ? j0 + per : n;
+        for (int i = j0; i < j1; i++) {
+            const unsigned f = sm.start[i];
+            if (!(f & 0x80000000u)) continue;
+            const unsigned d = f & 0x7FFFFFFFu;
+            const unsigned long long a2 = (unsigned long long)sm.base[i];
+            const int pos = (int)(a2 & 0xFFFFFFFFull);
+            const unsigned off = (unsigned)(a2 >> 32);
+            const unsigned c0 = (off + kWChunk - 1) >> kChunkShiftWarp;
+            const unsigned c1 = (off + d - 1) >> kChunkShiftWarp;
+            for (unsigned c = c0 + lane; c <= c1; c += 32) nchunk[c] = pos;
+        }
+    }
     __syncwarp();
-    if (lane < rem) list[lane] = x;
-    __syncwarp();
-    return rem;
 }
 
 // Append the lanes' claimed vertices (bit k of `claim` set: w[k] claimed) to
 // the warp list and flush whole groups of 32.
 __device__ __forceinline__ void warp_claims(WarpSmem& sm, int& nlist, const int (&w)[kWIpt],
-                                            unsigned claim, int level,
-                                            const VRec* __restrict__ vtab, int32_t* dist,
-                                            unsigned long long* cout, int32_t* nqv,
-                                            long long* nqbase, unsigned* nqoff, int32_t* nchunk,
-                                            int& found) {
+                                            unsigned claim, const LevelOut& lo, int& found) {
     const int lane = threadIdx.x & 31;
     const unsigned kFull = 0xFFFFFFFFu;
+    if (!__any_sync(kFull, claim != 0u)) return;
     const int mine = __popc(claim);
     int incl = mine;
 #pragma unroll
@@ -413,9 +476,10 @@ __device__ __forceinline__ void warp_claims(WarpSmem& sm, int& nlist, const int 
         if (claim >> k & 1u) sm.list[at++] = w[k];
     nlist += tot;
     __syncwarp();
-    if (nlist >= 32)
-        nlist = warp_flush(sm.list, nlist, false, level, vtab, dist, cout, nqv, nqbase, nqoff,
-                           nchunk, found);
+    if (nlist >= 32) {
+        warp_flush(sm, nlist, lo, found);
+        nlist = 0;
+    }
 }
 
 // One BFS level, warp-independent form (bfs.kernel = 1).  Top-down: warps
@@ -424,10 +488,11 @@ __device__ __forceinline__ void warp_claims(WarpSmem& sm, int& nlist, const int 
 // at distance level-1 and stops at the first (Beamer, Asanovic & Patterson,
 // "Direction-Optimizing Breadth-First Search", SC 2012).  Both append their
 // claims to the warp's list; there is no CTA barrier before the level end.
-template <bool DO>
-__global__ void __launch_bounds__(kWBlock, 4)
+template <bool DO, int MINB>
+__global__ void __launch_bounds__(kWBlock, MINB)
 k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
     __shared__ WarpSmem wsm[kWBlock / 32];
+    __shared__ LevelOut lo;
     const unsigned kFull = 0xFFFFFFFFu;
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -436,18 +501,23 @@ k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
     const int it = level - 1;
     const unsigned long long cin = st->cnt[it % 3];
     unsigned long long* cout = &st->cnt[(it + 1) % 3];
-    if (blockIdx.x == 0 && threadIdx.x == 0) st->cnt[(it + 2) % 3] = 0;
     const int nq = (int)(cin & 0xFFFFFFFFull);
     const unsigned total = (unsigned)(cin >> 32);
     const int cur = it & 1, nxt = cur ^ 1;
-    int32_t* nqv = st->q[nxt];
-    long long* nqbase = st->qbase[nxt];
-    unsigned* nqoff = st->qoff[nxt];
-    int32_t* nchunk = st->chunk[nxt];
-    const VRec* __restrict__ vtab = st->vtab;
+    if (threadIdx.x == 0) {
+        if (blockIdx.x == 0) st->cnt[(it + 2) % 3] = 0;
+        lo.vtab = st->vtab;
+        lo.dist = st->dist;
+        lo.cout = cout;
+        lo.nqv = st->q[nxt];
+        lo.nqbase = st->qbase[nxt];
+        lo.nqoff = st->qoff[nxt];
+        lo.nchunk = st->chunk[nxt];
+        lo.level = level;
+    }
+    __syncthreads();
     const int32_t* __restrict__ pool = st->pool;
     unsigned* bm = st->bitmap;
-    int32_t* dist = st->dist;
     const int mode = DO ? st->mode : 0;
     const unsigned gw = blockIdx.x * (kWBlock / 32) + warp;
     const unsigned nwarps = gridDim.x * (kWBlock / 32);
@@ -459,24 +529,45 @@ k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
         const unsigned* __restrict__ qoff = st->qoff[cur];
         const int32_t* __restrict__ chunk = st->chunk[cur];
         const unsigned nchunks = (total + kWChunk - 1) >> kChunkShiftWarp;
-        for (unsigned c = gw; c < nchunks; c += nwarps) {
-            const unsigned e0 = c << kChunkShiftWarp;
-            const unsigned e1 = e0 + kWChunk < total ? e0 + kWChunk : total;
-            const int s0 = chunk[c];
-            const int s1 = c + 1 < nchunks ? chunk[c + 1] : nq - 1;   // inclusive
-            const int nw = s1 - s0 + 1;
-            int w[kWIpt];
-            if (nw <= 32) {
-                // window in registers: lane j holds entry s0 + j.  The vertex
-                // of edge e is the last entry starting at or before e:
-                // entries started before the row (ballot) plus starts inside
-                // the row up to this lane (OR-reduced bit positions)
-                unsigned sj = 0xFFFFFFFFu;
-                long long bj = 0;
-                if (lane < nw) {
+        // A chunk's window: its first queue entry s0 and its size nw; with
+        // at most 32 entries, lane j holds entry s0 + j (start sj, base bj).
+        int s0 = 0, nw = 0;
+        unsigned sj = 0xFFFFFFFFu;
+        long long bj = 0;
+        auto load_window = [&](unsigned cc) {
+            s0 = 0;
+            nw = 0;
+            sj = 0xFFFFFFFFu;
+            bj = 0;
+            if (cc < nchunks) {
+                s0 = chunk[cc];
+                nw = (cc + 1 < nchunks ? chunk[cc + 1] : nq - 1) - s0 + 1;
+                if (nw <= 32 && lane < nw) {
                     sj = qoff[s0 + lane];
                     bj = qbase[s0 + lane] - (long long)sj;
                 }
+            }
+        };
+        // the neighbours of chunk cc (window loaded) into v[], lane-strided
+        // (-1 past the frontier's end)
+        auto load_adj = [&](unsigned cc, int (&v)[kWIpt]) {
+#pragma unroll
+            for (int k = 0; k < kWIpt; k++) v[k] = -1;
+            if (cc >= nchunks) return;
+            const unsigned e0 = cc << kChunkShiftWarp;
+            const unsigned e1 = e0 + kWChunk < total ? e0 + kWChunk : total;
+            if (nw == 1) {
+                // one vertex covers the chunk (hubs): no owner search
+                const long long b = __shfl_sync(kFull, bj, 0);
+#pragma unroll
+                for (int k = 0; k < kWIpt; k++) {
+                    const unsigned e = e0 + 32u * k + lane;
+                    if (e < e1) v[k] = __ldg(pool + b + e);
+                }
+            } else if (nw <= 32) {
+                // the vertex of edge e is the last entry starting at or
+                // before e: entries started before the row (ballot) plus
+                // starts inside the row up to this lane (OR-reduced bits)
 #pragma unroll
                 for (int k = 0; k < kWIpt; k++) {
                     const unsigned rs = e0 + 32u * k;
@@ -487,7 +578,7 @@ k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
                     const int j = before - 1 + __popc(bits & (kFull >> (31 - lane)));
                     const long long b = __shfl_sync(kFull, bj, j & 31);
                     const unsigned e = rs + lane;
-                    w[k] = e < e1 ? __ldg(pool + b + e) : -1;
+                    if (e < e1) v[k] = __ldg(pool + b + e);
                 }
             } else {
                 // larger window: staged in the warp's shared memory, one
@@ -499,22 +590,44 @@ k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
                 }
                 __syncwarp();
                 const unsigned a = e0 + lane * kWIpt;
-                int lo = 0, hi = nw;                    // last j with start[j] <= a
-                while (hi - lo > 1) {
-                    const int mid = (lo + hi) >> 1;
-                    if (sm.start[mid] <= a) lo = mid; else hi = mid;
+                int lo2 = 0, hi = nw;                   // last j with start[j] <= a
+                while (hi - lo2 > 1) {
+                    const int mid = (lo2 + hi) >> 1;
+                    if (sm.start[mid] <= a) lo2 = mid; else hi = mid;
                 }
-                int j = lo;
+                int j = lo2;
 #pragma unroll
                 for (int k = 0; k < kWIpt; k++) {
                     const unsigned e = a + k;
-                    w[k] = -1;
                     if (e < e1) {
                         while (sm.start[j + 1] <= e) j++;
-                        w[k] = __ldg(pool + sm.base[j] + e);
+                        v[k] = __ldg(pool + sm.base[j] + e);
                     }
                 }
                 __syncwarp();
+            }
+        };
+        // The next chunk's window is read while this chunk's neighbour loads
+        // are in flight, so a chunk waits on three round trips (neighbours,
+        // bitmap, claims), not five.
+        load_window(gw);
+        for (unsigned c = gw; c < nchunks; c += nwarps) {
+            const unsigned cn = c + nwarps;
+            int ns0 = 0, ns1 = -1;
+            if (cn < nchunks) {
+                ns0 = chunk[cn];
+                ns1 = cn + 1 < nchunks ? chunk[cn + 1] : nq - 1;   // inclusive
+            }
+            int w[kWIpt];
+            load_adj(c, w);
+            // the next chunk's register window
+            s0 = ns0;
+            nw = ns1 - ns0 + 1;
+            sj = 0xFFFFFFFFu;
+            bj = 0;
+            if (nw <= 32 && lane < nw) {
+                sj = qoff[s0 + lane];
+                bj = qbase[s0 + lane] - (long long)sj;
             }
             unsigned word[kWIpt];
 #pragma unroll
@@ -528,11 +641,12 @@ k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
                     if (!(atomicOr(bm + (w[k] >> 5), bit) & bit)) claim |= 1u << k;
                 }
             }
-            warp_claims(sm, nlist, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
-                        found);
+            warp_claims(sm, nlist, w, claim, lo, found);
         }
     } else {
         // bottom-up over all vertices, 256 per warp, lane-strided
+        const VRec* __restrict__ vtab = st->vtab;
+        const int32_t* dist = st->dist;
         const int nV = st->nV;
         const unsigned nvc = ((unsigned)nV + kWChunk - 1) >> kChunkShiftWarp;
         for (unsigned c = gw; c < nvc; c += nwarps) {
@@ -556,15 +670,12 @@ k_bfs_wlevel(BfsState* st, cudaGraphConditionalHandle cond) {
                     if (claim >> k & 1u) atomicOr(bm + (w[k] >> 5), 1u << (w[k] & 31));
                 }
             }
-            warp_claims(sm, nlist, w, claim, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
-                        found);
+            warp_claims(sm, nlist, w, claim, lo, found);
         }
     }
-    if (nlist > 0)
-        warp_flush(sm.list, nlist, true, level, vtab, dist, cout, nqv, nqbase, nqoff, nchunk,
-                   found);
+    if (nlist > 0) warp_flush(sm, nlist, lo, found);
     (void)kFull;
-    bfs_level_end<DO>(st, cond, found, level, nq, total, cout, nqoff);
+    bfs_level_end<DO>(st, cond, found, level, nq, total, cout, st->qoff[nxt]);
 }
 
 // One BFS level.  TopDown (always, or while st->mode == 0 when DO): the
@@ -735,10 +846,18 @@ k_bfs_level(BfsState* st, cudaGraphConditionalHandle cond) {
     bfs_level_end<DO>(st, cond, found, level, nq, total, cout, nqoff);
 }
 
-// The level kernel for bfs.kernel = `kernel` (top-down or direction-optimising).
-void* level_kernel(int kernel, bool dir_opt) {
-    if (kernel)
-        return dir_opt ? (void*)k_bfs_wlevel<true> : (void*)k_bfs_wlevel<false>;
+// The level kernel for bfs.kernel = `kernel` (top-down or direction-
+// optimising).  The warp kernel is compiled for 3, 4 and 5 resident CTAs per
+// SM (80, 64 and 48 registers); `per_sm` (bfs.warp_ctas_per_sm) picks the
+// build that lets that many CTAs reside.
+void* level_kernel(int kernel, bool dir_opt, int per_sm) {
+    if (kernel) {
+        if (per_sm >= 5)
+            return dir_opt ? (void*)k_bfs_wlevel<true, 5> : (void*)k_bfs_wlevel<false, 5>;
+        if (per_sm == 4)
+            return dir_opt ? (void*)k_bfs_wlevel<true, 4> : (void*)k_bfs_wlevel<false, 4>;
+        return dir_opt ? (void*)k_bfs_wlevel<true, 3> : (void*)k_bfs_wlevel<false, 3>;
+    }
     return dir_opt ? (void*)k_bfs_level<true> : (void*)k_bfs_level<false>;
 }
 
@@ -785,7 +904,7 @@ void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
         {
             void* args[] = {&bg.state, &handle};
             cudaKernelNodeParams p = {};
-            p.func = level_kernel(bg.kernel, variant != 0);
+            p.func = level_kernel(bg.kernel, variant != 0, bg.per_sm);
             p.gridDim = dim3(bg.grid);
             p.blockDim = dim3(bg.kernel ? kWBlock : kBfsBlock);
             p.kernelParams = args;
@@ -826,8 +945,8 @@ BfsGraph& bfs_graph_of(hn_graph* g) {
     // rebuilt when the vertex count changes, the edge count outgrows the
     // chunk table or a knob changes the level kernel or its grid
     const int kernel = (int)knob(kKnobBfsKernel);
-    const unsigned grid = (unsigned)(g->info.sms *
-                                     knob(kernel ? kKnobBfsWarpCtasPerSm : kKnobBfsCtasPerSm));
+    const int per_sm = (int)knob(kernel ? kKnobBfsWarpCtasPerSm : kKnobBfsCtasPerSm);
+    const unsigned grid = (unsigned)(g->info.sms * per_sm);
     if (g->bfs && (g->bfs->nV != g->nV || g->nE / kWChunk + 4 > g->bfs->nchunk_cap ||
                    g->bfs->grid != grid || g->bfs->kernel != kernel)) {
         HN_CUDA(cudaStreamSynchronize(g->stream));
@@ -838,6 +957,7 @@ BfsGraph& bfs_graph_of(hn_graph* g) {
         g->bfs = new BfsGraph();
         g->bfs->grid = grid;
         g->bfs->kernel = kernel;
+        g->bfs->per_sm = per_sm;
         try {
             build_bfs_graph(g, *g->bfs);
         } catch (...) {
@@ -923,7 +1043,7 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
             for (int lv = 0; lv <= nV; lv++) {
                 cudaGraphConditionalHandle none = 0;
                 void* args[] = {&bg.state, &none};
-                HN_CUDA(cudaLaunchKernel(level_kernel(bg.kernel, direction_optimizing),
+                HN_CUDA(cudaLaunchKernel(level_kernel(bg.kernel, direction_optimizing, bg.per_sm),
                                          dim3(bg.grid), dim3(bg.kernel ? kWBlock : kBfsBlock),
                                          args, 0, s));
                 count_launch();
@@ -953,6 +1073,10 @@ void bfs_run(hn_graph* g, const int32_t* sources, int k, int32_t* dist, int mem,
     if (k > 0) {
         const int first = ((k - 1) / BfsGraph::kRing) * BfsGraph::kRing;
         for (int i = first; i < k; i++) snap[i] = bg.h_ring[i - first];
+    }
+    if (k > 0) {
+        bg.last = snap[k - 1];
+        bg.have_last = true;
     }
     if (stats)
         for (int i = 0; i < k; i++) {
@@ -989,6 +1113,25 @@ int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist
     HN_REQUIRE(g->nV > 0 || k == 0, "empty graph");
     HN_CUDA(cudaSetDevice(g->device));
     bfs_run(g, sources, k, dist, mem, stats, false);
+    HN_API_END
+}
+
+int hn_bfs_level_trace(hn_graph_t* g, int32_t max_levels, double* us, int64_t* edges,
+                       int32_t* n_levels) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && n_levels && max_levels >= 0, "null argument");
+    *n_levels = 0;
+    if (!g->bfs || !g->bfs->h_ring || !g->bfs->have_last) return HN_OK;
+    const BfsState& t = g->bfs->last;
+    const int lv = t.level - 1 < kTraceLevels ? t.level - 1 : kTraceLevels;
+    const int n = lv < max_levels ? lv : max_levels;
+    unsigned long long prev = t.t_start;
+    for (int i = 0; i < n; i++) {
+        if (us) us[i] = (double)(t.t_end[i] - prev) / 1e3;
+        if (edges) edges[i] = (int64_t)t.lvl_edges[i];
+        prev = t.t_end[i];
+    }
+    *n_levels = n;
     HN_API_END
 }
 

@@ -281,6 +281,15 @@ int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k,
 int hn_bfs_do(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist,
               int mem, hn_bfs_stats_t* stats);
 
+/* Instrumentation: per-level device time (microseconds, from the GPU's
+ * global timer at each level's end inside the BFS CUDA graph) and frontier
+ * edges of the latest hn_bfs / hn_bfs_multi / hn_bfs_do source on this
+ * graph, for its first min(levels, max_levels, 32) levels.  us and edges
+ * may be NULL.  No reference counterpart (the reference times whole runs
+ * with Timer<DEVICE>, hornetsnest/test/BFSTest.cu:35-43). */
+int hn_bfs_level_trace(hn_graph_t* g, int32_t max_levels, double* us, int64_t* edges,
+                       int32_t* n_levels);
+
 /* Batched BFS: up to 64 BFS "slots" traversed together, one 64-bit mask
  * per vertex, each edge read once per level for all slots on it.  Source j
  * seeds slot slots[j] (slots NULL: slot j, k <= nslots); a slot seeded by

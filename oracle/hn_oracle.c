@@ -3,10 +3,12 @@
  * what each function restates; the reference line numbers are repeated at
  * each definition.  Single-threaded on purpose: the reference's host
  * verifiers are single-threaded, and this file doubles as the "port" CPU
- * baseline.
+ * baseline.  The one exception is the input generator hno_gen_rmat, which
+ * is not timed.
  */
 #include "hn_oracle.h"
 
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -24,6 +26,34 @@ static int cmp_i32(const void* a, const void* b) {
 
 static uint64_t pack(int32_t u, int32_t v) {
     return ((uint64_t)(uint32_t)u << 32) | (uint32_t)v;
+}
+
+/* LSD radix sort of 64-bit keys, 16 bits per pass (skipping passes whose
+ * digit is the same for every key). */
+static void radix_sort_u64(uint64_t* k, int64_t n) {
+    if (n < 2) return;
+    uint64_t* tmp = (uint64_t*)malloc(sizeof(uint64_t) * (size_t)n);
+    int64_t* cnt = (int64_t*)malloc(sizeof(int64_t) * 65536);
+    uint64_t* a = k;
+    uint64_t* b = tmp;
+    for (int shift = 0; shift < 64; shift += 16) {
+        memset(cnt, 0, sizeof(int64_t) * 65536);
+        for (int64_t i = 0; i < n; i++) cnt[(a[i] >> shift) & 0xFFFF]++;
+        if (cnt[(a[0] >> shift) & 0xFFFF] == n) continue;
+        int64_t sum = 0;
+        for (int d = 0; d < 65536; d++) {
+            int64_t c = cnt[d];
+            cnt[d] = sum;
+            sum += c;
+        }
+        for (int64_t i = 0; i < n; i++) b[cnt[(a[i] >> shift) & 0xFFFF]++] = a[i];
+        uint64_t* t = a;
+        a = b;
+        b = t;
+    }
+    if (a != k) memcpy(k, a, sizeof(uint64_t) * (size_t)n);
+    free(tmp);
+    free(cnt);
 }
 
 /* Build a CSR (int64 offsets) from sorted packed keys. */
@@ -48,7 +78,7 @@ int64_t hno_build_csr_undirected(int32_t nV, int64_t np, const int32_t* src,
         k[n++] = pack(src[i], dst[i]);
         k[n++] = pack(dst[i], src[i]);
     }
-    qsort(k, (size_t)n, sizeof(uint64_t), cmp_u64);
+    radix_sort_u64(k, n);
     int64_t m = 0;
     for (int64_t i = 0; i < n; i++)
         if (i == 0 || k[i] != k[i - 1]) k[m++] = k[i];
@@ -376,4 +406,102 @@ int32_t hno_ktruss(int32_t nV, const int64_t* off, const int32_t* adj,
     free(alive);
     free(sup);
     return K;
+}
+
+/* ---- synthetic inputs and checksums ---------------------------------- */
+
+/* SplitMix64 (S. Vigna's published finaliser). */
+static uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+typedef struct {
+    int scale, n;
+    uint64_t ta, tb, tc, seed;
+    int64_t i0, i1;
+    int32_t *src, *dst;
+} rmat_job;
+
+/* Pair i: a counter-based SplitMix64 stream per pair, one 32-bit uniform per
+ * recursion level (two per draw), quadrant thresholds a, a+b, a+b+c scaled to
+ * 2^32; a pair with an endpoint >= n is redrawn from the next attempt
+ * counter (64 attempts, then folded into range). */
+static void* rmat_worker(void* arg) {
+    rmat_job* j = (rmat_job*)arg;
+    for (int64_t i = j->i0; i < j->i1; i++) {
+        uint64_t base = splitmix64(j->seed ^ ((uint64_t)i * 0xD1B54A32D192ED03ull));
+        int done = 0;
+        for (int attempt = 0; attempt < 64 && !done; attempt++) {
+            uint64_t ctr = base + (uint64_t)attempt * 0x10000ull;
+            uint32_t u = 0, v = 0;
+            uint64_t bits = 0;
+            for (int l = 0; l < j->scale; l++) {
+                if ((l & 1) == 0) bits = splitmix64(ctr + (uint64_t)(l >> 1));
+                uint64_t r = (l & 1) ? (bits >> 32) : (bits & 0xFFFFFFFFull);
+                /* quadrants: [0,ta) -> (0,0), [ta,tb) -> (0,1),
+                 * [tb,tc) -> (1,0), [tc,2^32) -> (1,1) */
+                uint32_t ub = r >= j->tb;
+                uint32_t vb = (r >= j->ta && r < j->tb) || r >= j->tc;
+                u = (u << 1) | ub;
+                v = (v << 1) | vb;
+            }
+            if ((int32_t)u < j->n && (int32_t)v < j->n) {
+                j->src[i] = (int32_t)u;
+                j->dst[i] = (int32_t)v;
+                done = 1;
+            }
+        }
+        if (!done) {
+            j->src[i] = (int32_t)(base % (uint64_t)j->n);
+            j->dst[i] = (int32_t)((base >> 32) % (uint64_t)j->n);
+        }
+    }
+    return NULL;
+}
+
+/* The R-MAT pairs of this repository's input generator (hn_gen_rmat_host in
+ * hornet_b200/csrc/hn_gen.cu): the reference has no R-MAT generator, so the
+ * inputs are defined by this function and the library's, which the tests
+ * keep bit-identical. */
+int hno_gen_rmat(int32_t scale, int32_t n, int64_t np, double a, double b, double c,
+                 uint64_t seed, int32_t* src, int32_t* dst, int32_t nthreads) {
+    if (scale < 1 || scale > 31 || n <= 0 || (int64_t)n > ((int64_t)1 << scale)) return -1;
+    if (a < 0 || b < 0 || c < 0 || a + b + c > 1.0) return -1;
+    const double two32 = 4294967296.0;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    rmat_job jobs[256];
+    for (int t = 0; t < nthreads; t++) {
+        rmat_job* j = &jobs[t];
+        j->scale = scale;
+        j->n = n;
+        j->ta = (uint64_t)(a * two32);
+        j->tb = (uint64_t)((a + b) * two32);
+        j->tc = (uint64_t)((a + b + c) * two32);
+        j->seed = seed;
+        j->i0 = np * t / nthreads;
+        j->i1 = np * (t + 1) / nthreads;
+        j->src = src;
+        j->dst = dst;
+        if (pthread_create(&th[t], NULL, rmat_worker, j) != 0) {
+            rmat_worker(j);
+            th[t] = 0;
+        }
+    }
+    for (int t = 0; t < nthreads; t++)
+        if (th[t]) pthread_join(th[t], NULL);
+    return 0;
+}
+
+/* Order-independent checksum of a CSR's edge multiset:
+ * sum over edges (u, v) of splitmix64(u << 32 | v), mod 2^64. */
+uint64_t hno_adjacency_hash(int32_t nV, const int64_t* off, const int32_t* adj) {
+    uint64_t h = 0;
+    for (int32_t u = 0; u < nV; u++)
+        for (int64_t e = off[u]; e < off[u + 1]; e++) h += splitmix64(pack(u, adj[e]));
+    return h;
 }

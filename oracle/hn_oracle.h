@@ -90,6 +90,17 @@ void hno_cc_reference_colors(int32_t nV, const int64_t* off, const int32_t* adj,
 int32_t hno_ktruss(int32_t nV, const int64_t* off, const int32_t* adj,
                    int32_t* edge_truss);
 
+/* R-MAT edge pairs of this repository's input generator (restated from
+ * hn_gen_rmat_host, hornet_b200/csrc/hn_gen.cu; the reference has none):
+ * pair i depends only on (seed, i).  nthreads host threads.  Returns 0, or
+ * -1 on bad parameters. */
+int hno_gen_rmat(int32_t scale, int32_t n, int64_t np, double a, double b, double c,
+                 uint64_t seed, int32_t* src, int32_t* dst, int32_t nthreads);
+
+/* Order-independent checksum of the edge multiset of a CSR:
+ * sum of splitmix64(u << 32 | v) over its edges, mod 2^64. */
+uint64_t hno_adjacency_hash(int32_t nV, const int64_t* off, const int32_t* adj);
+
 #ifdef __cplusplus
 }
 #endif

@@ -54,6 +54,11 @@ def lib() -> ctypes.CDLL:
         l.hno_cc_reference_colors.restype = None
         l.hno_ktruss.argtypes = [I32, _P, _P, _P]
         l.hno_ktruss.restype = I32
+        l.hno_gen_rmat.argtypes = [I32, I32, I64, ctypes.c_double, ctypes.c_double,
+                                   ctypes.c_double, ctypes.c_uint64, _P, _P, I32]
+        l.hno_gen_rmat.restype = ctypes.c_int
+        l.hno_adjacency_hash.argtypes = [I32, _P, _P]
+        l.hno_adjacency_hash.restype = ctypes.c_uint64
         _lib = l
     return _lib
 
@@ -83,6 +88,26 @@ class Csr:
     def coo(self) -> Tuple[np.ndarray, np.ndarray]:
         src = np.repeat(np.arange(self.nV, dtype=np.int32), np.diff(self.off))
         return src, self.adj.copy()
+
+
+def gen_rmat(scale: int, np_pairs: int, seed: int, n_vertices: Optional[int] = None,
+             a: float = 0.57, b: float = 0.19, c: float = 0.19,
+             threads: Optional[int] = None) -> Tuple[np.ndarray, np.ndarray]:
+    """The repository's R-MAT input pairs (restated generator, bit-identical
+    to the library's hn_gen_rmat_host)."""
+    n = (1 << scale) if n_vertices is None else int(n_vertices)
+    src = np.empty(np_pairs, np.int32)
+    dst = np.empty(np_pairs, np.int32)
+    t = threads or min(32, os.cpu_count() or 1)
+    rc = lib().hno_gen_rmat(scale, n, np_pairs, a, b, c, seed & (2**64 - 1), _p(src), _p(dst), t)
+    if rc != 0:
+        raise ValueError("bad R-MAT parameters")
+    return src, dst
+
+
+def adjacency_hash(g: "Csr") -> int:
+    """Order-independent checksum of the graph's edge multiset."""
+    return int(lib().hno_adjacency_hash(g.nV, _p(g.off), _p(g.adj)))
 
 
 def build_csr_undirected(nV: int, src, dst) -> Csr:
