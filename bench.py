@@ -663,35 +663,6 @@ def bench_update(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
 # batch workload: many small graphs of uneven size
 # ---------------------------------------------------------------------------
 
-def c4_build(H, dev, n_graphs, seed=4096):
-    """n_graphs graphs, n ~ LogUniform[1024, 65536]; half Erdos-Renyi with
-    mean degree 8 (uniform pairs, 4n of them), half R-MAT edge factor 16
-    (a=.57 b=.19 c=.19, drawn at scale ceil(log2 n) with endpoints >= n
-    resampled); generated on the device into one disjoint union."""
-    import torch
-    rng = np.random.default_rng(seed)
-    sizes = np.exp(rng.uniform(np.log(1024), np.log(65536), n_graphs)).astype(np.int64)
-    kinds = rng.permutation(np.repeat([0, 1], [n_graphs // 2, n_graphs - n_graphs // 2]))
-    pairs = np.where(kinds == 0, 4 * sizes, 16 * sizes)
-    bases = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
-    poff = np.concatenate([[0], np.cumsum(pairs)]).astype(np.int64)
-    src = torch.empty(int(poff[-1]), dtype=torch.int32, device=f"cuda:{dev}")
-    dst = torch.empty_like(src)
-    for i in range(n_graphs):
-        n = int(sizes[i])
-        sc = int(np.ceil(np.log2(n)))
-        s, d = src[poff[i]:poff[i + 1]], dst[poff[i]:poff[i + 1]]
-        kw = dict(a=0.25, b=0.25, c=0.25) if kinds[i] == 0 else {}
-        H.gen_rmat_device(sc, int(pairs[i]), seed * 1_000_003 + i, s, d, n_vertices=n,
-                          device=dev, **kw)
-        s += int(bases[i])
-        d += int(bases[i])
-    csr = H.coo_to_csr_device(int(sizes.sum()), src, dst, device=dev)
-    del src, dst
-    h = H.hornet_from_device_csr(csr, device=dev)
-    return h, csr, sizes, bases, kinds
-
-
 def bench_batch(args, H, dev, stream, rank, world, peak, peak_kind, barrier, max_over_ranks,
                 sum_over_ranks):
     """Batched form (one hn_bfs_batch over all graphs x 8 sources + one TC
@@ -700,10 +671,10 @@ def bench_batch(args, H, dev, stream, rank, world, peak, peak_kind, barrier, max
     graph's own Hornet) on a seeded sample of the same graphs."""
     import ctypes
     import torch
-    from hornet_b200.batching import GraphBatch
+    from hornet_b200.batching import GraphBatch, synthetic_union
     K, W = max(1, min(args.steps, 8)), max(3, min(args.warmup, 3))
     t0 = time.perf_counter()
-    h, csr, sizes, bases, kinds = c4_build(H, dev, args.graphs, seed=4096 + rank)
+    h, csr, sizes, bases, kinds = synthetic_union(args.graphs, seed=4096 + rank, device=dev)
     H.lib().hn_graph_set_stream(h.handle, ctypes.c_void_p(stream.cuda_stream))
     build_s = time.perf_counter() - t0
     nV, nE = h.nV(), h.nE()

@@ -93,6 +93,7 @@ _SIGNATURES = {
     "hn_graph_degrees": [_P, _P, _INT],
     "hn_graph_device_view": [_P, _P],
     "hn_graph_memory": [_P, _P, _P, _P],
+    "hn_graph_adjacency_hash": [_P, _P],
     "hn_batch_create": [_P, _I64, _P, _P, _INT, _P],
     "hn_batch_reset": [_P, _I64, _P, _P, _INT],
     "hn_batch_size": [_P, _P],
@@ -394,6 +395,13 @@ class Hornet:
         d = np.empty(self.nV(), np.int32)
         _check(lib().hn_graph_degrees(self._h, d.ctypes.data_as(_P), HN_MEM_HOST))
         return d
+
+    def adjacency_hash(self) -> int:
+        """Order-independent checksum of the edge multiset (computed on the
+        device; hn_graph_adjacency_hash)."""
+        h = ctypes.c_uint64(0)
+        _check(lib().hn_graph_adjacency_hash(self._h, ctypes.byref(h)))
+        return int(h.value)
 
     def device(self) -> DeviceView:
         v = DeviceView()

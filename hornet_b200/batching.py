@@ -25,6 +25,47 @@ import numpy as np
 from . import HN_MEM_DEVICE, Hornet, _check, _P, lib
 
 
+def synthetic_specs(n_graphs: int, seed: int = 4096):
+    """The many-small-graphs workload: n_graphs graphs with vertex counts
+    log-uniform in [1024, 65536]; half Erdos-Renyi with mean degree 8
+    (4n uniform pairs), half R-MAT with edge factor 16 (a=.57 b=.19 c=.19,
+    16n pairs drawn at scale ceil(log2 n), endpoints >= n redrawn).  Returns
+    (sizes, bases, kinds, specs); graph i's pairs are
+    gen_rmat(scale, pairs, pair_seed, n_vertices=n, a, b, c) with
+    (scale, pairs, pair_seed, n, a, b, c) = specs[i]; kinds[i] is 0 for ER."""
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1024), np.log(65536), n_graphs)).astype(np.int64)
+    kinds = rng.permutation(np.repeat([0, 1], [n_graphs // 2, n_graphs - n_graphs // 2]))
+    pairs = np.where(kinds == 0, 4 * sizes, 16 * sizes)
+    bases = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    specs = []
+    for i in range(n_graphs):
+        n = int(sizes[i])
+        abc = (0.25, 0.25, 0.25) if kinds[i] == 0 else (0.57, 0.19, 0.19)
+        specs.append((int(np.ceil(np.log2(n))), int(pairs[i]), seed * 1_000_003 + i, n) + abc)
+    return sizes, bases, kinds, specs
+
+
+def synthetic_union(n_graphs: int, seed: int = 4096, device: int = 0):
+    """The graphs of synthetic_specs generated on the device into one
+    disjoint union.  Returns (hornet, device csr, sizes, bases, kinds)."""
+    import torch
+    from . import coo_to_csr_device, gen_rmat_device, hornet_from_device_csr
+    sizes, bases, kinds, specs = synthetic_specs(n_graphs, seed)
+    poff = np.concatenate([[0], np.cumsum([sp[1] for sp in specs])]).astype(np.int64)
+    src = torch.empty(int(poff[-1]), dtype=torch.int32, device=f"cuda:{device}")
+    dst = torch.empty_like(src)
+    for i, (sc, npairs, pseed, n, a, b, c) in enumerate(specs):
+        s, d = src[poff[i]:poff[i + 1]], dst[poff[i]:poff[i + 1]]
+        gen_rmat_device(sc, npairs, pseed, s, d, n_vertices=n, a=a, b=b, c=c, device=device)
+        s += int(bases[i])
+        d += int(bases[i])
+    csr = coo_to_csr_device(int(sizes.sum()), src, dst, device=device)
+    del src, dst
+    h = hornet_from_device_csr(csr, device=device)
+    return h, csr, sizes, bases, kinds
+
+
 class GraphBatch:
     """A batch of graphs as one Hornet.  `bases[i]` is the first vertex id of
     graph i in the union; `sizes[i]` its vertex count."""

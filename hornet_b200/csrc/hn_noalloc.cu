@@ -27,7 +27,13 @@
 //
 // The algorithm is the one hn_cc uses (ECL-CC style union-find on an
 // Afforest schedule, hn_cc.cu), written here a second time against a plain
-// CSR so that the existing path stays untouched.
+// CSR so that the existing path stays untouched.  Like hn_cc it needs an
+// undirected graph stored symmetrically (every edge in both endpoints'
+// lists): vertices of the giant component skip their remaining neighbours,
+// so an edge stored only in a giant-component vertex's list would be lost.
+// The CSR is validated first (offsets start at 0 and never decrease, every
+// id is a vertex) by one pass over off[] and adj[]; the union-find kernels
+// are skipped when the offsets are malformed.
 #include <mutex>
 
 #include "hn_graph.cuh"
@@ -37,7 +43,8 @@ namespace {
 
 constexpr int kNoAllocMaxVertices = 1 << 22;        // 4,194,304 vertices
 constexpr int kNoAllocCounters = 64;                // [0] giant root, [1] list size,
-                                                    // [2] components, [3] bad-id flag
+                                                    // [2] components, [3] bad-id flag,
+                                                    // [4] bad-offsets flag
 static __device__ __align__(256) int g_cc_scratch[kNoAllocMaxVertices + kNoAllocCounters];
 
 constexpr int kMaxDevices = 64;
@@ -71,29 +78,58 @@ __device__ __forceinline__ void na_link(int* __restrict__ parent, int u, int v) 
     }
 }
 
-__global__ void k_na_init(int* __restrict__ parent, int nV) {
+// Validation of the caller's CSR before anything follows it: off[0] == 0
+// and off non-decreasing (ctr[4]); then, only when the offsets are sound,
+// every id of adj[0, off[nV]) inside [0, nV) (ctr[3]).  The kernels after
+// them return at once when ctr[4] is set, so a malformed offset array is
+// never used to address adj.
+__global__ void k_na_check_off(const int32_t* __restrict__ off, int nV, int* __restrict__ ctr) {
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    bool bad = t0 == 0 && off[0] != 0;
+    for (long long v = t0; v < nV; v += (long long)gridDim.x * blockDim.x)
+        if (off[v + 1] < off[v]) bad = true;
+    if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) ctr[4] = 1;
+}
+
+__global__ void k_na_check_ids(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
+                               int nV, int* __restrict__ ctr) {
+    if (ctr[4]) return;
+    const long long m = off[nV];
+    bool bad = false;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int u = adj[i];
+        if (u < 0 || u >= nV) bad = true;
+    }
+    if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) ctr[3] = 1;
+}
+
+__global__ void k_na_init(int* __restrict__ parent, int nV, const int* __restrict__ ctr) {
+    if (ctr[4]) return;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
          v += (long long)gridDim.x * blockDim.x)
         parent[v] = (int)v;
 }
 
 // first kSampleNa neighbours of every vertex; ids outside [0,nV) are
-// flagged and skipped
+// skipped (k_na_check has flagged them)
 __global__ void k_na_sample(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                             int nV, int* __restrict__ parent, int* __restrict__ ctr) {
+    if (ctr[4]) return;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
          v += (long long)gridDim.x * blockDim.x) {
         int b = off[v], e = off[v + 1];
         int k = e - b < kSampleNa ? e - b : kSampleNa;
         for (int i = 0; i < k; i++) {
             int u = adj[b + i];
-            if (u < 0 || u >= nV) { ctr[3] = 1; continue; }
+            if (u < 0 || u >= nV) continue;
             na_link(parent, (int)v, u);
         }
     }
 }
 
-__global__ void k_na_compress(int* __restrict__ parent, int nV) {
+__global__ void k_na_compress(int* __restrict__ parent, int nV, const int* __restrict__ ctr) {
+    if (ctr[4]) return;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
          v += (long long)gridDim.x * blockDim.x)
         parent[v] = na_find(parent, (int)v);
@@ -101,6 +137,7 @@ __global__ void k_na_compress(int* __restrict__ parent, int nV) {
 
 // most frequent root among 256 evenly spaced vertices (one CTA of 256)
 __global__ void k_na_giant(const int* __restrict__ parent, int nV, int* __restrict__ ctr) {
+    if (ctr[4]) return;
     __shared__ int s_r[256];
     __shared__ unsigned long long s_key;
     int t = threadIdx.x;
@@ -117,6 +154,7 @@ __global__ void k_na_giant(const int* __restrict__ parent, int nV, int* __restri
 
 __global__ void k_na_worklist(const int32_t* __restrict__ off, const int* __restrict__ parent,
                               int nV, int* __restrict__ list, int* __restrict__ ctr) {
+    if (ctr[4]) return;
     const int gr = ctr[0];
     for (long long v0 = blockIdx.x * (long long)blockDim.x; v0 < nV;
          v0 += (long long)gridDim.x * blockDim.x) {
@@ -130,6 +168,7 @@ __global__ void k_na_worklist(const int32_t* __restrict__ off, const int* __rest
 __global__ void k_na_rest(const int32_t* __restrict__ off, const int32_t* __restrict__ adj,
                           int nV, const int* __restrict__ list, int* __restrict__ parent,
                           int* __restrict__ ctr) {
+    if (ctr[4]) return;
     const int n = ctr[1];
     const int lane = threadIdx.x & 31;
     long long wid = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -139,13 +178,14 @@ __global__ void k_na_rest(const int32_t* __restrict__ off, const int32_t* __rest
         int b = off[v], e = off[v + 1];
         for (int k = b + kSampleNa + lane; k < e; k += 32) {
             int u = adj[k];
-            if (u < 0 || u >= nV) { ctr[3] = 1; continue; }
+            if (u < 0 || u >= nV) continue;
             na_link(parent, v, u);
         }
     }
 }
 
 __global__ void k_na_finish(int* __restrict__ parent, int nV, int* __restrict__ ctr) {
+    if (ctr[4]) return;
     int mine = 0;
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
          v += (long long)gridDim.x * blockDim.x) {
@@ -191,24 +231,28 @@ extern "C" int hn_cc_csr_noalloc(int32_t nV, const int32_t* off, const int32_t* 
     int* list = scratch;
     int* ctr = scratch + kNoAllocMaxVertices;
     // the array keeps the previous call's contents: clear the counters
-    HN_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int) * 4, s));
+    HN_CUDA(cudaMemsetAsync(ctr, 0, sizeof(int) * 5, s));
     if (nV > 0) {
         int dev = 0, sms = 148;
         HN_CUDA(cudaGetDevice(&dev));
         HN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         long long gv = ((long long)nV + kB - 1) / kB;
         if (gv > (long long)sms * 8) gv = (long long)sms * 8;
-        HN_LAUNCH(k_na_init, gv, kB, 0, s, labels, nV);
+        HN_LAUNCH(k_na_check_off, gv, kB, 0, s, off, nV, ctr);
+        HN_LAUNCH(k_na_check_ids, (long long)sms * 8, kB, 0, s, off, adj, nV, ctr);
+        HN_LAUNCH(k_na_init, gv, kB, 0, s, labels, nV, ctr);
         HN_LAUNCH(k_na_sample, gv, kB, 0, s, off, adj, nV, labels, ctr);
-        HN_LAUNCH(k_na_compress, gv, kB, 0, s, labels, nV);
+        HN_LAUNCH(k_na_compress, gv, kB, 0, s, labels, nV, ctr);
         HN_LAUNCH(k_na_giant, 1, 256, 0, s, labels, nV, ctr);
         HN_LAUNCH(k_na_worklist, gv, kB, 0, s, off, labels, nV, list, ctr);
         HN_LAUNCH(k_na_rest, (long long)sms * 8, kB, 0, s, off, adj, nV, list, labels, ctr);
         HN_LAUNCH(k_na_finish, gv, kB, 0, s, labels, nV, ctr);
     }
-    int host_ctr[4] = {0, 0, 0, 0};
+    int host_ctr[5] = {0, 0, 0, 0, 0};
     HN_CUDA(cudaMemcpyAsync(host_ctr, ctr, sizeof(host_ctr), cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
+    if (host_ctr[4])
+        throw Error(HN_ERR_INVALID, "CSR offsets must start at 0 and never decrease");
     if (host_ctr[3]) throw Error(HN_ERR_INVALID, "CSR neighbour id outside [0, nV)");
     if (n_components) *n_components = host_ctr[2];
     HN_API_END

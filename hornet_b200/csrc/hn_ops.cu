@@ -22,6 +22,30 @@ __global__ void k_vertex_degree(hornet::HornetDevice hd, int32_t* out) {
         out[v] = hd.vertex((int)v).degree();
 }
 
+__device__ __forceinline__ unsigned long long mix64(unsigned long long x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// Order-independent checksum of the edge multiset: sum over edges (u, v) of
+// SplitMix64(u << 32 | v), a warp per vertex, one atomic per warp.
+__global__ void k_adjacency_hash(const VRec* __restrict__ vtab, const int32_t* __restrict__ pool,
+                                 int nV, unsigned long long* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    unsigned long long h = 0;
+    for (long long v = w0; v < nV; v += nw) {
+        const VRec r = vtab[v];
+        const unsigned long long hi = (unsigned long long)(unsigned)v << 32;
+        for (int i = lane; i < r.deg; i += 32) h += mix64(hi | (unsigned)pool[r.off + i]);
+    }
+    for (int o = 16; o; o >>= 1) h += __shfl_down_sync(0xFFFFFFFFu, h, o);
+    if (lane == 0 && h) atomicAdd(out, h);
+}
+
 hornet::HornetDevice view_of(hn_graph* g) {
     hn_device_view_t v;
     v.nV = g->nV;
@@ -78,5 +102,22 @@ extern "C" int hn_for_all_vertices_degree(hn_graph_t* g, int32_t* out) {
     HN_CUDA(cudaSetDevice(g->device));
     HN_LAUNCH(k_vertex_degree, grid_for(g, g->nV, 256), 256, 0, g->stream, view_of(g), out);
     HN_CUDA(cudaStreamSynchronize(g->stream));
+    HN_API_END
+}
+
+extern "C" int hn_graph_adjacency_hash(hn_graph_t* g, uint64_t* hash) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && hash, "null argument");
+    HN_CUDA(cudaSetDevice(g->device));
+    DevBuf<unsigned long long> acc;
+    acc.alloc(1, g->stream);
+    HN_CUDA(cudaMemsetAsync(acc.get(), 0, sizeof(unsigned long long), g->stream));
+    if (g->nV > 0)
+        HN_LAUNCH(k_adjacency_hash, grid_for(g, (long long)g->nV * 32, 256), 256, 0, g->stream,
+                  g->vtab, g->pool, g->nV, acc.get());
+    unsigned long long h = 0;
+    HN_CUDA(cudaMemcpyAsync(&h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, g->stream));
+    HN_CUDA(cudaStreamSynchronize(g->stream));
+    *hash = h;
     HN_API_END
 }

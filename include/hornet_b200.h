@@ -202,6 +202,12 @@ int hn_graph_export_csr(hn_graph_t* g, int32_t* off, int32_t* adj, int mem);
 int hn_graph_degrees(hn_graph_t* g, int32_t* deg, int mem);
 /* hornet.device() (Hornet.cuh:117): raw device view for user kernels. */
 int hn_graph_device_view(hn_graph_t* g, hn_device_view_t* view);
+/* Order-independent checksum of the graph's edge multiset, computed on the
+ * device: the sum over stored edges (u, v) of SplitMix64((u << 32) | v),
+ * modulo 2^64 (a validation aid with no reference counterpart: the
+ * reference's tests compare whole sorted COO exports, HornetInsertTest.cu:
+ * 42-75, which at full size means gigabytes on the host). */
+int hn_graph_adjacency_hash(hn_graph_t* g, uint64_t* hash);
 /* Slots held by the edge pool and by live blocks (for accounting). */
 int hn_graph_memory(hn_graph_t* g, int64_t* pool_slots, int64_t* used_slots,
                     int64_t* free_list_blocks);
@@ -386,12 +392,17 @@ int hn_graph_read_bin(const char* path, int device, hn_graph_t** out);
  * synchronisation of cudaMalloc/cudaFree): the same labels as
  * hn_cc(HN_CC_MIN_ID) computed over a caller-owned device CSR
  * (off[nV+1], adj[off[nV]]) into a caller-owned device array labels[nV],
- * with no cudaMalloc/cudaFree and no allocating library call.  Its only
- * working memory is a 16 MiB static device array inside the library, so
- * nV is limited to 4,194,304 (HN_ERR_CAPACITY above that).  The first call
- * on a device resolves that array's address: make it before any stream
- * capture.  All calls share the array; calls that overlap on the GPU race.
- * `stream` is a cudaStream_t (NULL = legacy default stream); the call
+ * with no cudaMalloc/cudaFree and no allocating library call.
+ * The CSR must be undirected and symmetric (each edge stored in both
+ * endpoints' lists), as hn_cc's graphs are; a one-sided CSR gives wrong
+ * labels without an error.  The offsets (off[0] == 0, never decreasing) and
+ * every id of adj[0, off[nV]) are checked on the device first:
+ * HN_ERR_INVALID, and labels not written, when they are malformed.
+ * Its only working memory is a 16 MiB static device array inside the
+ * library, so nV is limited to 4,194,304 (HN_ERR_CAPACITY above that).  The
+ * first call on a device resolves that array's address: make it before any
+ * stream capture.  All calls share the array; calls that overlap on the GPU
+ * race.  `stream` is a cudaStream_t (NULL = legacy default stream); the call
  * returns when the labels are ready.  *n_components (may be NULL) is host. */
 int hn_cc_csr_noalloc(int32_t nV, const int32_t* off, const int32_t* adj,
                       int32_t* labels, int32_t* n_components, void* stream);

@@ -90,6 +90,13 @@ void hno_cc_reference_colors(int32_t nV, const int64_t* off, const int32_t* adj,
 int32_t hno_ktruss(int32_t nV, const int64_t* off, const int32_t* adj,
                    int32_t* edge_truss);
 
+/* The same truss numbers by support peeling (Wang & Cheng, PVLDB 2012):
+ * supports once, then decremented per destroyed triangle.  An independent
+ * second computation, fast enough for the benchmark-scale pins; checked
+ * against hno_ktruss by the tests. */
+int32_t hno_ktruss_peel(int32_t nV, const int64_t* off, const int32_t* adj,
+                        int32_t* edge_truss);
+
 /* R-MAT edge pairs of this repository's input generator (restated from
  * hn_gen_rmat_host, hornet_b200/csrc/hn_gen.cu; the reference has none):
  * pair i depends only on (seed, i).  nthreads host threads.  Returns 0, or

@@ -54,6 +54,8 @@ def lib() -> ctypes.CDLL:
         l.hno_cc_reference_colors.restype = None
         l.hno_ktruss.argtypes = [I32, _P, _P, _P]
         l.hno_ktruss.restype = I32
+        l.hno_ktruss_peel.argtypes = [I32, _P, _P, _P]
+        l.hno_ktruss_peel.restype = I32
         l.hno_gen_rmat.argtypes = [I32, I32, I64, ctypes.c_double, ctypes.c_double,
                                    ctypes.c_double, ctypes.c_uint64, _P, _P, I32]
         l.hno_gen_rmat.restype = ctypes.c_int
@@ -180,6 +182,22 @@ def ktruss(g: Csr) -> Tuple[int, np.ndarray]:
     et = np.empty(max(1, g.nE), np.int32)
     k = lib().hno_ktruss(g.nV, _p(g.off), _p(g.adj), _p(et))
     return int(k), et[:g.nE].copy()
+
+
+def ktruss_peel(g: Csr) -> Tuple[int, np.ndarray]:
+    """Truss numbers by support peeling (independent of ktruss(); same
+    results, fast enough for benchmark-scale graphs)."""
+    et = np.empty(max(1, g.nE), np.int32)
+    k = lib().hno_ktruss_peel(g.nV, _p(g.off), _p(g.adj), _p(et))
+    return int(k), et[:g.nE].copy()
+
+
+def canon_labels_fast(lab: np.ndarray) -> np.ndarray:
+    """canon_labels, vectorised: every vertex gets the smallest vertex id
+    carrying its label."""
+    lab = np.asarray(lab)
+    uniq, first, inv = np.unique(lab, return_index=True, return_inverse=True)
+    return first.astype(np.int32)[inv]
 
 
 # ---------------------------------------------------------------------------

@@ -1,6 +1,16 @@
 """GPU: the benchmark's full-size graph (R-MAT scale 22, ef 16, generated on
-the device: 4,194,304 vertices, 128,302,074 directed edges), checked through
-size-independent properties, since the CPU oracle is too slow at this size:
+the device: 4,194,304 vertices, 128,302,074 directed edges).
+
+Pinned to the reference (tests/golden/fullsize.json, made on the CPU by
+tests/golden/make_fullsize.py): the graph's edge count and adjacency
+checksum; BFS distances from 8 of the benchmark's sources equal the
+reference's graph::BFS (xlib/src/Graph/BFS.cpp) byte for byte; CC labels
+equal graph::WCC (xlib/src/Graph/WCC.cpp) relabelled to minimum ids; the
+triangle total equals the restated hostCountTriangles
+(hornetsnest/test/TriangleTest2.cu:22-69); k-truss edge truss numbers equal
+the CPU truss decomposition (scale 18 and, when pinned, scale 22).
+
+Also checked through size-independent properties:
 
 * BFS: a BFS certificate on every source (source at 0; along every edge
   distances differ by at most one; every reached vertex other than the
@@ -15,6 +25,9 @@ size-independent properties, since the CPU oracle is too slow at this size:
   exported CSR exactly, and after the insert every list is strictly sorted.
 """
 import ctypes
+import hashlib
+import json
+import os
 
 import numpy as np
 import pytest
@@ -24,6 +37,23 @@ import hornet_b200 as H
 pytestmark = pytest.mark.gpu
 
 SCALE = 22
+GOLD_PATH = os.path.join(os.path.dirname(__file__), "golden", "fullsize.json")
+GOLD = json.load(open(GOLD_PATH)) if os.path.exists(GOLD_PATH) else {}
+
+
+def _sha(a) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, "<i4").tobytes()).hexdigest()
+
+
+def _device_rmat(scale, ef=16, seed=1):
+    import torch
+    n = 1 << scale
+    src = torch.empty(ef * n, dtype=torch.int32, device="cuda")
+    dst = torch.empty_like(src)
+    H.gen_rmat_device(scale, ef * n, seed, src, dst)
+    csr = H.coo_to_csr_device(n, src, dst)
+    del src, dst
+    return H.hornet_from_device_csr(csr), csr
 
 
 @pytest.fixture(scope="module")
@@ -45,6 +75,50 @@ def big():
     srcv = torch.repeat_interleave(torch.arange(nV, device="cuda", dtype=torch.int32), deg)
     yield h, off, adj, srcv
     H.tune_reset()
+
+
+def test_c2_pinned_to_reference(big):
+    """Graph, BFS (top-down and direction-optimising), CC and TC at scale 22
+    equal the reference's host code / the restated TC on the same graph."""
+    g = GOLD["rmat22"]
+    h, off, adj, srcv = big
+    assert (h.nV(), h.nE()) == (g["nV"], g["nE"])
+    assert h.adjacency_hash() == int(g["adjacency_hash"])
+    srcs = np.array(g["bfs"]["sources"], np.int32)
+    bfs = H.BfsTopDown(h)
+    for do in (False, True):
+        dist, st = bfs.run_multi(srcs, direction_optimizing=do)
+        for j in range(len(srcs)):
+            assert _sha(dist[j]) == g["bfs"]["sha256"][j], (do, j)
+            assert st[j].visited == g["bfs"]["reached"][j]
+            assert st[j].levels == g["bfs"]["levels"][j]
+    cc = H.CC(h)
+    lab = cc.run()
+    assert cc.n_components == g["cc"]["components"]
+    assert _sha(lab) == g["cc"]["sha256_min_id"]
+    assert H.TriangleCounting2(h).run() == g["tc"]["triangles"]
+
+
+def _check_ktruss(h, entry):
+    kt = H.KTruss(h)
+    kmax = kt.run()
+    et = kt.edge_truss
+    assert kmax == entry["max_k"]
+    ks, cnt = np.unique(et, return_counts=True)
+    assert {str(int(k)): int(c) for k, c in zip(ks, cnt)} == entry["edges_per_truss"]
+    assert _sha(et) == entry["edge_truss_sha256"]
+
+
+@pytest.mark.skipif("ktruss" not in GOLD.get("rmat22", {}), reason="scale-22 truss not pinned")
+def test_ktruss_scale22_pinned(big):
+    h, off, adj, srcv = big
+    _check_ktruss(h, GOLD["rmat22"]["ktruss"])
+
+
+def test_ktruss_scale18_pinned():
+    h, csr = _device_rmat(18)
+    assert h.nE() == GOLD["ktruss18"]["nE"]
+    _check_ktruss(h, GOLD["ktruss18"])
 
 
 def _bfs_certificate(dist, srcv, adj, s):
