@@ -169,6 +169,15 @@ def make_graph_device(H, scale, ef, seed, device):
     return H.hornet_from_device_csr(csr, device=device), csr
 
 
+def static_config(scale, nV, nE, world):
+    """The static-analytics workload's config, identical in both arms."""
+    return {"workload": f"static analytics: R-MAT scale {scale}, edge factor 16, "
+                        f"a=.57 b=.19 c=.19, BFS TopDown from 64 seeded non-isolated sources",
+            "nV": nV, "nE": nE, "sources": 64,
+            "parallelism": f"replicas x{world}",
+            "l2": "graph data > 126 MB L2; no flush"}
+
+
 def pick_sources(deg, k, seed):
     rng = np.random.default_rng(seed)
     cand = np.nonzero(deg > 0)[0]
@@ -404,12 +413,8 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
         "steps": K, "warmup": W, "ms_per_step": round(t_max * 1e3 / K, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic R-MAT (seeded), no dataset",
-        "config": {"workload": f"static analytics: R-MAT scale {scale}, edge factor 16, "
-                               f"a=.57 b=.19 c=.19, BFS TopDown from 64 seeded non-isolated sources",
-                   "nV": nV, "nE": nE, "sources": 64,
-                   "graph500_gteps": round(value / 2, 4),
-                   "parallelism": f"replicas x{world}",
-                   "l2": "graph data > 126 MB L2; no flush"},
+        "config": static_config(scale, nV, nE, world),
+        "graph500_gteps": round(value / 2, 4),
         "e2e": {"value": round(e2e_value, 4), "unit": "GTEPS", "h2d_bytes_per_step": 4,
                 "d2h_bytes_per_step": 4 * nV + 8},
         "roofline": roof,
@@ -456,6 +461,16 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
                   "triangles": int(tc.countTriangles()), "ms": round(t * 1e3, 3),
                   "roofline": troof, "kernels_ms": {k: round(v["ms"], 3) for k, v in rep.items()},
                   "rep_ms": [round(x * 1e3, 2) for x in tc_reps], "clocks": tc_clocks}
+    cpu = not args.no_cpu
+    if cpu:
+        from oracle import oracle as O
+        g_host = O.Csr(off.astype(np.int64), adj)
+        sec, e = O.time_tc_sample(g_host, stride=16, first=7)
+        also["tc"]["cpu_baseline"] = {
+            "value": round(e / sec, 1), "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": f"restated hostCountTriangles (hornetsnest/test/TriangleTest2.cu:22-69) "
+                      f"over every 16th edge of the degree-oriented graph: {e} oriented "
+                      f"edges in {sec:.1f} s"}
     # connected components
     cc = H.CC(h)
     lab = torch.empty(nV, dtype=torch.int32, device=f"cuda:{dev}")
@@ -469,6 +484,12 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
                            peak_kind, rep, f"R-MAT scale {scale} CC")
     also["cc"] = {"metric": "CC edges/s", "value": round(nE / t, 1), "unit": "edges/s",
                   "components": cc.n_components, "ms": round(t * 1e3, 3), "roofline": croof}
+    if cpu and O.ref_available():
+        sec, ncomp = O.ref_time_wcc(g_host)
+        also["cc"]["cpu_baseline"] = {
+            "value": round(nE / sec, 1), "unit": "edges/s", "cores": 1, "kind": "reference",
+            "sample": f"graph::WCC (xlib/src/Graph/WCC.cpp) on the whole graph, {sec:.2f} s, "
+                      f"{ncomp} components"}
     # k-truss decomposition (all K, incremental peel), timed once
     if not args.no_ktruss:
         kt = H.KTruss(h)
@@ -477,8 +498,19 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
         tk = time.perf_counter() - t0
         also["ktruss"] = {"metric": "k-truss edges/s", "value": round(nE / tk, 1),
                           "unit": "edges/s", "max_k": int(kmax), "ms": round(tk * 1e3, 3),
-                          "note": "all K from 3 to max_k; host-timed single run "
-                                  "(one host round trip per peel round)"}
+                          "note": "all K from 3 to max_k; host-timed single run"}
+        if cpu:
+            s16, d16 = O.gen_rmat(16, 16 << 16, 1)
+            g16 = O.build_csr_undirected(1 << 16, s16, d16)
+            t0 = time.perf_counter()
+            k16, _ = O.ktruss_peel(g16)
+            sec = time.perf_counter() - t0
+            also["ktruss"]["cpu_baseline"] = {
+                "value": round(g16.nE / sec, 1), "unit": "edges/s", "cores": 1, "kind": "port",
+                "sample": f"support-peeling truss decomposition (the oracle's; the restated "
+                          f"KTruss.cu:90-174 loop needs minutes at scale 14) on the R-MAT scale-16 "
+                          f"graph of the same generator: {g16.nE} edges, max K {k16}, "
+                          f"{sec:.1f} s"}
     # one 1M-edge uniform insert + erase on the same graph
     rng = np.random.default_rng(77)
     b = 1_000_000
@@ -490,6 +522,14 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
     also["update_1M"] = {"metric": "update edges/s", "insert": round(b / ti, 1),
                          "erase": round(b / te, 1), "unit": "edges/s",
                          "note": "one 1M uniform batch on the scale-22 graph; see --workload update"}
+    if cpu:
+        sbi, sbe, _, _ = O.time_update(g_host, bs.cpu().numpy(), bd.cpu().numpy())
+        also["update_1M"]["cpu_baseline"] = {
+            "value": round(2 * b / (sbi + sbe), 1), "unit": "edges/s", "cores": 1,
+            "kind": "port", "insert": round(b / sbi, 1), "erase": round(b / sbe, 1),
+            "sample": "restated multiset update model (BatchUpdate.i.cuh:485-524; the "
+                      "reference has no CPU dynamic graph): the same 1M batch inserted then "
+                      f"erased on the same graph, {sbi:.2f} s + {sbe:.2f} s"}
     return also
 
 
@@ -871,14 +911,17 @@ def bench_serve(args, H, dev, rank, world):
 
 
 def run_reference(args):
+    """The reference's own CPU BFS (graph::BFS, xlib/src/Graph/BFS.cpp,
+    compiled from the reference sources into oracle/_ref/ref_driver) on the
+    same graph and sources.  The graph comes from the oracle's restatement
+    of the input generator, so this arm loads nothing of hornet_b200."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     from oracle import oracle as O
-    import hornet_b200 as H
     scale = args.scale or 22
     n = 1 << scale
-    s, d = H.gen_rmat_host(scale, 16 * n, 1)   # host generator: no device use
+    s, d = O.gen_rmat(scale, 16 * n, 1)
     g = O.build_csr_undirected(n, s, d)
     del s, d
     deg = np.diff(g.off)
@@ -901,9 +944,7 @@ def run_reference(args):
         "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(sec * 1e3 / K, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic R-MAT (seeded), no dataset",
-        "config": {"workload": f"static analytics: R-MAT scale {scale}, edge factor 16, "
-                               f"a=.57 b=.19 c=.19, BFS TopDown from 64 seeded non-isolated sources",
-                   "nV": g.nV, "nE": g.nE},
+        "config": static_config(scale, g.nV, g.nE, world),
         "cpu_baseline": {"value": round(value, 5), "unit": "GTEPS", "cores": used,
                          "kind": "reference",
                          "sample": f"graph::BFS (xlib/src/Graph/BFS.cpp), {per_step} source per "

@@ -104,6 +104,9 @@ _SIGNATURES = {
     "hn_bfs_multi": [_P, _P, _I32, _P, _INT, _P],
     "hn_bfs_do": [_P, _P, _I32, _P, _INT, _P],
     "hn_bfs_level_trace": [_P, _I32, _P, _P, _P],
+    "hn_bfs_validate": [_P, _I32, _P, _INT, _P],
+    "hn_cc_validate": [_P, _P, _INT, _P],
+    "hn_ktruss_validate": [_P, _I32, _P, _INT, _P],
     "hn_bfs_batch": [_P, _P, _P, _I32, _I32, _P, _INT, _P],
     "hn_tc": [_P, _P, _INT, _P],
     "hn_tc_local": [_P, _P, _I32, _P, _INT],
@@ -396,6 +399,21 @@ class Hornet:
         _check(lib().hn_graph_degrees(self._h, d.ctypes.data_as(_P), HN_MEM_HOST))
         return d
 
+    def save_bin(self, path: str) -> None:
+        """getCSR + GraphStd::writeBinary (hn_graph_write_bin): the graph's
+        current adjacency in the reference's .bin format."""
+        _check(lib().hn_graph_write_bin(self._h, path.encode()))
+
+    @staticmethod
+    def load_bin(path: str, device: int = 0) -> "Hornet":
+        """GraphStd::readBinary + HornetInit (hn_graph_read_bin): a device
+        graph from a .bin file (the fast reload of a saved graph)."""
+        h = Hornet.__new__(Hornet)
+        h._h = ctypes.c_void_p()
+        h._device = device
+        _check(lib().hn_graph_read_bin(path.encode(), device, ctypes.byref(h._h)))
+        return h
+
     def adjacency_hash(self) -> int:
         """Order-independent checksum of the edge multiset (computed on the
         device; hn_graph_adjacency_hash)."""
@@ -497,13 +515,24 @@ class StaticAlgorithm:
         pass
 
     def validate(self) -> bool:
+        """Certify the last result on the device (the reference's validate()
+        methods are stubs returning true, TopDown.cu:113-128,
+        CC.cu:163-203)."""
         raise NotImplementedError
+
+
+def _violations(fn, *args) -> int:
+    v = ctypes.c_int64(-1)
+    _check(fn(*args, ctypes.byref(v)))
+    return v.value
 
 
 class BfsTopDown(StaticAlgorithm):
     """hornetsnest BfsTopDown (TopDown.cuh:52-70): set_parameters(src), run().
-    validate() checks against the CPU oracle when it is importable (the
-    reference's own validate() is a stub returning true, TopDown.cu:113-128)."""
+    validate() certifies the last run's distances on the device
+    (hn_bfs_validate: source at 0, no edge skips a level, every reached
+    vertex has a parent one level closer); the reference's own validate()
+    is a stub returning true (TopDown.cu:113-128)."""
 
     def __init__(self, hornet: Hornet):
         super().__init__(hornet)
@@ -524,7 +553,15 @@ class BfsTopDown(StaticAlgorithm):
         p, mem = _out_ptr(out)
         _check(lib().hn_bfs(self.hornet.handle, self.source, p, mem, ctypes.byref(self.stats)))
         self.distances = out
+        self.distances_source = self.source
         return out
+
+    def validate(self) -> bool:
+        if self.distances is None:
+            return False
+        p, mem = _out_ptr(self.distances)
+        return _violations(lib().hn_bfs_validate, self.hornet.handle, self.distances_source, p,
+                           mem) == 0
 
     def run_multi(self, sources, out=None, direction_optimizing: bool = False):
         srcs = np.ascontiguousarray(sources, np.int32)
@@ -616,6 +653,22 @@ class TriangleCounting2(StaticAlgorithm):
     def countTriangles(self) -> int:
         return self._total
 
+    def validate(self) -> bool:
+        """The total against two other kernels: the owner counts (each
+        triangle credited once) sum to it, and the per-vertex counts (every
+        triangle credited to its three vertices) sum to three times it."""
+        total = ctypes.c_uint64()
+        owner = np.empty(max(1, self.hornet.nV()), np.uint64)
+        _check(lib().hn_tc_owner(self.hornet.handle, owner.ctypes.data_as(_P), HN_MEM_HOST,
+                                 ctypes.byref(total)))
+        pv = self._per_vertex
+        if pv is None:
+            pv = np.empty(self.hornet.nV(), np.uint64)
+            t2 = ctypes.c_uint64()
+            _check(lib().hn_tc(self.hornet.handle, pv.ctypes.data_as(_P), HN_MEM_HOST,
+                               ctypes.byref(t2)))
+        return total.value == self._total and int(pv.sum(dtype=np.uint64)) == 3 * self._total
+
     def local(self, seeds, out=None):
         """Triangles containing each seed vertex (hn_tc_local).  seeds: host
         int array, or a device int32 tensor (then `out`, a device int64
@@ -664,6 +717,13 @@ class CC(StaticAlgorithm):
     def reference_colors(self):
         return self.run(HN_CC_REFERENCE)
 
+    def validate(self) -> bool:
+        """Certify the last minimum-id labels on the device (hn_cc_validate)."""
+        if self.labels is None:
+            return False
+        p, mem = _out_ptr(self.labels)
+        return _violations(lib().hn_cc_validate, self.hornet.handle, p, mem) == 0
+
 
 class KTruss(StaticAlgorithm):
     """hornetsnest KTruss (KTruss.cuh:43-78): run(), getMaxK(); edge_truss
@@ -692,6 +752,15 @@ class KTruss(StaticAlgorithm):
 
     def getMaxK(self) -> int:
         return self.max_k
+
+    def validate(self) -> bool:
+        """Certify the last edge truss numbers on the device
+        (hn_ktruss_validate: the edges numbered >= t form a t-truss)."""
+        if self.edge_truss is None:
+            return False
+        et = np.ascontiguousarray(self.edge_truss, np.int32)
+        return _violations(lib().hn_ktruss_validate, self.hornet.handle, self.max_k,
+                           et.ctypes.data_as(_P), HN_MEM_HOST) == 0
 
     def runForK(self, K: int):
         """KTruss::runForK (KTruss.cu:114-119) + copyOffsetArrayHost: the

@@ -352,6 +352,30 @@ int hn_ktruss(hn_graph_t* g, int32_t* max_k, int32_t* edge_truss, int mem);
  * *removed (may be NULL) the directed edges erased. */
 int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t* removed);
 
+/* ---- result certificates (StaticAlgorithm::validate) --------------------
+ * The reference's validate() methods return true without checking
+ * (hornetsnest/src/Static/BreadthFirstSearch/TopDown.cu:113-128,
+ * ConnectedComponents/CC.cu:163-203).  These check a result on the device
+ * without recomputing it; *violations = number of failed conditions (0:
+ * the result is certified).  Arrays are in `mem`.
+ * hn_bfs_validate: dist (int32[nV]) are the BFS distances from src iff
+ *   dist[src] == 0, no edge from a reached vertex leads to an unreached one
+ *   or skips a level, and every other reached vertex has an in-edge from
+ *   the level before.
+ * hn_cc_validate: min-id labels (int32[nV]) of an undirected graph:
+ *   constant along edges, labels[v] <= v, labels[labels[v]] == labels[v],
+ *   and propagating the roots' labels along edges reproduces them.
+ * hn_ktruss_validate: edge truss numbers (int32[nE], sorted-COO order) of a
+ *   simple undirected graph: in [2, max_k] with max_k attained, equal on
+ *   both directions, and every edge numbered t >= 3 in >= t-2 triangles
+ *   whose other edges are numbered >= t (the edges numbered >= t form a
+ *   t-truss; maximality is not checked). */
+int hn_bfs_validate(hn_graph_t* g, int32_t src, const int32_t* dist, int mem,
+                    int64_t* violations);
+int hn_cc_validate(hn_graph_t* g, const int32_t* labels, int mem, int64_t* violations);
+int hn_ktruss_validate(hn_graph_t* g, int32_t max_k, const int32_t* edge_truss, int mem,
+                       int64_t* violations);
+
 /* ---- operator primitives with built-in operators -----------------------
  * forAllEdges(hornet, vertex_array, size, op, lb) with the BinarySearch or
  * VertexBased<vw> load balancer (primitives/Operator++.cuh:143-215,

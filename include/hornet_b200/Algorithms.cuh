@@ -4,9 +4,10 @@
 //   TriangleCounting2 (Static/TriangleCounting/triangle2.cuh:18-37)
 //   CC                (Static/ConnectedComponents/CC.cuh:53-69)
 //   KTruss            (Static/KTruss/KTruss.cuh:12-92)
-// validate() compares against nothing on the host (the reference's BFS and
-// CC validators are stubs that return true, TopDown.cu:113-128,
-// CC.cu:163-203); the parity suite checks results against the CPU oracle.
+// validate() certifies the last result on the device through the C ABI
+// (hn_bfs_validate, hn_cc_validate, hn_ktruss_validate; TC against its two
+// other counting kernels), where the reference's BFS and CC validators are
+// stubs that return true (TopDown.cu:113-128, CC.cu:163-203).
 #pragma once
 
 #include <cstdint>
@@ -42,7 +43,13 @@ public:
         if (d_distances) cudaFree(d_distances);
         d_distances = nullptr;
     }
-    bool validate() override { return true; }
+    bool validate() override {
+        int64_t bad = -1;
+        return _levels > 0 &&
+               hn_bfs_validate(hornet.handle(), bfs_source, d_distances, HN_MEM_DEVICE, &bad) ==
+                   HN_OK &&
+               bad == 0;
+    }
     dist_t getLevels() const { return _levels; }
     const dist_t* distances() const { return d_distances; }  // device
 
@@ -76,7 +83,17 @@ public:
         if (triPerVertex) cudaFree(triPerVertex);
         triPerVertex = nullptr;
     }
-    bool validate() override { return true; }
+    // the total against the owner counts (each triangle credited once) and
+    // the per-vertex counts (three credits per triangle)
+    bool validate() override {
+        uint64_t owner = 0, t = 0;
+        std::vector<uint64_t> pv((size_t)(hornet.nV() > 0 ? hornet.nV() : 1));
+        if (hn_tc_owner(hornet.handle(), pv.data(), HN_MEM_HOST, &owner) != HN_OK) return false;
+        if (hn_tc(hornet.handle(), pv.data(), HN_MEM_HOST, &t) != HN_OK) return false;
+        uint64_t sum = 0;
+        for (int32_t v = 0; v < hornet.nV(); v++) sum += pv[(size_t)v];
+        return owner == _total && t == _total && sum == 3 * _total;
+    }
 
 private:
     triangle_t* triPerVertex = nullptr;
@@ -103,7 +120,21 @@ public:
         if (d_colors) cudaFree(d_colors);
         d_colors = nullptr;
     }
-    bool validate() override { return true; }
+    // certifies minimum-id labels (run_min_label); the reference colouring
+    // of run() is certified through the min-id labels of the same graph
+    bool validate() override {
+        color_t* lab = nullptr;
+        if (cudaMalloc(&lab, sizeof(color_t) * (size_t)(hornet.nV() > 0 ? hornet.nV() : 1)) !=
+            cudaSuccess)
+            return false;
+        int64_t bad = -1;
+        int32_t n = 0;
+        bool ok = hn_cc(hornet.handle(), HN_CC_MIN_ID, lab, HN_MEM_DEVICE, &n) == HN_OK &&
+                  hn_cc_validate(hornet.handle(), lab, HN_MEM_DEVICE, &bad) == HN_OK &&
+                  bad == 0 && n == _ncomp;
+        cudaFree(lab);
+        return ok;
+    }
     const color_t* colors() const { return d_colors; }  // device
     int32_t components() const { return _ncomp; }
 
@@ -154,7 +185,13 @@ public:
         ::hornet::hn_check(hn_ktruss_keep(hornet.handle(), max_K, &_maxK, &removed));
     }
     void release() override {}
-    bool validate() override { return true; }
+    bool validate() override {
+        int64_t bad = -1;
+        return hn_ktruss_validate(hornet.handle(), _maxK,
+                                  _edge_truss.empty() ? nullptr : _edge_truss.data(),
+                                  HN_MEM_HOST, &bad) == HN_OK &&
+               bad == 0;
+    }
 
 private:
     int32_t _maxK = 0;

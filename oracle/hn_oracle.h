@@ -70,6 +70,12 @@ int64_t hno_bfs(int32_t nV, const int64_t* off, const int32_t* adj, int32_t src,
 uint64_t hno_tc_oriented(int32_t nV, const int64_t* off, const int32_t* adj,
                          uint64_t* per_vertex);
 
+/* hno_tc_oriented over the oriented edges first, first + stride, ... (CSR
+ * order) only: a uniform edge sample for a bounded CPU timing; *edges = the
+ * number of sampled edges. */
+uint64_t hno_tc_oriented_sample(int32_t nV, const int64_t* off, const int32_t* adj,
+                                int32_t first, int32_t stride, int64_t* edges);
+
 /* Connected components of an undirected graph labelled by the minimum vertex
  * id of each component (xlib/src/Graph/WCC.cpp:54-98 relabelled).  Returns
  * the number of components. */

@@ -54,6 +54,8 @@ def lib() -> ctypes.CDLL:
         l.hno_cc_reference_colors.restype = None
         l.hno_ktruss.argtypes = [I32, _P, _P, _P]
         l.hno_ktruss.restype = I32
+        l.hno_tc_oriented_sample.argtypes = [I32, _P, _P, I32, I32, _P]
+        l.hno_tc_oriented_sample.restype = ctypes.c_uint64
         l.hno_ktruss_peel.argtypes = [I32, _P, _P, _P]
         l.hno_ktruss_peel.restype = I32
         l.hno_gen_rmat.argtypes = [I32, I32, I64, ctypes.c_double, ctypes.c_double,
@@ -166,6 +168,18 @@ def tc(g: Csr, per_vertex: bool = False):
     return (int(t), pv) if per_vertex else int(t)
 
 
+def time_tc_sample(g: Csr, stride: int, first: int = 0) -> Tuple[float, int]:
+    """Seconds of the restated hostCountTriangles over a uniform sample of
+    the degree-oriented graph's edges (every stride-th in CSR order), and
+    the number of sampled edges.  The orientation is not timed."""
+    import time
+    o = orient_by_degree(g)
+    e = ctypes.c_int64()
+    t0 = time.perf_counter()
+    lib().hno_tc_oriented_sample(o.nV, _p(o.off), _p(o.adj), first, stride, ctypes.byref(e))
+    return time.perf_counter() - t0, int(e.value)
+
+
 def cc_min_label(g: Csr) -> Tuple[np.ndarray, int]:
     lab = np.empty(g.nV, np.int32)
     n = lib().hno_cc_min_label(g.nV, _p(g.off), _p(g.adj), _p(lab))
@@ -237,6 +251,29 @@ def ref_wcc(g: Csr) -> np.ndarray:
         write_csr(cp, g)
         subprocess.run([REF_DRIVER, "wcc", cp, op], check=True, stdout=subprocess.DEVNULL)
         return np.fromfile(op, np.int32)
+
+
+def ref_time_wcc(g: Csr) -> Tuple[float, int]:
+    """Seconds spent in graph::WCC::run (reference host code) and the
+    component count."""
+    with tempfile.TemporaryDirectory() as d:
+        cp, op = os.path.join(d, "g.csr"), os.path.join(d, "o.bin")
+        write_csr(cp, g)
+        out = subprocess.run([REF_DRIVER, "wcc", cp, op], check=True, capture_output=True,
+                             text=True).stdout.split()
+        return float(out[0]), int(out[1])
+
+
+def time_update(g: Csr, bsrc, bdst) -> Tuple[float, float, int, int]:
+    """Seconds of the restated insert (both dedup flags) and of the erase
+    (removeBatchDuplicates) of one batch on g, and the edges each applied."""
+    import time
+    t0 = time.perf_counter()
+    g2, a = insert(g, bsrc, bdst, 3)
+    t1 = time.perf_counter()
+    _, r = erase(g2, bsrc, bdst, 1)
+    t2 = time.perf_counter()
+    return t1 - t0, t2 - t1, a, r
 
 
 def ref_time_bfs(g: Csr, sources) -> Tuple[float, int]:

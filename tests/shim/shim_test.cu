@@ -149,6 +149,7 @@ int main(int argc, char** argv) {
         KTruss kt(kg);
         kt.init();
         kt.run();
+        std::printf("ktruss_validate %s\n", kt.validate() ? "PASSED" : "NOT PASSED");
         long long at_least3 = 0;
         for (int t : kt.edgeTruss()) at_least3 += t >= 3;
         const int maxk = kt.getMaxK();
@@ -159,6 +160,20 @@ int main(int argc, char** argv) {
         kt.runForKDynamic(3);
         const bool ok = off_ok && (long long)kg.nE() == at_least3 && kt.getMaxK() == maxk;
         std::printf("ktruss_max %d\nktruss_keep %s\n", maxk, ok ? "PASSED" : "NOT PASSED");
+    }
+    // validate() of each algorithm on the (symmetric) input graph
+    {
+        HornetGPU vg(init);
+        BfsTopDown b2(vg);
+        b2.set_parameters(0);
+        b2.run();
+        CC c2(vg);
+        c2.run();
+        TriangleCounting2 t2(vg);
+        t2.init();
+        t2.run();
+        const bool ok = b2.validate() && c2.validate() && t2.validate();
+        std::printf("validate %s\n", ok ? "PASSED" : "NOT PASSED");
     }
     cudaFree(d_dist);
     cudaFree(d_cnt);

@@ -597,3 +597,76 @@ def test_pool_grows_in_place_under_many_inserts():
     # their batch's weight
     np.testing.assert_array_equal(np.sort(w[w < (1 << 30)]), np.arange(g.nE, dtype=np.uint32))
     assert set(np.unique(w[w >= (1 << 30)]).tolist()) == {1 << 30, (1 << 30) + 1, (1 << 30) + 2}
+
+
+def test_validate_certifies_results_and_catches_errors():
+    """validate() (device certificates; the reference's are stubs returning
+    true) accepts the computed BFS, CC, TC and k-truss results and rejects
+    results with one error planted on the host."""
+    g = GRAPHS["rmat10"]()
+    h = build(g)
+    bfs = H.BfsTopDown(h)
+    bfs.set_parameters(3)
+    dist = bfs.run()
+    assert bfs.validate()
+    reached = np.nonzero((dist != O.INF) & (dist > 1))[0]
+    wrong = dist.copy()
+    wrong[reached[0]] += 1                       # a vertex one level too far
+    bfs.distances = wrong
+    assert not bfs.validate()
+    wrong = dist.copy()
+    wrong[reached[1]] = O.INF                    # a reached vertex dropped
+    bfs.distances = wrong
+    assert not bfs.validate()
+    cc = H.CC(h)
+    lab = cc.run()
+    assert cc.validate()
+    comps = np.unique(lab)
+    if len(comps) >= 2:
+        merged = lab.copy()
+        merged[merged == comps[1]] = comps[0]    # two components under one label
+        cc.labels = merged
+        assert not cc.validate()
+    tc = H.TriangleCounting2(h)
+    tc.run()
+    assert tc.validate()
+    tc._total += 1
+    assert not tc.validate()
+    kt = H.KTruss(build(T.rmat_graph(8, 16, seed=2)))
+    kt.run()
+    assert kt.validate()
+    et = kt.edge_truss.copy()
+    top = np.nonzero(et == kt.max_k)[0]
+    kt.edge_truss = et.copy()
+    kt.edge_truss[top[0]] = 2                    # one direction of an edge changed
+    assert not kt.validate()
+
+
+def test_device_graph_save_and_reload(tmp_path):
+    """A device graph saved after updates (hn_graph_write_bin, the
+    reference's GraphStd .bin format) reloads into an identical graph
+    (hn_graph_read_bin), and the file is byte-identical to the host writer's
+    output for the exported CSR (pinned to the reference's example/G.bin by
+    the CPU format tests)."""
+    g = T.rmat_graph(10, 8, seed=21)
+    h = build(g)
+    rng = np.random.default_rng(2)
+    bs = rng.integers(0, g.nV, 3000).astype(np.int32)
+    bd = rng.integers(0, g.nV, 3000).astype(np.int32)
+    h.insert(H.BatchUpdate(h, bs, bd), True, True)
+    p = str(tmp_path / "g.bin")
+    h.save_bin(p)
+    h2 = H.Hornet.load_bin(p)
+    assert h2.nV() == h.nV() and h2.nE() == h.nE()
+    s1, d1 = h.getCOO(True)
+    s2, d2 = h2.getCOO(True)
+    np.testing.assert_array_equal(s1, s2)
+    np.testing.assert_array_equal(d1, d2)
+    assert h2.adjacency_hash() == h.adjacency_hash()
+    off, adj = h.getCSR()
+    q = str(tmp_path / "host.bin")
+    H.write_bin(q, off.astype(np.int32), adj)
+    assert open(p, "rb").read() == open(q, "rb").read()
+    # the reloaded graph is a full dynamic graph: it takes further updates
+    assert h2.erase(H.BatchUpdate(h2, bs, bd), True) == h.erase(H.BatchUpdate(h, bs, bd), True)
+    assert h2.adjacency_hash() == h.adjacency_hash()

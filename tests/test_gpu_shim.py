@@ -45,4 +45,6 @@ def test_shim_reference_style_program():
         ncomp = int(r.stdout.split("cc_components")[1].split()[0])
         assert ncomp == O.cc_min_label(g)[1]
         assert "ktruss_keep PASSED" in r.stdout
+        assert "ktruss_validate PASSED" in r.stdout
+        assert "validate PASSED" in r.stdout
         assert int(r.stdout.split("ktruss_max")[1].split()[0]) == O.ktruss(g)[0]
