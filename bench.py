@@ -870,18 +870,23 @@ def bench_serve(args, H, dev, rank, world):
                 if r.kind in S.QUERY_KINDS]
         row = {"rate_rps": rate if rate > 0 else "saturation"}
         res = {}
-        for mode in ("per_request", "per_request_do", "batched"):
+        for mode in args.serve_modes.split(","):
             h = H.hornet_from_device_arrays(nV, nE, off_d, adj_d, device=dev)
             srv = S.Server(h, batched=mode == "batched",
                            single_bfs="do" if mode != "per_request" else "td",
-                           msbfs_min=args.msbfs_min)
+                           msbfs_min=args.msbfs_min, workers=args.serve_workers)
             srv.run(warm)                       # CUDA graphs built, read-only
-            srv.calls, srv.split_for_memory = 0, 0
+            srv.calls, srv.split_for_memory, srv.max_inflight = 0, 0, 0
             srv.groups = {k: 0 for k in srv.groups}
             srv.service_s = {k: 0.0 for k in srv.service_s}
             rep = srv.run(reqs)
             res[mode] = rep.results
             row[mode] = rep.summary()
+            row[mode]["workers"] = rep.workers
+            row[mode]["max_queries_in_flight"] = rep.max_inflight
+            row[mode]["update_calls_ms"] = rep.update_calls_ms
+            row[mode]["update_parts_ms"] = rep.update_parts_ms
+            srv.close()
             del srv, h
             gc.collect()
         same = S.same_results(res["per_request"], res["batched"]) and \
@@ -893,6 +898,8 @@ def bench_serve(args, H, dev, rank, world):
         row["throughput_x_vs_per_request_do"] = round(bt["throughput_rps"] / pd["throughput_rps"], 2)
         row["p99_ms"] = {m: row[m]["latency_ms"]["all"]["p99"]
                          for m in ("per_request", "per_request_do", "batched")}
+        row["p999_ms"] = {m: row[m]["latency_ms"]["all"]["p999"]
+                          for m in ("per_request", "per_request_do", "batched")}
         table.append(row)
     sat = [r for r in table if r["rate_rps"] == "saturation"]
     head = sat[0] if sat else table[-1]
@@ -966,6 +973,10 @@ def main():
     ap.add_argument("--requests", type=int, default=1000)
     ap.add_argument("--msbfs-min", type=int, default=4,
                     help="serve: smallest run of BFS queries answered by one batched traversal")
+    ap.add_argument("--serve-modes", default="per_request,per_request_do,batched",
+                    help="serve: the loops to run, in this order")
+    ap.add_argument("--serve-workers", type=int, default=4,
+                    help="serve: query views (worker threads) of the batched loop")
     ap.add_argument("--graphs", type=int, default=4096)
     ap.add_argument("--sample-graphs", type=int, default=128)
     ap.add_argument("--scale", type=int, default=0)

@@ -94,6 +94,9 @@ _SIGNATURES = {
     "hn_graph_device_view": [_P, _P],
     "hn_graph_memory": [_P, _P, _P, _P],
     "hn_graph_adjacency_hash": [_P, _P],
+    "hn_graph_view_create": [_P, _P, _P],
+    "hn_graph_view_refresh": [_P],
+    "hn_gather_int32": [_P, _P, _P, _I64, _P],
     "hn_batch_create": [_P, _I64, _P, _P, _INT, _P],
     "hn_batch_reset": [_P, _I64, _P, _P, _INT],
     "hn_batch_size": [_P, _P],
@@ -398,6 +401,30 @@ class Hornet:
         d = np.empty(self.nV(), np.int32)
         _check(lib().hn_graph_degrees(self._h, d.ctypes.data_as(_P), HN_MEM_HOST))
         return d
+
+    def view(self, stream=None) -> "Hornet":
+        """A query view (hn_graph_view_create): the same resident graph on its
+        own stream and scratch, for read-only calls that run concurrently
+        with those on other views.  Call refresh_view() on it after updating
+        this graph; destroy views before the graph."""
+        v = Hornet.__new__(Hornet)
+        v._h = ctypes.c_void_p()
+        v._device = self._device
+        v._parent = self
+        _check(lib().hn_graph_view_create(self._h, None if stream is None else
+                                          ctypes.c_void_p(stream), ctypes.byref(v._h)))
+        return v
+
+    def refresh_view(self) -> None:
+        _check(lib().hn_graph_view_refresh(self._h))
+
+    def gather(self, dev_ptr: int, idx) -> np.ndarray:
+        """src[idx] for a device int32 array at dev_ptr (hn_gather_int32)."""
+        ix = np.ascontiguousarray(idx, np.int64)
+        out = np.empty(len(ix), np.int32)
+        _check(lib().hn_gather_int32(self._h, ctypes.c_void_p(dev_ptr), ix.ctypes.data_as(_P),
+                                     len(ix), out.ctypes.data_as(_P)))
+        return out
 
     def save_bin(self, path: str) -> None:
         """getCSR + GraphStd::writeBinary (hn_graph_write_bin): the graph's

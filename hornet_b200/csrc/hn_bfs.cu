@@ -868,7 +868,9 @@ const char* level_kernel_name(int kernel, bool dir_opt) {
 
 void build_bfs_graph(hn_graph* g, BfsGraph& bg) {
     const int nV = g->nV;
-    const long long nchunk_cap = g->nE / kWChunk + 4;   // the finer of the two granularities
+    // the finer of the two granularities, with room for the graph to grow
+    // by a quarter before the table (and the CUDA graph) is rebuilt
+    const long long nchunk_cap = (g->nE + g->nE / 4) / kWChunk + 1024;
     HN_CUDA(cudaMalloc((void**)&bg.state, sizeof(BfsState)));
     HN_CUDA(cudaMallocHost((void**)&bg.h_state, sizeof(BfsState)));
     HN_CUDA(cudaMalloc((void**)&bg.qbuf, sizeof(int32_t) * 2 * ((size_t)nV + 1)));

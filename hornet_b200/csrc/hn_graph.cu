@@ -689,6 +689,14 @@ void free_graph_object(hn_graph* g) {
     g->bfs = nullptr;
     free_ms_graph(g->ms);
     g->ms = nullptr;
+    if (g->parent) {
+        // a view borrows the parent's vertex table and pool
+        g->vtab = nullptr;
+        g->pool = nullptr;
+        g->wpool = nullptr;
+        g->vm_pool = nullptr;
+        g->vm_wpool = nullptr;
+    }
     if (g->vtab) cudaFreeAsync(g->vtab, g->stream);
     release_pool(g);
     if (g->stream) cudaStreamSynchronize(g->stream);
@@ -777,6 +785,19 @@ int create_impl(int32_t nV, int64_t nE, const OffT* off, const int32_t* adj, uns
 }
 
 }  // namespace
+
+// The parent's current shape, copied into a view (host fields only).
+static void view_copy(hn_graph* v) {
+    const hn_graph* p = v->parent;
+    v->nV = p->nV;
+    v->nE = p->nE;
+    v->key_bits = p->key_bits;
+    v->vtab = p->vtab;
+    v->pool = p->pool;
+    v->pool_cap = p->pool_cap;
+    v->weighted = p->weighted;
+    v->wpool = p->wpool;
+}
 
 extern "C" {
 
@@ -886,12 +907,46 @@ int hn_graph_reset_csr(hn_graph_t* g, int32_t nV, int64_t nE, const int32_t* off
     HN_REQUIRE(nV >= 0 && nE >= 0 && off != nullptr && (nE == 0 || adj != nullptr),
                "bad CSR");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    require_owner(g);
     HN_CUDA(cudaSetDevice(g->device));
     DevBuf<long long> d_off;
     DevBuf<int32_t> d_adj_own;
     const int32_t* d_adj = nullptr;
     stage_csr(g, nV, nE, off, adj, mem, d_off, d_adj_own, d_adj);
     build_from_csr(g, nV, nE, d_off.get(), d_adj, (flags & HN_CSR_SORTED) != 0);
+    HN_API_END
+}
+
+int hn_graph_view_create(hn_graph_t* parent, void* stream, hn_graph_t** out) {
+    HN_API_BEGIN
+    HN_REQUIRE(parent && out, "null argument");
+    HN_REQUIRE(!parent->parent, "a view of a view: create it from the graph itself");
+    *out = nullptr;
+    hn_graph* v = new hn_graph();
+    try {
+        init_graph_object(v, parent->device);
+        v->parent = parent;
+        view_copy(v);
+        if (stream) {
+            HN_CUDA(cudaStreamDestroy(v->stream));
+            v->stream = (cudaStream_t)stream;
+            v->own_stream = false;
+        }
+    } catch (...) {
+        free_graph_object(v);
+        throw;
+    }
+    *out = v;
+    HN_API_END
+}
+
+int hn_graph_view_refresh(hn_graph_t* view) {
+    HN_API_BEGIN
+    HN_REQUIRE(view && view->parent, "not a query view");
+    HN_CUDA(cudaSetDevice(view->device));
+    // the parent's pending work (an update) finishes before the view reads
+    HN_CUDA(cudaStreamSynchronize(view->parent->stream));
+    view_copy(view);
     HN_API_END
 }
 

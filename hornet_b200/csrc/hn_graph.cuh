@@ -208,7 +208,18 @@ struct hn_graph {
     hn::Persist scratch[8];               // reusable device scratch
     hn::BfsGraph* bfs = nullptr;          // instantiated BFS CUDA graph
     hn::MsGraph* ms = nullptr;            // instantiated batched-BFS CUDA graph
+
+    // a query view (hn_graph_view_create): shares the parent's vertex table
+    // and edge pool read-only, owns its stream and scratch
+    hn_graph* parent = nullptr;
 };
+
+namespace hn {
+// Update entry points call this: a query view never changes the graph.
+inline void require_owner(const hn_graph* g) {
+    if (g->parent) throw Error(HN_ERR_STATE, "a query view cannot update the graph");
+}
+}  // namespace hn
 
 struct hn_batch {
     hn_graph* g = nullptr;

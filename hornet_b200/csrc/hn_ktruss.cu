@@ -458,6 +458,7 @@ extern "C" int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t*
     HN_API_BEGIN
     HN_REQUIRE(g != nullptr, "graph is null");
     HN_REQUIRE(K >= 2, "K must be at least 2");
+    require_owner(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     if (removed) *removed = 0;

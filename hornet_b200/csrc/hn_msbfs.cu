@@ -414,7 +414,8 @@ __global__ void __launch_bounds__(BLOCK) k_ms_apply(MsState* st, cudaGraphCondit
 
 void build_ms_graph(hn_graph* g, MsGraph& mg) {
     const int nV = g->nV;
-    const long long nchunk_cap = g->nE / kMsChunk + 4;
+    // room for the graph to grow by a quarter before a rebuild
+    const long long nchunk_cap = (g->nE + g->nE / 4) / kMsChunk + 1024;
     HN_CUDA(cudaMalloc((void**)&mg.state, sizeof(MsState)));
     HN_CUDA(cudaMallocHost((void**)&mg.h_state, sizeof(MsState)));
     HN_CUDA(cudaMalloc((void**)&mg.qbuf, sizeof(int32_t) * 2 * ((size_t)nV + 1)));

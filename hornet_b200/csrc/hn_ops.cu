@@ -46,6 +46,13 @@ __global__ void k_adjacency_hash(const VRec* __restrict__ vtab, const int32_t* _
     if (lane == 0 && h) atomicAdd(out, h);
 }
 
+__global__ void k_gather_i32(const int32_t* __restrict__ src, const long long* __restrict__ idx,
+                             long long n, int32_t* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = src[idx[i]];
+}
+
 hornet::HornetDevice view_of(hn_graph* g) {
     hn_device_view_t v;
     v.nV = g->nV;
@@ -119,5 +126,22 @@ extern "C" int hn_graph_adjacency_hash(hn_graph_t* g, uint64_t* hash) {
     HN_CUDA(cudaMemcpyAsync(&h, acc.get(), sizeof(h), cudaMemcpyDeviceToHost, g->stream));
     HN_CUDA(cudaStreamSynchronize(g->stream));
     *hash = h;
+    HN_API_END
+}
+
+extern "C" int hn_gather_int32(hn_graph_t* g, const int32_t* src, const int64_t* idx, int64_t n,
+                               int32_t* out) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && src && (idx || n == 0) && (out || n == 0) && n >= 0, "null argument");
+    if (n == 0) return HN_OK;
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    DevBuf<long long> d_idx((size_t)n, s);
+    DevBuf<int32_t> d_out((size_t)n, s);
+    HN_CUDA(cudaMemcpyAsync(d_idx.get(), idx, sizeof(long long) * n, cudaMemcpyHostToDevice, s));
+    HN_LAUNCH(k_gather_i32, grid_for(g, n, 256), 256, 0, s, src, (const long long*)d_idx.get(),
+              (long long)n, d_out.get());
+    HN_CUDA(cudaMemcpyAsync(out, d_out.get(), sizeof(int32_t) * n, cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaStreamSynchronize(s));
     HN_API_END
 }

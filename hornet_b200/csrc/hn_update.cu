@@ -820,20 +820,22 @@ int hn_batch_reset_w(hn_batch_t* b, int64_t n, const int32_t* src, const int32_t
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     hn_graph* g = b->g;
     HN_CUDA(cudaSetDevice(g->device));
+    // stream-ordered from the device's memory pool: a batch per request
+    // costs no device-wide synchronisation (cudaMalloc / cudaFree would)
     if ((size_t)n > b->cap) {
-        if (b->src) HN_CUDA(cudaFree(b->src));
-        if (b->dst) HN_CUDA(cudaFree(b->dst));
+        if (b->src) HN_CUDA(cudaFreeAsync(b->src, g->stream));
+        if (b->dst) HN_CUDA(cudaFreeAsync(b->dst, g->stream));
         b->src = b->dst = nullptr;
         b->cap = 0;
-        HN_CUDA(cudaMalloc((void**)&b->src, sizeof(int32_t) * (size_t)n));
-        HN_CUDA(cudaMalloc((void**)&b->dst, sizeof(int32_t) * (size_t)n));
+        HN_CUDA(cudaMallocAsync((void**)&b->src, sizeof(int32_t) * (size_t)n, g->stream));
+        HN_CUDA(cudaMallocAsync((void**)&b->dst, sizeof(int32_t) * (size_t)n, g->stream));
         b->cap = (size_t)n;
     }
     if (weights && (size_t)n > b->wcap) {
-        if (b->w) HN_CUDA(cudaFree(b->w));
+        if (b->w) HN_CUDA(cudaFreeAsync(b->w, g->stream));
         b->w = nullptr;
         b->wcap = 0;
-        HN_CUDA(cudaMalloc((void**)&b->w, sizeof(uint32_t) * (size_t)n));
+        HN_CUDA(cudaMallocAsync((void**)&b->w, sizeof(uint32_t) * (size_t)n, g->stream));
         b->wcap = (size_t)n;
     }
     b->n = n;
@@ -860,11 +862,13 @@ int hn_batch_destroy(hn_batch_t* b) {
     HN_API_BEGIN
     if (!b) return HN_OK;
     // the batch may outlive its graph (garbage-collection order), so only
-    // its own device id is used here
+    // its own device id is used here.  Every call that read the buffers has
+    // returned (calls are synchronous), so they go back to the memory pool
+    // in the legacy stream's order, without a device-wide synchronisation.
     cudaSetDevice(b->device);
-    if (b->src) cudaFree(b->src);
-    if (b->dst) cudaFree(b->dst);
-    if (b->w) cudaFree(b->w);
+    if (b->src) cudaFreeAsync(b->src, 0);
+    if (b->dst) cudaFreeAsync(b->dst, 0);
+    if (b->w) cudaFreeAsync(b->w, 0);
     delete b;
     (void)cudaGetLastError();
     HN_API_END
@@ -875,6 +879,7 @@ int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
     HN_REQUIRE(g && b, "null argument");
     HN_REQUIRE(b->g == g, "batch belongs to another graph");
     HN_REQUIRE((flags & ~(HN_DEDUP_BATCH | HN_DEDUP_GRAPH)) == 0, "unknown flags");
+    require_owner(g);
     HN_CUDA(cudaSetDevice(g->device));
     run_update(g, b, flags, true, applied);
     HN_API_END
@@ -885,6 +890,7 @@ int hn_insert_count_triangles(hn_graph_t* g, hn_batch_t* b, int64_t* applied,
     HN_API_BEGIN
     HN_REQUIRE(g && b && new_triangles, "null argument");
     HN_REQUIRE(b->g == g, "batch belongs to another graph");
+    require_owner(g);
     HN_CUDA(cudaSetDevice(g->device));
     unsigned long long t = 0;
     run_update(g, b, HN_DEDUP_BATCH | HN_DEDUP_GRAPH, true, applied, &t);
@@ -897,6 +903,7 @@ int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
     HN_REQUIRE(g && b, "null argument");
     HN_REQUIRE(b->g == g, "batch belongs to another graph");
     HN_REQUIRE((flags & ~HN_DEDUP_BATCH) == 0, "unknown flags");
+    require_owner(g);
     HN_CUDA(cudaSetDevice(g->device));
     run_update(g, b, flags, false, applied);
     HN_API_END
@@ -909,6 +916,7 @@ int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int3
     HN_REQUIRE(n >= 0 && n <= 0x7FFFFFFF, "batch size must be in [0, 2^31)");
     HN_REQUIRE(n == 0 || (src && dst && ops), "null batch arrays");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    require_owner(g);
     if (inserted) *inserted = 0;
     if (erased) *erased = 0;
     if (n == 0) return HN_OK;

@@ -4,35 +4,44 @@ Requests are update batches (insert or erase), single-source BFS queries
 (distances to a few target vertices plus the number of vertices reached) and
 local triangle-count queries (triangles containing each vertex of a seed
 set).  The graph stays on the device for the whole run.  Two loops serve the
-same stream:
+same stream, and a query always sees exactly the updates that arrived
+before it (arrival-order semantics, as the reference's one-call-per-request
+use gives):
 
 * the plain per-request loop: one library call per request, in arrival
-  order (hn_insert / hn_erase, hn_bfs — or hn_bfs_do with single_bfs="do" —,
-  hn_tc_local);
-* the batched loop, which keeps arrival-order semantics — a query sees
-  exactly the updates that arrived before it — while
-  - coalescing a run of consecutive update batches into one
-    hn_update_coalesced call (the last operation on an edge decides it, which
-    on a simple graph is what applying the batches in order gives),
-  - answering a run of consecutive queries together: up to `max_slots` BFS
-    sources in one hn_bfs_batch traversal (one slot per request, so every
-    request gets its own single-source distances) when the run holds at
-    least `msbfs_min` of them, otherwise one direction-optimising traversal
-    per BFS (hn_bfs_do: the same distances, fewer edges read); all local-TC
-    seed sets in one hn_tc_local call,
-  - admitting a coalesced update only while its working memory fits in
-    the free device memory (less a reserve); a run that does not fit is split.
+  order, on one stream (hn_insert / hn_erase, hn_bfs -- or hn_bfs_do with
+  single_bfs="do" --, hn_tc_local);
+* the continuous-batching loop:
+  - queries run on query views (hn_graph_view_create: the same resident
+    graph, each view with its own stream and scratch), one per worker
+    thread, so queries overlap on the device.  A query that arrives while
+    others are on the GPU is admitted as soon as a view is free, whatever
+    the state of the ones already running;
+  - the queries of one epoch (between two updates) are grouped when they
+    can share work: at least `msbfs_min` waiting BFS queries go to one
+    batched traversal (hn_bfs_batch, one slot per request), waiting
+    local-TC queries to one hn_tc_local call; a BFS that waits alone runs
+    direction-optimising (hn_bfs_do: same distances, fewer edges read);
+  - an update is a fence: it starts when the queries of the previous epoch
+    have finished, and a run of consecutive waiting updates is coalesced
+    into one hn_update_coalesced call (the last operation on an edge decides
+    it, which on a simple graph is what applying the batches in order
+    gives), split where its working memory would not fit in the free device
+    memory (less a reserve); the views then take the graph's new shape
+    (hn_graph_view_refresh).
 
-Latency of a request = completion time of the call that answered it minus its
-arrival time, both on the host clock; the run reports p50/p99 per request
-kind and overall, and the throughput (requests / time of the last
+Latency of a request = completion time of the call that answered it minus
+its arrival time, on the host clock; the run reports p50/p99/p999 per
+request kind and overall, and the throughput (requests / time of the last
 completion).
 """
 from __future__ import annotations
 
 import ctypes
+import threading
 import time
 from collections import deque
+from concurrent.futures import FIRST_COMPLETED, ThreadPoolExecutor, wait
 from dataclasses import dataclass, field
 from typing import Dict, List, Optional
 
@@ -87,17 +96,30 @@ def _pct(a, q):
     return float(np.percentile(a, q)) if len(a) else float("nan")
 
 
+class _View:
+    """A query view with its own distance rows (device int32 [slots][nV])."""
+
+    def __init__(self, hornet: Hornet, slots: int):
+        import torch
+        self.g = hornet if slots == 0 else hornet.view()
+        self.rows = max(1, slots)
+        self.dist = torch.empty((self.rows, hornet.nV()), dtype=torch.int32,
+                                device=f"cuda:{hornet._device}")
+
+
 class Server:
     """Serves a request stream on `hornet` (kept resident).  `batched`
-    selects the batched loop; otherwise the plain per-request loop."""
+    selects the continuous-batching loop (query views on `workers` threads);
+    otherwise the plain per-request loop."""
 
     # device bytes per coalesced update entry: keys and sort buffers,
     # scan values, net sets, the update pipeline's own per-edge buffers
     UPDATE_BYTES_PER_EDGE = 96
 
-    def __init__(self, hornet: Hornet, batched: bool = True, max_slots: int = 64,
+    def __init__(self, hornet: Hornet, batched: bool = True, max_slots: int = 16,
                  max_update_edges: int = 1 << 24, reserve_bytes: int = 2 << 30,
-                 free_bytes_fn=None, single_bfs: str = "", msbfs_min: int = 4):
+                 free_bytes_fn=None, single_bfs: str = "", msbfs_min: int = 4,
+                 workers: int = 4):
         import torch
         self.h = hornet
         self.batched = batched
@@ -111,14 +133,34 @@ class Server:
         self.reserve = int(reserve_bytes)
         self.dev = hornet._device
         self.nV = hornet.nV()
-        self._free = free_bytes_fn or (lambda: torch.cuda.mem_get_info(self.dev)[0])
-        slots = self.max_slots if batched else 1
-        self.dist = torch.empty((slots, self.nV), dtype=torch.int32, device=f"cuda:{self.dev}")
-        self.dist_flat = self.dist.view(-1)
+        self._free_fn = free_bytes_fn or (lambda: torch.cuda.mem_get_info(self.dev)[0])
+        self._free_at, self._free_val = -1.0, 0
+        self.workers = max(1, int(workers)) if batched else 1
+        # the plain loop queries the graph itself; the batched loop one view
+        # per worker
+        self.views = [_View(hornet, self.max_slots if batched else 0)
+                      for _ in range(self.workers)]
         self.calls = 0
         self.split_for_memory = 0
         self.groups = {"update": 0, "bfs": 0, "tc_local": 0}
         self.service_s = {"update": 0.0, "bfs": 0.0, "tc_local": 0.0}
+        self.max_inflight = 0
+        self.update_call_s: List[float] = []     # device-synchronous update call times
+        self.update_parts_s = {"free_query": 0.0, "concat": 0.0, "call": 0.0, "refresh": 0.0}
+        self._lock = threading.Lock()
+
+    def _free(self) -> int:
+        """Free device bytes, queried at most every 0.25 s (the query takes
+        about a millisecond; the free memory moves only with pool growth)."""
+        now = time.perf_counter()
+        if now - self._free_at > 0.25:
+            self._free_val = self._free_fn()
+            self._free_at = now
+        return self._free_val
+
+    def close(self):
+        """Release the views (before the graph)."""
+        self.views = []
 
     # ---- library calls ---------------------------------------------------
     def _update_plain(self, r: Request):
@@ -129,21 +171,25 @@ class Server:
                                      d.ctypes.data_as(_P), HN_MEM_HOST, ctypes.byref(b)))
         try:
             n = ctypes.c_int64()
+            tc = time.perf_counter()
             if r.kind == "insert":
                 _check(lib().hn_insert(self.h.handle, b, HN_DEDUP_BATCH | HN_DEDUP_GRAPH,
                                        ctypes.byref(n)))
             else:
                 _check(lib().hn_erase(self.h.handle, b, HN_DEDUP_BATCH, ctypes.byref(n)))
+            self.update_call_s.append(time.perf_counter() - tc)
         finally:
             lib().hn_batch_destroy(b)
         self.calls += 1
-        return None
 
     def _update_group(self, group: List[Request]):
         """Coalesced updates, split where the working set would not fit."""
         start = 0
         while start < len(group):
-            budget = max(0, self._free() - self.reserve) // self.UPDATE_BYTES_PER_EDGE
+            tq = time.perf_counter()
+            free_b = self._free()
+            self.update_parts_s["free_query"] += time.perf_counter() - tq
+            budget = max(0, free_b - self.reserve) // self.UPDATE_BYTES_PER_EDGE
             budget = min(budget, self.max_update_edges)
             end, total = start, 0
             while end < len(group) and (end == start or total + group[end].n_edges <= budget):
@@ -152,86 +198,76 @@ class Server:
             if end < len(group):
                 self.split_for_memory += 1
             part = group[start:end]
+            tq = time.perf_counter()
             src = np.concatenate([r.src for r in part]).astype(np.int32, copy=False)
             dst = np.concatenate([r.dst for r in part]).astype(np.int32, copy=False)
             ops = np.concatenate([np.full(r.n_edges, 1 if r.kind == "insert" else 0, np.uint8)
                                   for r in part])
+            tc = time.perf_counter()
+            self.update_parts_s["concat"] += tc - tq
             self.h.update_coalesced(src, dst, ops)
+            self.update_call_s.append(time.perf_counter() - tc)
+            self.update_parts_s["call"] += time.perf_counter() - tc
             self.calls += 1
             self.groups["update"] += 1
             start = end
 
-    def _bfs_group(self, group: List[Request], results):
-        import torch
+    def _bfs_unit(self, v: _View, group: List[Request], results):
         k = len(group)
         srcs = np.array([r.source for r in group], np.int32)
         stats = (BfsStats * k)()
+        g = v.g.handle
+        base = v.dist.data_ptr()
         if k >= self.msbfs_min:
-            _check(lib().hn_bfs_batch(self.h.handle, srcs.ctypes.data_as(_P), None, k, k,
-                                      ctypes.c_void_p(self.dist.data_ptr()), HN_MEM_DEVICE,
-                                      stats))
-            self.calls += 1
+            _check(lib().hn_bfs_batch(g, srcs.ctypes.data_as(_P), None, k, k,
+                                      ctypes.c_void_p(base), HN_MEM_DEVICE, stats))
+            calls = 1
         else:
             for j in range(k):
-                row = ctypes.c_void_p(self.dist.data_ptr() + 4 * j * self.nV)
+                row = ctypes.c_void_p(base + 4 * j * self.nV)
                 if self.single_bfs == "do":
                     one = srcs[j:j + 1]
-                    _check(lib().hn_bfs_do(self.h.handle, one.ctypes.data_as(_P), 1, row,
-                                           HN_MEM_DEVICE, ctypes.byref(stats[j])))
+                    _check(lib().hn_bfs_do(g, one.ctypes.data_as(_P), 1, row, HN_MEM_DEVICE,
+                                           ctypes.byref(stats[j])))
                 else:
-                    _check(lib().hn_bfs(self.h.handle, int(srcs[j]), row, HN_MEM_DEVICE,
+                    _check(lib().hn_bfs(g, int(srcs[j]), row, HN_MEM_DEVICE,
                                         ctypes.byref(stats[j])))
-                self.calls += 1
-        self.groups["bfs"] += 1
+            calls = k
         idx = np.concatenate([j * self.nV + np.asarray(r.targets, np.int64)
                               for j, r in enumerate(group)])
-        got = torch.take(self.dist_flat, torch.from_numpy(idx).to(self.dist.device)).cpu().numpy()
+        got = v.g.gather(base, idx)
         at = 0
         for j, r in enumerate(group):
             n = len(r.targets)
             results[r.rid] = (got[at:at + n].copy(), int(stats[j].visited))
             at += n
+        return calls
 
-    def _tc_group(self, group: List[Request], results):
+    def _tc_unit(self, v: _View, group: List[Request], results):
         seeds = np.concatenate([np.asarray(r.seeds, np.int32) for r in group])
         out = np.empty(len(seeds), np.uint64)
-        _check(lib().hn_tc_local(self.h.handle, seeds.ctypes.data_as(_P), len(seeds),
+        _check(lib().hn_tc_local(v.g.handle, seeds.ctypes.data_as(_P), len(seeds),
                                  out.ctypes.data_as(_P), HN_MEM_HOST))
-        self.calls += 1
-        self.groups["tc_local"] += 1
         at = 0
         for r in group:
             results[r.rid] = out[at:at + len(r.seeds)].copy()
             at += len(r.seeds)
+        return 1
 
-    # ---- loop --------------------------------------------------------------
-    def _take(self, pending: deque) -> List[Request]:
-        return take_group(pending, self.batched, self.max_slots)
+    def _run_unit(self, v: _View, kind: str, group: List[Request], results, t0):
+        """One query unit on view v (a worker thread); returns the unit's
+        completion time (seconds since t0)."""
+        ts = time.perf_counter()
+        calls = self._bfs_unit(v, group, results) if kind == "bfs" else \
+            self._tc_unit(v, group, results)
+        te = time.perf_counter()
+        with self._lock:
+            self.calls += calls
+            self.groups[kind] += 1
+            self.service_s[kind] += te - ts
+        return te - t0
 
-    def _execute(self, group: List[Request], results):
-        t0 = time.perf_counter()
-        self._execute_group(group, results)
-        kind = "update" if group[0].kind in UPDATE_KINDS else \
-            ("bfs" if group[0].kind == "bfs" else "tc_local")
-        self.service_s[kind] += time.perf_counter() - t0
-
-    def _execute_group(self, group: List[Request], results):
-        if group[0].kind in UPDATE_KINDS:
-            if self.batched:
-                self._update_group(group)
-            else:
-                self._update_plain(group[0])
-                self.groups["update"] += 1
-            for r in group:
-                results[r.rid] = None
-            return
-        bfs = [r for r in group if r.kind == "bfs"]
-        tcs = [r for r in group if r.kind == "tc_local"]
-        if bfs:
-            self._bfs_group(bfs, results)
-        if tcs:
-            self._tc_group(tcs, results)
-
+    # ---- loops ---------------------------------------------------------------
     def run(self, requests: List[Request]) -> ServeReport:
         reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
         n = len(reqs)
@@ -239,40 +275,162 @@ class Server:
         kinds = [r.kind for r in reqs]
         pos = {r.rid: i for i, r in enumerate(reqs)}
         results: Dict[int, object] = {}
-        pending: deque = deque()
-        i = 0
-        done = 0
         t0 = time.perf_counter()
-        last = 0.0
-        while done < n:
-            now = time.perf_counter() - t0
-            while i < n and reqs[i].arrival <= now:
-                pending.append(reqs[i])
-                i += 1
-            if not pending:
-                wait = reqs[i].arrival - (time.perf_counter() - t0)
-                if wait > 2e-3:
-                    time.sleep(wait - 1e-3)
-                continue
-            group = self._take(pending)
-            self._execute(group, results)
-            last = time.perf_counter() - t0
-            for r in group:
-                lat[pos[r.rid]] = last - r.arrival
-            done += len(group)
+        if self.batched:
+            last = self._run_batched(reqs, lat, pos, results, t0)
+        else:
+            last = self._run_plain(reqs, lat, pos, results, t0)
         lat_ms = {}
         for kind in ("insert", "erase", "bfs", "tc_local", "all"):
             sel = lat if kind == "all" else lat[[k == kind for k in kinds]]
             if len(sel):
                 lat_ms[kind] = {"n": int(len(sel)), "p50": round(_pct(sel, 50) * 1e3, 3),
                                 "p99": round(_pct(sel, 99) * 1e3, 3),
+                                "p999": round(_pct(sel, 99.9) * 1e3, 3),
                                 "mean": round(float(sel.mean()) * 1e3, 3)}
         rep = ServeReport("batched" if self.batched else "per_request", n, last,
                           n / last if last > 0 else float("inf"), lat_ms, self.calls,
                           dict(self.groups), self.split_for_memory, results)
         rep.service_ms = {k: round(v * 1e3, 2) for k, v in self.service_s.items()}
         rep.single_bfs = self.single_bfs
+        rep.workers = self.workers
+        rep.max_inflight = self.max_inflight
+        u = np.array(self.update_call_s)
+        rep.update_parts_ms = {k: round(v * 1e3, 2) for k, v in self.update_parts_s.items()}
+        rep.update_calls_ms = {"n": int(len(u)), "p50": round(_pct(u, 50) * 1e3, 3),
+                               "p99": round(_pct(u, 99) * 1e3, 3),
+                               "max": round(float(u.max()) * 1e3 if len(u) else 0.0, 3),
+                               "sum": round(float(u.sum()) * 1e3, 2)}
         return rep
+
+    def _run_plain(self, reqs, lat, pos, results, t0) -> float:
+        n = len(reqs)
+        v = self.views[0]
+        i = done = 0
+        last = 0.0
+        while done < n:
+            now = time.perf_counter() - t0
+            if reqs[i].arrival > now:
+                wait_s = reqs[i].arrival - now
+                if wait_s > 2e-3:
+                    time.sleep(wait_s - 1e-3)
+                continue
+            r = reqs[i]
+            ts = time.perf_counter()
+            if r.kind in UPDATE_KINDS:
+                self._update_plain(r)
+                self.groups["update"] += 1
+                results[r.rid] = None
+                kind = "update"
+            else:
+                kind = r.kind
+                self.calls += self._bfs_unit(v, [r], results) if kind == "bfs" else \
+                    self._tc_unit(v, [r], results)
+                self.groups[kind] += 1
+            te = time.perf_counter()
+            self.service_s[kind] += te - ts
+            last = te - t0
+            lat[pos[r.rid]] = last - r.arrival
+            i += 1
+            done += 1
+        return last
+
+    def _run_batched(self, reqs, lat, pos, results, t0) -> float:
+        n = len(reqs)
+        pending: deque = deque()
+        free = list(self.views)
+        inflight = {}                      # future -> (view, requests)
+        i = done = 0
+        last = 0.0
+        with ThreadPoolExecutor(max_workers=self.workers) as ex:
+
+            def harvest(futs):
+                nonlocal done, last
+                for f in futs:
+                    v, grp = inflight.pop(f)
+                    t = f.result()
+                    free.append(v)
+                    last = max(last, t)
+                    for r in grp:
+                        lat[pos[r.rid]] = t - r.arrival
+                    done += len(grp)
+
+            while done < n:
+                now = time.perf_counter() - t0
+                while i < n and reqs[i].arrival <= now:
+                    pending.append(reqs[i])
+                    i += 1
+                ready = [f for f in inflight if f.done()]
+                if ready:
+                    harvest(ready)
+                    continue
+                if pending and pending[0].kind in UPDATE_KINDS:
+                    if inflight:                       # fence: the epoch's queries first
+                        harvest(wait(list(inflight), return_when=FIRST_COMPLETED)[0])
+                        continue
+                    group = [pending.popleft()]
+                    while pending and pending[0].kind in UPDATE_KINDS:
+                        group.append(pending.popleft())
+                    ts = time.perf_counter()
+                    self._update_group(group)
+                    tr = time.perf_counter()
+                    for v in self.views:
+                        v.g.refresh_view()
+                    te = time.perf_counter()
+                    self.update_parts_s["refresh"] += te - tr
+                    self.service_s["update"] += te - ts
+                    last = max(last, te - t0)
+                    for r in group:
+                        results[r.rid] = None
+                        lat[pos[r.rid]] = te - t0 - r.arrival
+                    done += len(group)
+                    continue
+                if pending and free:
+                    for kind, grp in query_units(pending, len(free), self.msbfs_min,
+                                                 self.max_slots):
+                        v = free.pop()
+                        f = ex.submit(self._run_unit, v, kind, grp, results, t0)
+                        inflight[f] = (v, grp)
+                    self.max_inflight = max(self.max_inflight, len(inflight))
+                    continue
+                # nothing to start: wait for a completion or the next arrival
+                timeout = None
+                if i < n:
+                    timeout = max(0.0, reqs[i].arrival - (time.perf_counter() - t0))
+                if inflight:
+                    harvest(wait(list(inflight), timeout=timeout,
+                                 return_when=FIRST_COMPLETED)[0])
+                elif timeout is not None and timeout > 2e-3:
+                    time.sleep(timeout - 1e-3)
+        return last
+
+
+def query_units(pending: deque, nfree: int, msbfs_min: int, max_slots: int):
+    """Query units for up to nfree free views, popped from the front of
+    `pending` up to the first update (so a unit never crosses an update):
+    the waiting local-TC queries as one unit; the waiting BFS queries as one
+    batched unit when there are at least msbfs_min of them (at most
+    max_slots per unit), else one unit each.  Requests that get no view now
+    go back to the front of `pending`, in arrival order."""
+    qs = []
+    while pending and pending[0].kind in QUERY_KINDS:
+        qs.append(pending.popleft())
+    units = []
+    bfs = [r for r in qs if r.kind == "bfs"]
+    tcs = [r for r in qs if r.kind == "tc_local"]
+    if tcs:
+        units.append(("tc_local", tcs))
+    while bfs:
+        if len(bfs) >= msbfs_min:
+            units.append(("bfs", bfs[:max_slots]))
+            bfs = bfs[max_slots:]
+        else:
+            units.append(("bfs", [bfs.pop(0)]))
+    keep = units[:nfree]
+    back = sorted([r for _, g in units[nfree:] for r in g], key=lambda r: (r.arrival, r.rid))
+    for r in reversed(back):
+        pending.appendleft(r)
+    return keep
 
 
 def take_group(pending: deque, batched: bool, max_slots: int) -> List[Request]:

@@ -178,6 +178,27 @@ int hn_graph_destroy(hn_graph_t* g);
  * stream created with the graph. */
 int hn_graph_set_stream(hn_graph_t* g, void* stream);
 
+/* ---- query views (no reference counterpart) ------------------------------
+ * A query view shares the graph's vertex table and edge pool read-only and
+ * owns its stream (`stream`, a cudaStream_t; NULL = a private one) and its
+ * scratch, so read-only calls on different views of one graph -- BFS
+ * (hn_bfs, hn_bfs_multi, hn_bfs_do, hn_bfs_batch), hn_tc_local, hn_tc,
+ * hn_cc, the exports -- run concurrently on the device, from different
+ * host threads.  The reference has one HornetGraph and synchronous calls,
+ * so concurrent queries on one resident graph have no counterpart there.
+ * Updates go to the graph itself; a view rejects them (HN_ERR_STATE).
+ * While the graph is being updated no call may run on its views; after the
+ * update, hn_graph_view_refresh takes the graph's new edge count (it waits
+ * for the graph's stream).  hn_graph_destroy frees a view; a view must be
+ * destroyed before its graph. */
+int hn_graph_view_create(hn_graph_t* g, void* stream, hn_graph_t** view);
+int hn_graph_view_refresh(hn_graph_t* view);
+
+/* out[i] = src[idx[i]] for device int32 array src (e.g. a row of BFS
+ * distances) and host index / output arrays, on g's stream. */
+int hn_gather_int32(hn_graph_t* g, const int32_t* src, const int64_t* idx, int64_t n,
+                    int32_t* out);
+
 /* ---- queries (hornet/include/Core/Hornet.cuh:113-127,
  *               HornetOperations/HornetQuery.i.cuh) ------------------------ */
 int hn_graph_nv(const hn_graph_t* g, int32_t* nV);

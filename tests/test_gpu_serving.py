@@ -136,3 +136,40 @@ def test_serving_splits_updates_to_fit_memory():
     assert rep.split_for_memory > 0
     assert S.same_results(rep.results, ref)
     assert_same_graph(h, g_end)
+
+
+def test_query_views_run_concurrently_and_reject_updates():
+    """Query views of one resident graph answer BFS and local-TC calls from
+    several host threads at once with the graph's own results, reject
+    updates (HN_ERR_STATE), and see an update of the graph after
+    refresh_view()."""
+    from concurrent.futures import ThreadPoolExecutor
+    g = T.rmat_graph(12, 8, seed=3)
+    h = build(g)
+    views = [h.view() for _ in range(3)]
+    srcs = [0, 5, 17, 99, 1234, 777, 2048, 4000]
+
+    def one(i):
+        v = views[i % 3]
+        d = H.BfsTopDown(v).run_multi([srcs[i]], direction_optimizing=bool(i & 1))[0][0]
+        return d, H.TriangleCounting2(v).local(np.array([srcs[i]], np.int32))
+
+    with ThreadPoolExecutor(3) as ex:
+        outs = list(ex.map(one, range(len(srcs))))
+    _, pv = O.tc(g, per_vertex=True)
+    for s, (d, t) in zip(srcs, outs):
+        np.testing.assert_array_equal(d, O.bfs(g, s)[0])
+        assert int(t[0]) == int(pv[s])
+    bs = np.array([1, 2], np.int32)
+    bd = np.array([2, 1], np.int32)
+    with pytest.raises(H.HornetError) as e:
+        views[0].insert(H.BatchUpdate(views[0], bs, bd), True, True)
+    assert e.value.code == H.HN_ERR_STATE
+    s2, d2 = T.uniform_new_edges(g, 500, seed=8)
+    h.insert(H.BatchUpdate(h, s2, d2), True, True)
+    g2, _ = O.insert(g, s2, d2, 3)
+    for v in views:
+        v.refresh_view()
+        assert v.nE() == g2.nE
+    d, _ = H.BfsTopDown(views[1]).run_multi([5])
+    np.testing.assert_array_equal(d[0], O.bfs(g2, 5)[0])

@@ -63,3 +63,18 @@ def test_same_results():
     assert S.same_results(a, b)
     b[1] = (np.array([1, 3], np.int32), 5)
     assert not S.same_results(a, b)
+
+
+def test_query_units_stop_at_updates_and_return_the_rest():
+    kinds = ["bfs", "tc_local", "bfs", "bfs", "tc_local", "insert", "bfs"]
+    pend = deque(_stream(kinds))
+    units = S.query_units(pend, 2, msbfs_min=4, max_slots=16)
+    # two free views: the TC unit (both TC queries) and the first lone BFS
+    assert [(k, [r.rid for r in g]) for k, g in units] == [("tc_local", [1, 4]), ("bfs", [0])]
+    # the other BFS queries wait at the front, in arrival order, before the update
+    assert [r.rid for r in pend] == [2, 3, 5, 6]
+    # enough BFS queries share one batched unit, capped at max_slots
+    pend = deque(_stream(["bfs"] * 7 + ["erase"]))
+    units = S.query_units(pend, 4, msbfs_min=3, max_slots=5)
+    assert [len(g) for _, g in units] == [5, 1, 1]
+    assert [r.kind for r in pend] == ["erase"]
