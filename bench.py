@@ -401,6 +401,9 @@ def bench_static(args, H, h, deg, nV, nE, stream, dev, rank, world, peak, peak_k
                 do_edges[0] += st[0].edges_scanned
 
         t_do = event_time(stream, timed_do)
+        if not args.no_c3c5:
+            also["c3_updates"] = c3_summary(H, dev, peak, peak_kind)
+            also["c5_serve"] = c5_summary(args, H, dev, rank, world)
         also["bfs_direction_optimizing"] = {
             "metric": "BFS GTEPS", "value": round(do_edges[0] / t_do / 1e9, 4), "unit": "GTEPS",
             "ms_per_step": round(t_do * 1e3 / K, 4),
@@ -531,6 +534,94 @@ def static_extras(args, H, h, nV, nE, stream, dev, peak, peak_kind, scale, tunin
                       "reference has no CPU dynamic graph): the same 1M batch inserted then "
                       f"erased on the same graph, {sbi:.2f} s + {sbe:.2f} s"}
     return also
+
+
+def c3_batch(H, rng, kind, b, nV, scale, seed):
+    """b directed entries of the dynamic-update configuration: b/2 pairs (no
+    self loops) with their mirrors, uniform or R-MAT-distributed; the R-MAT
+    kind replaces ~5 % of its pairs by copies of other pairs of the batch."""
+    half = b // 2
+    if kind == "uniform":
+        u = rng.integers(0, nV, half).astype(np.int32)
+        v = rng.integers(0, nV, half).astype(np.int32)
+    else:
+        u, v = H.gen_rmat_host(scale, half, seed)
+        ndup = half // 20
+        to = rng.choice(half, ndup, replace=False)
+        frm = rng.integers(0, half, ndup)
+        u[to], v[to] = u[frm], v[frm]
+    keep = u != v
+    u, v = u[keep], v[keep]
+    return np.concatenate([u, v]), np.concatenate([v, u])
+
+
+def c3_summary(H, dev, peak, peak_kind, scale=24):
+    """The dynamic-update configuration, compact: R-MAT scale 24 resident;
+    batches of 1K..10M directed edges, uniform and R-MAT-distributed with ~5 %
+    in-batch duplicates, each inserted (both dedup flags) then erased
+    (batch dedup); device time per call from CUDA events on the graph's
+    stream."""
+    import ctypes
+    import torch
+    t0 = time.perf_counter()
+    stream = torch.cuda.Stream(device=dev)
+    h, csr = make_graph_device(H, scale, 16, 1, dev)
+    H.lib().hn_graph_set_stream(h.handle, ctypes.c_void_p(stream.cuda_stream))
+    nV, nE = h.nV(), h.nE()
+    deg0 = np.asarray(h.degrees(), np.int64)
+    rng = np.random.default_rng(2024)
+    rows, tot_e, tot_t = [], 0, 0.0
+    for kind in ("uniform", "rmat"):
+        for i, b in enumerate([1_000, 10_000, 100_000, 1_000_000, 10_000_000]):
+            bs_h, bd_h = c3_batch(H, rng, kind, b, nV, scale, 77 + i)
+            batch = H.BatchUpdate(h, torch.from_numpy(bs_h).cuda(dev),
+                                  torch.from_numpy(bd_h).cuda(dev))
+            n = len(bs_h)
+            ins = [0]
+            ti = event_time(stream, lambda: ins.__setitem__(0, h.insert(batch, True, True)))
+            te = event_time(stream, lambda: h.erase(batch, True))
+            keys = np.unique((bs_h.astype(np.int64) << 32) | bd_h.astype(np.int64))
+            uu = np.unique(keys >> 32)
+            # model bytes (insert): 8 b + 4 applied + 4 sum of the touched
+            # sources' degrees
+            ib = 8 * n + 4 * ins[0] + 4 * int(deg0[uu].sum())
+            rows.append({"kind": kind, "batch": n, "insert_edges_per_s": round(n / ti, 1),
+                         "erase_edges_per_s": round(n / te, 1),
+                         "insert_ms": round(ti * 1e3, 4), "erase_ms": round(te * 1e3, 4),
+                         "applied": int(ins[0]), "insert_frac": round(ib / ti / 1e9 / peak, 4)})
+            tot_e += 2 * n
+            tot_t += ti + te
+    del h, csr
+    return {"metric": "update edges/s", "value": round(tot_e / tot_t, 1), "unit": "edges/s",
+            "config": f"R-MAT scale {scale} ef 16 (nV {nV}, nE {nE}); batches 1K..10M, uniform "
+                      "and R-MAT with ~5% in-batch duplicates, each inserted then erased",
+            "per_batch": rows, "peak_kind": peak_kind,
+            "wall_s": round(time.perf_counter() - t0, 1)}
+
+
+def c5_summary(args, H, dev, rank, world):
+    """The serving configuration, compact: scale 25 resident, the seeded
+    request mix at saturation (all requests at time 0), the plain
+    per-request loops and the continuous-batching loop."""
+    import copy
+    a = copy.copy(args)
+    a.rates = "0"
+    a.requests = args.c5_requests
+    a.scale = 0
+    t0 = time.perf_counter()
+    r = bench_serve(a, H, dev, rank, world)
+    row = r["per_rate"][0]
+    out = {"metric": "served requests/s", "unit": "requests/s",
+           "value": row["batched"]["throughput_rps"], "config": r["config"]["workload"],
+           "requests": a.requests, "results_identical": r["results_identical"]}
+    for m in ("per_request", "per_request_do", "batched"):
+        lat = row[m]["latency_ms"]["all"]
+        out[m] = {"throughput_rps": row[m]["throughput_rps"], "p50_ms": lat["p50"],
+                  "p99_ms": lat["p99"], "p999_ms": lat["p999"]}
+    out["throughput_x_vs_per_request"] = row["throughput_x"]
+    out["throughput_x_vs_per_request_do"] = row["throughput_x_vs_per_request_do"]
+    out["wall_s"] = round(time.perf_counter() - t0, 1)
+    return out
 
 
 def cpu_baseline_bfs(h, sources, args):
@@ -985,6 +1076,9 @@ def main():
     ap.add_argument("--no-extras", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-ktruss", action="store_true")
+    ap.add_argument("--no-c3c5", action="store_true",
+                    help="static: skip the compact dynamic-update and serving summaries")
+    ap.add_argument("--c5-requests", type=int, default=600)
     ap.add_argument("--autotune", action="store_true",
                     help="tune the knobs of each workload first and save them")
     ap.add_argument("--knob", action="append", default=[],
