@@ -62,6 +62,7 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"tc.thread_dc", 32, 1, 1024, false},
     {"bfs.kernel", 1, 0, 1, false},
     {"bfs.warp_ctas_per_sm", 4, 1, 8, false},
+    {"ktruss.device_rounds", 1, 0, 1, false},
 };
 std::atomic<long long> g_knob[kNumKnobs];
 // every knob starts at its default (static initialisation, in definition

@@ -137,6 +137,7 @@ enum Knob {
     kKnobTcThreadDc,
     kKnobBfsKernel,
     kKnobBfsWarpCtasPerSm,
+    kKnobKtDeviceRounds,
     kNumKnobs
 };
 long long knob(Knob k);

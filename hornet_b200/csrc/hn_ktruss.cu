@@ -33,6 +33,25 @@ namespace {
 
 constexpr int kB = 256;
 
+// Device state of the peel rounds.  Every kernel of a round reads its
+// arrays and counts from here, so one instantiated CUDA graph (a WHILE node
+// around the round's kernels) serves every round of every K: the frontier
+// buffers swap, the lists shrink and K advances on the device or between
+// graph launches, never as baked-in kernel arguments.
+struct KtPeel {
+    const long long* off;     // current adjacency lists (rebuilt as edges die)
+    const int32_t* adj;
+    const int32_t* canon;
+    int32_t* F;               // this round's frontier (canonical edge ids)
+    int32_t* NF;              // the next round's frontier
+    int nf;                   // |F|
+    int nNF;                  // |NF| (appended atomically)
+    int nheavy;               // frontier edges left to the heavy kernel
+    int K;
+    long long remaining;      // alive edges
+    long long rounds;         // peel rounds run
+};
+
 __global__ void k_kt_src(const long long* __restrict__ off, int nV, int32_t* __restrict__ src) {
     for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nV;
          u += (long long)gridDim.x * blockDim.x)
@@ -85,11 +104,13 @@ __global__ void k_kt_live_pos(const int32_t* __restrict__ canon, long long n,
 }
 
 // Frontier of round K: alive edges of the list L with support < K - 2.
-__global__ void k_kt_frontier(const int32_t* __restrict__ L, int nL, int K,
+__global__ void k_kt_frontier(const int32_t* __restrict__ L, int nL,
                               const int32_t* __restrict__ sup,
                               const unsigned char* __restrict__ alive,
-                              unsigned char* __restrict__ inF, int32_t* __restrict__ F,
-                              int* __restrict__ nF) {
+                              unsigned char* __restrict__ inF, KtPeel* st) {
+    const int K = st->K;
+    int32_t* F = st->F;
+    int* nF = &st->nf;
     for (long long i0 = blockIdx.x * (long long)blockDim.x; i0 < nL;
          i0 += (long long)gridDim.x * blockDim.x) {
         long long i = i0 + threadIdx.x;
@@ -153,14 +174,19 @@ __device__ __forceinline__ void kt_triangle(int e, int e1, int e2, int K,
 // Frontier edges whose shorter list has at most 32 entries: a thread each.
 // Longer ones go to a list for k_kt_peel_heavy (a CTA each): the dense
 // core's hub-hub edges would otherwise run one long intersection per thread.
-__global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __restrict__ adj,
-                          const int32_t* __restrict__ src, const int32_t* __restrict__ canon,
+__global__ void k_kt_peel(KtPeel* st, const int32_t* __restrict__ src,
                           const int32_t* __restrict__ eadj,
-                          const int32_t* __restrict__ F, int nF, int K,
                           const unsigned char* __restrict__ alive,
                           const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
-                          int32_t* __restrict__ NF, int* __restrict__ nNF,
-                          int32_t* __restrict__ heavy, int* __restrict__ nheavy) {
+                          int32_t* __restrict__ heavy) {
+    const long long* __restrict__ off = st->off;
+    const int32_t* __restrict__ adj = st->adj;
+    const int32_t* __restrict__ canon = st->canon;
+    const int32_t* __restrict__ F = st->F;
+    const int nF = st->nf, K = st->K;
+    int32_t* NF = st->NF;
+    int* nNF = &st->nNF;
+    int* nheavy = &st->nheavy;
     for (long long f0 = blockIdx.x * (long long)blockDim.x; f0 < nF;
          f0 += (long long)gridDim.x * blockDim.x) {
         const long long f = f0 + threadIdx.x;
@@ -193,18 +219,20 @@ __global__ void k_kt_peel(const long long* __restrict__ off, const int32_t* __re
     }
 }
 
-__global__ void k_kt_peel_heavy(const long long* __restrict__ off,
-                                const int32_t* __restrict__ adj,
-                                const int32_t* __restrict__ src,
-                                const int32_t* __restrict__ canon,
+__global__ void k_kt_peel_heavy(KtPeel* st, const int32_t* __restrict__ src,
                                 const int32_t* __restrict__ eadj,
-                                const int32_t* __restrict__ heavy, const int* __restrict__ nheavy,
-                                int K, const unsigned char* __restrict__ alive,
-                                const unsigned char* __restrict__ inF, int32_t* __restrict__ sup,
-                                int32_t* __restrict__ NF, int* __restrict__ nNF) {
+                                const int32_t* __restrict__ heavy,
+                                const unsigned char* __restrict__ alive,
+                                const unsigned char* __restrict__ inF, int32_t* __restrict__ sup) {
+    const long long* __restrict__ off = st->off;
+    const int32_t* __restrict__ adj = st->adj;
+    const int32_t* __restrict__ canon = st->canon;
+    const int K = st->K;
+    int32_t* NF = st->NF;
+    int* nNF = &st->nNF;
     // a CTA per heavy edge: its shorter list is searched by all threads,
     // so a round whose frontier is a few hub-hub edges still spreads them
-    const long long nh = *nheavy;
+    const long long nh = st->nheavy;
     for (long long h = blockIdx.x; h < nh; h += gridDim.x) {
         const int e = heavy[h];
         const int u = src[e], v = eadj[e];
@@ -222,27 +250,48 @@ __global__ void k_kt_peel_heavy(const long long* __restrict__ off,
     }
 }
 
-__global__ void k_kt_retire(const int32_t* __restrict__ F, int nF, const int32_t* __restrict__ NF,
-                            const int* __restrict__ nNF, int K, unsigned char* __restrict__ alive,
+__global__ void k_kt_retire(const KtPeel* st, unsigned char* __restrict__ alive,
                             unsigned char* __restrict__ inF, int32_t* __restrict__ truss) {
-    int nn = *nNF;
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nF || i < nn;
+    const int32_t* __restrict__ F = st->F;
+    const int nF = st->nf, K = st->K;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nF;
          i += (long long)gridDim.x * blockDim.x) {
-        if (i < nF) {
-            int e = F[i];
-            alive[e] = 0;
-            inF[e] = 0;
-            truss[e] = K - 1;
-        }
+        int e = F[i];
+        alive[e] = 0;
+        inF[e] = 0;
+        truss[e] = K - 1;
     }
 }
 
-__global__ void k_kt_mark(const int32_t* __restrict__ NF, const int* __restrict__ nNF,
-                          unsigned char* __restrict__ inF) {
-    int nn = *nNF;
+__global__ void k_kt_mark(const KtPeel* st, unsigned char* __restrict__ inF) {
+    const int32_t* __restrict__ NF = st->NF;
+    const int nn = st->nNF;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nn;
          i += (long long)gridDim.x * blockDim.x)
         inF[NF[i]] = 1;
+}
+
+// End of a round (one thread): the peeled edges leave the alive count, the
+// next frontier becomes the current one, and the WHILE loop continues while
+// it is non-empty.
+__global__ void k_kt_advance(KtPeel* st, cudaGraphConditionalHandle cond, int in_graph) {
+    st->remaining -= st->nf;
+    st->rounds++;
+    int32_t* t = st->F;
+    st->F = st->NF;
+    st->NF = t;
+    st->nf = st->nNF;
+    st->nNF = 0;
+    st->nheavy = 0;
+    if (in_graph) cudaGraphSetConditional(cond, st->nf > 0 ? 1u : 0u);
+}
+
+// Start of a K (one thread): its value, empty frontier counters.
+__global__ void k_kt_begin(KtPeel* st, int K) {
+    st->K = K;
+    st->nf = 0;
+    st->nNF = 0;
+    st->nheavy = 0;
 }
 
 __global__ void k_kt_out(const int32_t* __restrict__ canon, const int32_t* __restrict__ truss,
@@ -313,9 +362,6 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
     read_scalars(g, 1);
     long long remaining = ((int*)g->h_scalar)[0];
     int K = 3;
-    int* nF = cnt + 1;
-    int* nNF = cnt + 2;
-    int* nheavy = cnt + 3;  // frontier edges left to k_kt_peel_heavy (right after nNF)
     int* nL = cnt + 4;      // alive-list length
     int* minsup = cnt + 5;  // smallest support on the alive list
     // the frontier of each K scans only the alive edges, and K jumps to the
@@ -387,38 +433,133 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
         lm = keep;
         cflag.release();
     };
+    // the peel rounds of one K: a CUDA graph whose WHILE node repeats
+    // peel -> heavy peel -> retire -> mark -> advance until a round finds no
+    // new frontier, with no host round trip between rounds
+    DevBuf<KtPeel> st(1, s);
+    KtPeel* h_st = nullptr;
+    HN_CUDA(cudaMallocHost((void**)&h_st, sizeof(KtPeel)));
+    struct HostFree {
+        KtPeel* p;
+        ~HostFree() { cudaFreeHost(p); }
+    } h_st_free{h_st};
+    *h_st = KtPeel{loff, ladj, lcanon, F.get(), NF.get(), 0, 0, 0, K, remaining, 0};
+    HN_CUDA(cudaMemcpyAsync(st.get(), h_st, sizeof(KtPeel), cudaMemcpyHostToDevice, s));
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    struct GraphFree {
+        cudaGraph_t* g;
+        cudaGraphExec_t* e;
+        ~GraphFree() {
+            if (*e) cudaGraphExecDestroy(*e);
+            if (*g) cudaGraphDestroy(*g);
+        }
+    } graph_free{&graph, &exec};
+    const bool device_rounds = knob(kKnobKtDeviceRounds) != 0;
+    if (device_rounds) {
+        HN_CUDA(cudaGraphCreate(&graph, 0));
+        cudaGraphConditionalHandle cond;
+        HN_CUDA(cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        HN_CUDA(cudaGraphAddNode(&cnode, graph, nullptr, 0, &cp));
+        cudaGraph_t body = cp.conditional.phGraph_out[0];
+        KtPeel* a_st = st.get();
+        const int32_t* a_src = src.get();
+        const int32_t* a_eadj = adj.get();
+        const unsigned char* a_alive_c = alive.get();
+        unsigned char* a_alive = alive.get();
+        const unsigned char* a_inF_c = inF.get();
+        unsigned char* a_inF = inF.get();
+        int32_t* a_sup = sup.get();
+        int32_t* a_heavy = H.get();
+        const int32_t* a_heavy_c = H.get();
+        int32_t* a_truss = truss.get();
+        const unsigned sms = (unsigned)g->info.sms;
+        void* peel_args[] = {&a_st, &a_src, &a_eadj, &a_alive_c, &a_inF_c, &a_sup, &a_heavy};
+        void* heavy_args[] = {&a_st, &a_src, &a_eadj, &a_heavy_c, &a_alive_c, &a_inF_c, &a_sup};
+        void* retire_args[] = {&a_st, &a_alive, &a_inF, &a_truss};
+        void* mark_args[] = {&a_st, &a_inF};
+        int one = 1;
+        void* adv_args[] = {&a_st, &cond, &one};
+        struct N {
+            void* f;
+            unsigned grid, block;
+            void** args;
+        } nodes[] = {{(void*)k_kt_peel, sms * 16, 128, peel_args},
+                     {(void*)k_kt_peel_heavy, sms * 8, 256, heavy_args},
+                     {(void*)k_kt_retire, sms * 8, kB, retire_args},
+                     {(void*)k_kt_mark, sms * 8, kB, mark_args},
+                     {(void*)k_kt_advance, 1, 1, adv_args}};
+        cudaGraphNode_t prev = nullptr;
+        for (const N& n : nodes) {
+            cudaKernelNodeParams p = {};
+            p.func = n.f;
+            p.gridDim = dim3(n.grid);
+            p.blockDim = dim3(n.block);
+            p.kernelParams = n.args;
+            cudaGraphNode_t node;
+            HN_CUDA(cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &p));
+            prev = node;
+        }
+        HN_CUDA(cudaGraphInstantiate(&exec, graph, 0));
+    }
     while (true) {
         if (remaining <= 0) { K--; break; }
         const int ms = ((int*)g->h_scalar)[5];
         if (ms + 3 > K) K = ms + 3;
-        HN_CUDA(cudaMemsetAsync(nF, 0, sizeof(int), s));
-        HN_LAUNCH(k_kt_frontier, grid_for(g, n_alive, kB), kB, 0, s, L.get(), n_alive, K,
-                  sup.get(), alive.get(), inF.get(), F.get(), nF);
-        HN_CUDA(cudaMemcpyAsync(g->h_scalar, nF, sizeof(int), cudaMemcpyDeviceToHost, s));
-        HN_CUDA(cudaStreamSynchronize(s));
-        int nf = ((int*)g->h_scalar)[0];
-        while (nf > 0) {
-            HN_CUDA(cudaMemsetAsync(nNF, 0, 2 * sizeof(int), s));   // nNF, nheavy
-            HN_LAUNCH(k_kt_peel, grid_for(g, nf, 128), 128, 0, s, (const long long*)loff,
-                      (const int32_t*)ladj, src.get(), (const int32_t*)lcanon,
-                      (const int32_t*)adj.get(), F.get(), nf, K, alive.get(), inF.get(), sup.get(),
-                      NF.get(), nNF, H.get(), nheavy);
-            HN_LAUNCH(k_kt_peel_heavy, std::min<long long>(nf, (long long)g->info.sms * 8), 256, 0, s,
-                      (const long long*)loff, (const int32_t*)ladj, src.get(),
-                      (const int32_t*)lcanon, (const int32_t*)adj.get(), (const int32_t*)H.get(),
-                      (const int*)nheavy, K, alive.get(), inF.get(), sup.get(), NF.get(), nNF);
-            HN_LAUNCH(k_kt_retire, grid_for(g, nf, kB), kB, 0, s, F.get(), nf, NF.get(), nNF, K,
-                      alive.get(), inF.get(), truss.get());
-            HN_LAUNCH(k_kt_mark, grid_for(g, nf, kB), kB, 0, s, NF.get(), nNF, inF.get());
-            remaining -= nf;
-            HN_CUDA(cudaMemcpyAsync(g->h_scalar, nNF, sizeof(int), cudaMemcpyDeviceToHost, s));
+        HN_LAUNCH(k_kt_begin, 1, 1, 0, s, st.get(), K);
+        HN_LAUNCH(k_kt_frontier, grid_for(g, n_alive, kB), kB, 0, s, L.get(), n_alive,
+                  sup.get(), alive.get(), inF.get(), st.get());
+        const long long rounds_before = h_st->rounds;
+        if (device_rounds) {
+            HN_CUDA(cudaGraphLaunch(exec, s));
+        } else {
+            // host-driven rounds: launches sized to each frontier, one
+            // read-back of the next frontier's size per round
+            HN_CUDA(cudaMemcpyAsync(&h_st->nf, &st.get()->nf, sizeof(int), cudaMemcpyDeviceToHost,
+                                    s));
             HN_CUDA(cudaStreamSynchronize(s));
-            nf = ((int*)g->h_scalar)[0];
-            std::swap(F.p, NF.p);
+            int nf = h_st->nf;
+            while (nf > 0) {
+                HN_LAUNCH(k_kt_peel, grid_for(g, nf, 128), 128, 0, s, st.get(), src.get(),
+                          (const int32_t*)adj.get(), (const unsigned char*)alive.get(),
+                          (const unsigned char*)inF.get(), sup.get(), H.get());
+                HN_LAUNCH(k_kt_peel_heavy, std::min<long long>(nf, (long long)g->info.sms * 8),
+                          256, 0, s, st.get(), src.get(), (const int32_t*)adj.get(),
+                          (const int32_t*)H.get(), (const unsigned char*)alive.get(),
+                          (const unsigned char*)inF.get(), sup.get());
+                HN_LAUNCH(k_kt_retire, grid_for(g, nf, kB), kB, 0, s, (const KtPeel*)st.get(),
+                          alive.get(), inF.get(), truss.get());
+                HN_LAUNCH(k_kt_mark, grid_for(g, nf, kB), kB, 0, s, (const KtPeel*)st.get(),
+                          inF.get());
+                HN_LAUNCH(k_kt_advance, 1, 1, 0, s, st.get(), (cudaGraphConditionalHandle)0, 0);
+                HN_CUDA(cudaMemcpyAsync(&h_st->nf, &st.get()->nf, sizeof(int),
+                                        cudaMemcpyDeviceToHost, s));
+                HN_CUDA(cudaStreamSynchronize(s));
+                nf = h_st->nf;
+            }
         }
-        if (remaining <= 0) { K--; break; }
+        // the state comes back with the alive-list compaction's read-back
+        HN_CUDA(cudaMemcpyAsync(h_st, st.get(), sizeof(KtPeel), cudaMemcpyDeviceToHost, s));
         n_alive = compact(L.get(), n_alive);
+        remaining = h_st->remaining;
+        if (device_rounds)
+            count_launch((int)(5 * (h_st->rounds - rounds_before)));   // kernels the WHILE node ran
+        if (remaining <= 0) { K--; break; }
+        const long long* old_off = loff;
         shrink_lists();
+        if (loff != old_off) {
+            h_st->off = loff;
+            h_st->adj = ladj;
+            h_st->canon = lcanon;
+            HN_CUDA(cudaMemcpyAsync(st.get(), h_st, 3 * sizeof(void*), cudaMemcpyHostToDevice, s));
+            HN_CUDA(cudaStreamSynchronize(s));   // h_st is the copy's source
+        }
         K++;
     }
     if (d_edge_truss)

@@ -138,6 +138,10 @@ int hn_profile_report(char* buf, int64_t len);
  *                       bfs.warp_strided apply to it) (0..1, 1)
  *   bfs.warp_ctas_per_sm  CTAs per SM of the warp-chunk level kernel, 256
  *                       threads each (1..8, 4)
+ *   ktruss.device_rounds  1: the peel rounds of each K run in a CUDA graph
+ *                       (WHILE node, no host round trip per round); 0: one
+ *                       host round trip per round, launches sized to the
+ *                       frontier (0..1, 1)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);

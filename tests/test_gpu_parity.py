@@ -670,3 +670,19 @@ def test_device_graph_save_and_reload(tmp_path):
     # the reloaded graph is a full dynamic graph: it takes further updates
     assert h2.erase(H.BatchUpdate(h2, bs, bd), True) == h.erase(H.BatchUpdate(h, bs, bd), True)
     assert h2.adjacency_hash() == h.adjacency_hash()
+
+
+@pytest.mark.parametrize("device_rounds", [1, 0])
+def test_ktruss_round_drivers(device_rounds):
+    """The peel rounds driven on the device (a CUDA graph's WHILE node) and
+    from the host give the oracle's truss numbers."""
+    g = T.rmat_graph(9, 8, seed=3)
+    h = build(g)
+    kmax, et = O.ktruss(g)
+    try:
+        H.tune_set("ktruss.device_rounds", device_rounds)
+        kt = H.KTruss(h)
+        assert kt.run() == kmax
+        np.testing.assert_array_equal(kt.edge_truss, et)
+    finally:
+        H.tune_reset()
