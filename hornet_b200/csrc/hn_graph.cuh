@@ -138,6 +138,7 @@ enum Knob {
     kKnobBfsKernel,
     kKnobBfsWarpCtasPerSm,
     kKnobKtDeviceRounds,
+    kKnobUpdateBigMin,
     kNumKnobs
 };
 long long knob(Knob k);

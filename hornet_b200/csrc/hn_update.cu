@@ -173,7 +173,8 @@ __global__ void __launch_bounds__(kB)
 k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
        const long long* __restrict__ totals, bool insert, const VRec* __restrict__ vtab,
        long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap,
-       long long* __restrict__ seg_old_off, AllocState* st) {
+       long long* __restrict__ seg_old_off, AllocState* st, int big_min,
+       int32_t* __restrict__ big_list, int* __restrict__ nbig) {
     __shared__ int s_need[kNumClasses], s_push[kNumClasses];
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_need[c] = s_push[c] = 0;
     __syncthreads();
@@ -192,8 +193,12 @@ k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart
             if (r.cap > 0) atomicAdd(&s_push[cap_class(r.cap)], 1);
         }
         seg_ncap[s] = ncap;
-        seg_work[s] = k > 0 ? r.deg : 0;
+        // long old lists (hubs) are moved by k_scatter_big, not by the tiles
+        const bool big = k > 0 && r.deg >= big_min;
+        seg_work[s] = k > 0 && !big ? r.deg : 0;
         seg_old_off[s] = r.off;   // the scatter reads it without the seg_u -> vtab chain
+        const int at = warp_append(nbig, big);
+        if (big) big_list[at] = (int)s;
     }
     __syncthreads();
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) {
@@ -392,6 +397,124 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             }
         }
         __syncthreads();
+    }
+}
+
+// Old lists of at least update.big_min entries (hubs), in chunks of
+// kBigChunk entries.  A chunk that no batch entry falls inside keeps one
+// shift for all its entries (insert: + the batch entries below it; erase:
+// - the deleted entries below it), so it is moved as a block: 16-byte
+// loads into shared memory, 16-byte stores at the shifted place (scalar
+// stores at the unaligned ends).  A chunk with batch entries inside uses the
+// per-entry rule of k_scatter_old on the few entries that fall in it.  The
+// hubs' chunks are numbered through an exclusive scan of their chunk counts
+// (chunk_pre, nbig + 1 entries), and CTAs take chunk numbers round-robin.
+constexpr int kBigChunk = 4096;
+
+__global__ void k_big_chunks(const int32_t* __restrict__ big_list, int nbig,
+                             const int32_t* __restrict__ seg_u, const VRec* __restrict__ vtab,
+                             int* __restrict__ nch) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nbig; i += gridDim.x * blockDim.x)
+        nch[i] = i < nbig ? (vtab[seg_u[big_list[i]]].deg + kBigChunk - 1) / kBigChunk : 0;
+}
+
+template <bool INSERT>
+__global__ void __launch_bounds__(kSB)
+k_scatter_big(const int32_t* __restrict__ big_list, int nbig, const int32_t* __restrict__ seg_u,
+              const int32_t* __restrict__ seg_kstart, const long long* __restrict__ seg_old_off,
+              const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
+              const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
+              const int* __restrict__ chunk_pre) {
+    __shared__ __align__(16) int32_t sbuf[kBigChunk];
+    const int total = chunk_pre[nbig];
+    for (int q = blockIdx.x; q < total; q += gridDim.x) {
+        // the hub of chunk q: last i with chunk_pre[i] <= q (uniform in the CTA)
+        int lo_i = 0, hi_i = nbig;
+        while (hi_i - lo_i > 1) {
+            const int mid = (lo_i + hi_i) >> 1;
+            if (chunk_pre[mid] <= q) lo_i = mid; else hi_i = mid;
+        }
+        const int i = lo_i, c = q - chunk_pre[lo_i];
+        const int sg = big_list[i];
+        const int deg = vtab[seg_u[sg]].deg;
+        const long long old_off = seg_old_off[sg], new_off = seg_new_off[sg];
+        const int k0 = seg_kstart[sg], nb = seg_kstart[sg + 1] - k0;
+        const int32_t* B = cdst + k0;
+        const int32_t* A = pool + old_off;
+        const int r0 = c * kBigChunk;
+        const int n = deg - r0 < kBigChunk ? deg - r0 : kBigChunk;
+        const int32_t a_lo = A[r0], a_hi = A[r0 + n - 1];
+        const int lo = lower_bound32(B, nb, a_lo);   // batch entries below the chunk
+        const int hi = upper_bound32(B, nb, a_hi);   // ... and up to its last entry
+        if (lo == hi) {
+            // one shift for the whole chunk
+            const long long d0 = new_off + r0 + (INSERT ? lo : -lo);
+            if ((old_off & 3) == 0) {
+                const int4* a4 = reinterpret_cast<const int4*>(A + r0);
+                for (int v = threadIdx.x; v < n / 4; v += kSB)
+                    reinterpret_cast<int4*>(sbuf)[v] = __ldcs(a4 + v);
+                for (int v = (n & ~3) + threadIdx.x; v < n; v += kSB) sbuf[v] = A[r0 + v];
+            } else {
+                for (int v = threadIdx.x; v < n; v += kSB) sbuf[v] = A[r0 + v];
+            }
+            __syncthreads();
+            const int lead = (int)((4 - (d0 & 3)) & 3) < n ? (int)((4 - (d0 & 3)) & 3) : n;
+            if (threadIdx.x < lead) pool[d0 + threadIdx.x] = sbuf[threadIdx.x];
+            const int nq = (n - lead) / 4;
+            int4* o4 = reinterpret_cast<int4*>(pool + d0 + lead);
+            for (int q = threadIdx.x; q < nq; q += kSB) {
+                const int b = lead + 4 * q;
+                o4[q] = make_int4(sbuf[b], sbuf[b + 1], sbuf[b + 2], sbuf[b + 3]);
+            }
+            for (int v = lead + 4 * nq + threadIdx.x; v < n; v += kSB) pool[d0 + v] = sbuf[v];
+        } else {
+            // batch entries inside the chunk: the per-entry rule on [lo, hi),
+            // searched in shared memory when they fit there; each thread
+            // takes four consecutive entries of the old list
+            const int m = hi - lo;
+            const bool staged = m <= kBigChunk;   // uniform in the CTA
+            if (staged) {
+                for (int v = threadIdx.x; v < m; v += kSB) sbuf[v] = B[lo + v];
+                __syncthreads();
+            }
+            const int32_t* Bn = staged ? sbuf : B + lo;
+            const bool vec = (old_off & 3) == 0;
+            for (int v4 = threadIdx.x; 4 * v4 < n; v4 += kSB) {
+                const int rb = r0 + 4 * v4;
+                int32_t xs[4];
+                if (vec && 4 * v4 + 4 <= n) {
+                    const int4 q = __ldcs(reinterpret_cast<const int4*>(A + rb));
+                    xs[0] = q.x; xs[1] = q.y; xs[2] = q.z; xs[3] = q.w;
+                } else {
+#pragma unroll
+                    for (int t = 0; t < 4; t++) xs[t] = 4 * v4 + t < n ? A[rb + t] : 0;
+                }
+#pragma unroll
+                for (int t = 0; t < 4; t++) {
+                    if (4 * v4 + t >= n) break;
+                    const int r = rb + t;
+                    const int32_t x = xs[t];
+                    if (INSERT) {
+                        pool[new_off + r + lo + lower_bound32(Bn, m, x)] = x;
+                    } else {
+                        const int ubl = upper_bound32(Bn, m, x);
+                        int lbl = ubl;
+                        if (ubl > 0 && Bn[ubl - 1] == x) lbl = lower_bound32(Bn, ubl, x);
+                        const int cnt = ubl - lbl;   // copies of x this batch deletes
+                        bool keep = true;
+                        if (cnt > 0) {
+                            // rank of this copy among the equal values of the old list
+                            long long first = r;
+                            if (r > 0 && A[r - 1] == x)
+                                first = lower_bound_dev(A, (long long)r, x);
+                            keep = (r - first) >= cnt;
+                        }
+                        if (keep) pool[new_off + r - (lo + ubl)] = x;
+                    }
+                }
+            }
+        }
+        __syncthreads();   // sbuf is reused by the next chunk
     }
 }
 
@@ -637,16 +760,25 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     wv.release();
     keys2.release();
     scan.release();
-    // 4. plan
+    // 4. plan (weighted graphs keep every list on the tile path, which moves
+    // the weights with their neighbours)
+    const int big_min = g->weighted ? INT_MAX : (int)knob(kKnobUpdateBigMin);
+    DevBuf<int32_t> big_list(n + 1, s);
+    DevBuf<int> big_ctr(1, s);   // hubs listed
+    HN_CUDA(cudaMemsetAsync(big_ctr.get(), 0, sizeof(int), s));
     HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
-              insert, g->vtab, seg_work.get(), seg_ncap.get(), seg_old_off.get(), st);
+              insert, g->vtab, seg_work.get(), seg_ncap.get(), seg_old_off.get(), st, big_min,
+              big_list.get(), big_ctr.get());
     // 5. host plan (the one synchronisation of the batch)
     cudaEvent_t plan_ev = nullptr;   // profiled: the stream's idle time across the plan
     if (g_profiling) profile_begin(s, &plan_ev);
     HN_CUDA(cudaMemcpyAsync(g->h_scalar, totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
                             s));
     HN_CUDA(cudaMemcpyAsync(g->h_alloc, st, sizeof(AllocState), cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaMemcpyAsync((int*)(g->h_scalar + 2), big_ctr.get(), sizeof(int),
+                            cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
+    const int nbig = *(const int*)(g->h_scalar + 2);
     if (g->h_alloc->error) {
         HN_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(int), s));
         throw Error(HN_ERR_INVALID, "batch vertex id outside [0, nV)");
@@ -703,6 +835,31 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     const long long grid_sc = (long long)g->info.sms * kScatterCtas;
     DevBuf<long long> splits;
     lb_splits(g, seg_work.get(), nseg, g->nE, Tile::TILE, splits);
+    DevBuf<int> chunk_pre;
+    if (nbig > 0) {
+        chunk_pre.alloc((size_t)nbig + 1, s);
+        HN_LAUNCH(k_big_chunks, grid_for(g, (long long)nbig + 1, kB), kB, 0, s, big_list.get(),
+                  nbig, seg_u.get(), g->vtab, chunk_pre.get());
+        {
+            ProfileScope ps("cub_scan_big", s);
+            size_t tb = 0;
+            HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, chunk_pre.get(), chunk_pre.get(),
+                                                  nbig + 1, s));
+            DevBuf<char> tmp(tb, s);
+            HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, chunk_pre.get(), chunk_pre.get(),
+                                                  nbig + 1, s));
+            count_launch();
+        }
+        const long long grid_big = (long long)g->info.sms * 8;
+        if (insert)
+            HN_LAUNCH(k_scatter_big<true>, grid_big, kSB, 0, s, big_list.get(), nbig, seg_u.get(),
+                      seg_kstart.get(), seg_old_off.get(), seg_new_off.get(), cdst.get(),
+                      g->vtab, g->pool, (const int*)chunk_pre.get());
+        else
+            HN_LAUNCH(k_scatter_big<false>, grid_big, kSB, 0, s, big_list.get(), nbig,
+                      seg_u.get(), seg_kstart.get(), seg_old_off.get(), seg_new_off.get(),
+                      cdst.get(), g->vtab, g->pool, (const int*)chunk_pre.get());
+    }
     if (insert) {
         HN_LAUNCH(k_scatter_old<true>, grid_sc, kSB, 0, s, seg_work.get(), nseg,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),

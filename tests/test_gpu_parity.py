@@ -686,3 +686,50 @@ def test_ktruss_round_drivers(device_rounds):
         np.testing.assert_array_equal(kt.edge_truss, et)
     finally:
         H.tune_reset()
+
+
+@pytest.mark.parametrize("big_min", [2048, 4, 1 << 30])
+def test_updates_on_long_lists(big_min):
+    """Insert and erase batches that reach long adjacency lists (a star with
+    20,000 leaves beside an R-MAT graph) equal the oracle's multiset model,
+    with the long lists moved by the chunked hub scatter (update.big_min:
+    the default 2048, 4 = nearly every list) or by the tiles alone (2^30).
+    Batches hit chunks with and without batch entries inside, and a
+    multigraph stage makes the erase rank rule apply inside hub chunks."""
+    n_star = 20001
+    star = O.build_csr_undirected(n_star, np.zeros(n_star - 1, np.int32),
+                                  np.arange(1, n_star, dtype=np.int32))
+    g, base = T.disjoint_union([star, T.rmat_graph(12, 16, seed=7)])
+    rng = np.random.default_rng(11)
+    try:
+        H.tune_set("update.big_min", big_min)
+        h = build(g)
+        for step in range(8):
+            if step % 2 == 0:
+                # edges from the hub (or, every other time, from the first
+                # R-MAT vertex) to leaves in one id range, so most chunks of
+                # the hub's list see no batch entry, plus random edges
+                hub = 0 if step % 4 == 0 else n_star
+                lo = int(rng.integers(1, n_star - 600))
+                leaves = rng.integers(lo, lo + 500, 300).astype(np.int32)
+                s = np.concatenate([np.full(300, hub, np.int32),
+                                    rng.integers(0, g.nV, 2000).astype(np.int32)])
+                d = np.concatenate([leaves, rng.integers(0, g.nV, 2000).astype(np.int32)])
+                flags = (True, True) if step != 4 else (False, False)   # step 4: multigraph
+                h.insert(H.BatchUpdate(h, s, d), *flags)
+                g, _ = O.insert(g, s, d, 3 if flags[0] else 0)
+            else:
+                es, ed = g.coo()
+                hub_edges = np.nonzero(es == 0)[0]
+                pick = np.concatenate([rng.choice(hub_edges, 400, replace=False),
+                                       rng.integers(0, len(es), 1500)])
+                s, d = es[pick], ed[pick]
+                if step == 5:   # duplicates in the batch: several copies of an edge go
+                    s = np.concatenate([s, s[:50]])
+                    d = np.concatenate([d, d[:50]])
+                dedup = step != 5
+                h.erase(H.BatchUpdate(h, s, d), dedup)
+                g, _ = O.erase(g, s, d, 1 if dedup else 0)
+            assert_same_graph(h, g)
+    finally:
+        H.tune_reset()
