@@ -980,17 +980,18 @@ def bench_serve(args, H, dev, rank, world):
             srv.close()
             del srv, h
             gc.collect()
-        same = S.same_results(res["per_request"], res["batched"]) and \
-            S.same_results(res["per_request"], res["per_request_do"])
+        modes = list(res)
+        same = all(S.same_results(res[modes[0]], res[m]) for m in modes[1:])
         identical &= same
         row["results_identical"] = same
-        pr, pd, bt = row["per_request"], row["per_request_do"], row["batched"]
-        row["throughput_x"] = round(bt["throughput_rps"] / pr["throughput_rps"], 2)
-        row["throughput_x_vs_per_request_do"] = round(bt["throughput_rps"] / pd["throughput_rps"], 2)
-        row["p99_ms"] = {m: row[m]["latency_ms"]["all"]["p99"]
-                         for m in ("per_request", "per_request_do", "batched")}
-        row["p999_ms"] = {m: row[m]["latency_ms"]["all"]["p999"]
-                          for m in ("per_request", "per_request_do", "batched")}
+        bt = row["batched"]
+        if "per_request" in row:
+            row["throughput_x"] = round(bt["throughput_rps"] / row["per_request"]["throughput_rps"], 2)
+        if "per_request_do" in row:
+            row["throughput_x_vs_per_request_do"] = round(
+                bt["throughput_rps"] / row["per_request_do"]["throughput_rps"], 2)
+        row["p99_ms"] = {m: row[m]["latency_ms"]["all"]["p99"] for m in modes}
+        row["p999_ms"] = {m: row[m]["latency_ms"]["all"]["p999"] for m in modes}
         table.append(row)
     sat = [r for r in table if r["rate_rps"] == "saturation"]
     head = sat[0] if sat else table[-1]
@@ -1005,7 +1006,7 @@ def bench_serve(args, H, dev, rank, world):
                        "nV": nV, "nE": nE, "requests_per_rate": args.requests,
                        "parallelism": f"replicas x{world}", "l2": "graph > 126 MB L2; no flush"},
             "per_rate": table, "results_identical": identical,
-            "saturation_throughput_x": head["throughput_x"], "build_s": round(build_s, 2)}
+            "saturation_throughput_x": head.get("throughput_x"), "build_s": round(build_s, 2)}
 
 
 def run_reference(args):
@@ -1062,7 +1063,7 @@ def main():
     ap.add_argument("--workload", default="static", choices=["static", "update", "batch", "serve"])
     ap.add_argument("--rates", default="250,500,1000,2000,0")
     ap.add_argument("--requests", type=int, default=1000)
-    ap.add_argument("--msbfs-min", type=int, default=4,
+    ap.add_argument("--msbfs-min", type=int, default=16,
                     help="serve: smallest run of BFS queries answered by one batched traversal")
     ap.add_argument("--serve-modes", default="per_request,per_request_do,batched",
                     help="serve: the loops to run, in this order")

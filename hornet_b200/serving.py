@@ -118,7 +118,7 @@ class Server:
 
     def __init__(self, hornet: Hornet, batched: bool = True, max_slots: int = 16,
                  max_update_edges: int = 1 << 24, reserve_bytes: int = 2 << 30,
-                 free_bytes_fn=None, single_bfs: str = "", msbfs_min: int = 4,
+                 free_bytes_fn=None, single_bfs: str = "", msbfs_min: int = 16,
                  workers: int = 4):
         import torch
         self.h = hornet
