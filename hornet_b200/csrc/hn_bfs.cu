@@ -1101,6 +1101,7 @@ int hn_bfs(hn_graph_t* g, int32_t src, int32_t* dist, int mem, hn_bfs_stats_t* s
     HN_REQUIRE(g && dist, "null argument");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_REQUIRE(g->nV > 0, "empty graph");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     bfs_run(g, &src, 1, dist, mem, stats, false);
     HN_API_END
@@ -1113,6 +1114,7 @@ int hn_bfs_multi(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist
     HN_REQUIRE(k >= 0, "negative source count");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_REQUIRE(g->nV > 0 || k == 0, "empty graph");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     bfs_run(g, sources, k, dist, mem, stats, false);
     HN_API_END
@@ -1144,6 +1146,7 @@ int hn_bfs_do(hn_graph_t* g, const int32_t* sources, int32_t k, int32_t* dist, i
     HN_REQUIRE(k >= 0, "negative source count");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_REQUIRE(g->nV > 0 || k == 0, "empty graph");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     bfs_run(g, sources, k, dist, mem, stats, true);
     HN_API_END

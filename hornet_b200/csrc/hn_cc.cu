@@ -212,6 +212,7 @@ extern "C" int hn_cc(hn_graph_t* g, int mode, int32_t* labels, int mem, int32_t*
     HN_REQUIRE(g && labels, "null argument");
     HN_REQUIRE(mode == HN_CC_MIN_ID || mode == HN_CC_REFERENCE, "bad CC mode");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     const int nV = g->nV;

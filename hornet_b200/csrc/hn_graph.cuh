@@ -139,6 +139,7 @@ enum Knob {
     kKnobBfsWarpCtasPerSm,
     kKnobKtDeviceRounds,
     kKnobUpdateBigMin,
+    kKnobUpdateInPlace,
     kNumKnobs
 };
 long long knob(Knob k);
@@ -214,6 +215,9 @@ struct hn_graph {
     // a query view (hn_graph_view_create): shares the parent's vertex table
     // and edge pool read-only, owns its stream and scratch
     hn_graph* parent = nullptr;
+
+    // set while a call that uses this handle's stream and scratch runs
+    std::atomic<int> in_use{0};
 };
 
 namespace hn {
@@ -221,6 +225,26 @@ namespace hn {
 inline void require_owner(const hn_graph* g) {
     if (g->parent) throw Error(HN_ERR_STATE, "a query view cannot update the graph");
 }
+
+// Held for the duration of a call that uses the handle's stream and scratch
+// (traversals, counts, updates): one handle serves one host thread at a
+// time, and a second thread's call on a busy handle is refused instead of
+// sharing the scratch.  Concurrent queries use one view per thread.
+class HandleUse {
+public:
+    explicit HandleUse(hn_graph* g) : g_(g) {
+        int idle = 0;
+        if (!g_->in_use.compare_exchange_strong(idle, 1, std::memory_order_acquire))
+            throw Error(HN_ERR_STATE,
+                        "graph handle in use by another host thread (use one view per thread)");
+    }
+    ~HandleUse() { g_->in_use.store(0, std::memory_order_release); }
+    HandleUse(const HandleUse&) = delete;
+    HandleUse& operator=(const HandleUse&) = delete;
+
+private:
+    hn_graph* g_;
+};
 }  // namespace hn
 
 struct hn_batch {

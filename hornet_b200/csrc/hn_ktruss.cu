@@ -22,6 +22,8 @@
 // lives on the (u < v) position.
 #include <cub/cub.cuh>
 
+#include <optional>
+
 #include <algorithm>
 #include <climits>
 
@@ -578,6 +580,7 @@ extern "C" int hn_ktruss(hn_graph_t* g, int32_t* max_k, int32_t* edge_truss, int
     HN_API_BEGIN
     HN_REQUIRE(g != nullptr, "graph is null");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     DevBuf<int32_t> tmp;
@@ -600,6 +603,8 @@ extern "C" int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t*
     HN_REQUIRE(g != nullptr, "graph is null");
     HN_REQUIRE(K >= 2, "K must be at least 2");
     require_owner(g);
+    std::optional<HandleUse> use;   // released before the erase call below takes it
+    use.emplace(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     if (removed) *removed = 0;
@@ -631,6 +636,7 @@ extern "C" int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t*
     if (max_k) *max_k = kmax;
     if (nrem == 0) return HN_OK;
     // the below-K edges leave the graph through the ordinary erase pipeline
+    use.reset();
     hn_batch_t* b = nullptr;
     rc = hn_batch_create(g, nrem, esrc.get(), edst.get(), HN_MEM_DEVICE, &b);
     if (rc != HN_OK) return rc;

@@ -506,6 +506,7 @@ extern "C" int hn_bfs_batch(hn_graph_t* g, const int32_t* sources, const int32_t
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     HN_REQUIRE(g->nV > 0, "empty graph");
     HN_REQUIRE(g->nE < 0xFFFFFFFFll, "batched BFS needs nE < 2^32");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     const int nV = g->nV;

@@ -938,6 +938,7 @@ extern "C" int hn_tc(hn_graph_t* g, uint64_t* per_vertex, int mem, uint64_t* tot
     HN_API_BEGIN
     HN_REQUIRE(g != nullptr, "graph is null");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     if (g->nV == 0) {

@@ -181,6 +181,7 @@ extern "C" int hn_tc_local(hn_graph_t* g, const int32_t* seeds, int32_t k, uint6
     HN_REQUIRE(k >= 0, "negative seed count");
     HN_REQUIRE(mem == HN_MEM_HOST || mem == HN_MEM_DEVICE, "bad memory kind");
     if (k == 0) return HN_OK;
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     const int32_t* d_seeds = seeds;

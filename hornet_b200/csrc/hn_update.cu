@@ -71,10 +71,14 @@ __global__ void k_pack(const int32_t* __restrict__ src, const int32_t* __restric
 // first of each run (thrust::unique_copy) and mark_duplicate_edges clears the
 // flag of the FIRST batch entry equal to each graph edge
 // (BatchUpdateKernels.cuh:27-58 with xlib lower_bound_left).
+//
+// apos[i] = the number of old-list entries <= x, so that a kept entry's
+// place in the merged list (its rank among the kept batch entries of its
+// vertex + apos) is known before any old list is rewritten in place.
 __global__ void k_mark_insert(const unsigned long long* __restrict__ keys, long long n, int L,
                               unsigned flags, const VRec* __restrict__ vtab,
                               const int32_t* __restrict__ pool,
-                              unsigned long long* __restrict__ val) {
+                              unsigned long long* __restrict__ val, int32_t* __restrict__ apos) {
     const unsigned long long mask = (1ull << L) - 1;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -83,13 +87,14 @@ __global__ void k_mark_insert(const unsigned long long* __restrict__ keys, long 
         bool first = (i == 0) || (k != kp);
         bool head = (i == 0) || ((k >> L) != (kp >> L));
         bool keep = first || !(flags & HN_DEDUP_BATCH);
-        if (keep && first && (flags & HN_DEDUP_GRAPH)) {
+        if (keep) {
             int u = (int)(k >> L);
             int x = (int)(k & mask);
             VRec r = vtab[u];
             const int32_t* a = pool + r.off;
-            long long p = lower_bound_dev(a, (long long)r.deg, x);
-            if (p < r.deg && a[p] == x) keep = false;
+            const long long ub = upper_bound_dev(a, (long long)r.deg, x);
+            if (first && (flags & HN_DEDUP_GRAPH) && ub > 0 && a[ub - 1] == x) keep = false;
+            apos[i] = (int32_t)ub;
         }
         val[i] = ((unsigned long long)head << 32) | (unsigned long long)keep;
     }
@@ -138,7 +143,8 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
                           int32_t* __restrict__ cdst, int32_t* __restrict__ cseg,
                           int32_t* __restrict__ seg_u, int32_t* __restrict__ seg_kstart,
                           long long* __restrict__ totals, const uint32_t* __restrict__ wsorted,
-                          uint32_t* __restrict__ cw) {
+                          uint32_t* __restrict__ cw, const int32_t* __restrict__ apos,
+                          int32_t* __restrict__ capos) {
     const unsigned long long mask = (1ull << L) - 1;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
@@ -154,6 +160,7 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
             cdst[pos] = (int)(k & mask);
             cseg[pos] = (int)seg;
             if (cw) cw[pos] = wsorted[i];
+            if (capos) capos[pos] = apos[i];
         }
         if (i == n - 1) {
             long long kept = pos + (long long)(v & 1);
@@ -166,15 +173,29 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
 }
 
 // Per touched vertex: new degree / class; request and release counts.
-// seg_work[s] = old degree if the vertex changes, else 0.  The per-class
-// counts are gathered in shared memory and added once per CTA (a global
-// atomic per segment serialises on the few popular classes).
+// A vertex whose block class does not change (pow2_ceil of the new degree
+// equals its capacity, the reference's Vertex::limit() test,
+// BatchUpdateKernels.cuh:150-198) is updated in place (seg_ncap = kInPlace):
+// only the part of its list from the first entry that moves, [base, deg),
+// is rewritten (insert: base = the old entries <= the smallest batch entry;
+// erase: base = the old entries below the smallest deleted one), and only
+// when that part has at most kInPlaceMax entries, so that one warp can stage
+// it.  Other vertices move to a new block (seg_ncap = new capacity, 0 for
+// an emptied list, -1 for a vertex without batch entries) and their whole
+// list is the work.  seg_work[s] = entries the scatter moves (0 for hubs,
+// which k_scatter_big moves).  The per-class counts are gathered in shared
+// memory and added once per CTA (a global atomic per segment serialises on
+// the few popular classes).
+constexpr int kInPlace = -2;
+constexpr int kInPlaceMax = 2048;
+
 __global__ void __launch_bounds__(kB)
 k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
        const long long* __restrict__ totals, bool insert, const VRec* __restrict__ vtab,
+       const int32_t* __restrict__ pool, const int32_t* __restrict__ cdst, bool in_place,
        long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap,
-       long long* __restrict__ seg_old_off, AllocState* st, int big_min,
-       int32_t* __restrict__ big_list, int* __restrict__ nbig) {
+       int32_t* __restrict__ seg_base, long long* __restrict__ seg_old_off, AllocState* st,
+       int big_min, int32_t* __restrict__ big_list, int* __restrict__ nbig) {
     __shared__ int s_need[kNumClasses], s_push[kNumClasses];
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_need[c] = s_push[c] = 0;
     __syncthreads();
@@ -182,20 +203,36 @@ k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart
     for (long long s = blockIdx.x * (long long)blockDim.x + threadIdx.x; s <= nseg;
          s += (long long)gridDim.x * blockDim.x) {
         if (s == nseg) { seg_work[s] = 0; continue; }
-        int k = seg_kstart[s + 1] - seg_kstart[s];
+        const int k0 = seg_kstart[s];
+        int k = seg_kstart[s + 1] - k0;
         int u = seg_u[s];
         VRec r = vtab[u];
         int ncap = -1;  // -1: vertex unchanged
+        int base = 0;
+        // long old lists (hubs) are moved by k_scatter_big, not by the tiles
+        const bool big = k > 0 && r.deg >= big_min;
         if (k > 0) {
             int nd = insert ? r.deg + k : r.deg - k;
             ncap = pow2_ceil(nd);
-            if (ncap > 0) atomicAdd(&s_need[cap_class(ncap)], 1);
-            if (r.cap > 0) atomicAdd(&s_push[cap_class(r.cap)], 1);
+            bool here = in_place && !big && nd > 0 && ncap == r.cap;
+            if (here) {
+                const int32_t b0 = cdst[k0];
+                const int32_t* a = pool + r.off;
+                base = insert ? (int)upper_bound_dev(a, (long long)r.deg, b0)
+                              : (int)lower_bound_dev(a, (long long)r.deg, b0);
+                here = r.deg - base <= kInPlaceMax;
+            }
+            if (here) {
+                ncap = kInPlace;
+            } else {
+                base = 0;
+                if (ncap > 0) atomicAdd(&s_need[cap_class(ncap)], 1);
+                if (r.cap > 0) atomicAdd(&s_push[cap_class(r.cap)], 1);
+            }
         }
         seg_ncap[s] = ncap;
-        // long old lists (hubs) are moved by k_scatter_big, not by the tiles
-        const bool big = k > 0 && r.deg >= big_min;
-        seg_work[s] = k > 0 && !big ? r.deg : 0;
+        seg_base[s] = base;
+        seg_work[s] = k > 0 && !big ? r.deg - base : 0;
         seg_old_off[s] = r.off;   // the scatter reads it without the seg_u -> vtab chain
         const int at = warp_append(nbig, big);
         if (big) big_list[at] = (int)s;
@@ -221,7 +258,7 @@ __device__ __forceinline__ void cta_range(long long n, long long& s0, long long&
 __global__ void __launch_bounds__(kB)
 k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
          long long* const* __restrict__ fl, AllocState* st,
-         long long* __restrict__ seg_new_off) {
+         const long long* __restrict__ seg_old_off, long long* __restrict__ seg_new_off) {
     __shared__ int s_cnt[kNumClasses], s_base[kNumClasses];
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_cnt[c] = 0;
     __syncthreads();
@@ -239,7 +276,7 @@ k_assign(const int32_t* __restrict__ seg_ncap, long long nseg, Plan plan,
     __syncthreads();
     for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         int ncap = seg_ncap[s];
-        long long off = 0;
+        long long off = ncap == kInPlace ? seg_old_off[s] : 0;
         if (ncap > 0) {
             int c = cap_class(ncap);
             int r = s_base[c] + atomicAdd(&s_cnt[c], 1);
@@ -277,22 +314,33 @@ __device__ __forceinline__ int upper_bound32(const int32_t* a, int n, int32_t x)
     return lo;
 }
 
-// Old adjacency of every changed vertex -> its new block.  The batch
-// entries the tile's segments search are one contiguous run of cdst (the
-// segments are consecutive sources and cdst is sorted by source): when the
-// run has at most kStage entries it is staged in shared memory, so the
-// per-item searches do not wait on global loads.
+// Old adjacency of every changed vertex -> its place in the new block, or
+// in its own block for a vertex updated in place (only its entries from
+// seg_base on are work items).  The batch entries the tile's segments search
+// are one contiguous run of cdst (the segments are consecutive sources and
+// cdst is sorted by source): when the run has at most kStage entries it is
+// staged in shared memory, so the per-item searches do not wait on global
+// loads.
+//
+// In place, an entry's new slot may be another entry's old slot, so every
+// item's value and destination are read and computed before the barrier
+// and stored after it.  That orders the reads before the writes within the
+// CTA; a vertex updated in place whose items span two tiles (two CTAs)
+// would not be ordered, so the tiles leave it alone and the tile holding
+// its first item lists it for k_inplace_span, which moves it whole.
 template <bool INSERT>
 __global__ void __launch_bounds__(kSB, kScatterCtas)
 k_scatter_old(const long long* __restrict__ prefix, long long nseg,
               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
-              const long long* __restrict__ seg_old_off, int32_t* __restrict__ pool,
+              const long long* __restrict__ seg_old_off, const int32_t* __restrict__ seg_ncap,
+              const int32_t* __restrict__ seg_base, int32_t* __restrict__ pool,
               const long long* __restrict__ splits, long long split_tiles,
-              uint32_t* __restrict__ wpool) {
+              uint32_t* __restrict__ wpool, int32_t* __restrict__ span_list,
+              int* __restrict__ nspan, long long span_cap) {
     __shared__ Tile t;
-    __shared__ long long s_old[Tile::TILE + 1];
-    __shared__ long long s_new[Tile::TILE + 1];
+    __shared__ long long s_old[Tile::TILE + 1];   // old slot of item e: s_old[b] + e
+    __shared__ long long s_new[Tile::TILE + 1];   // slot before the batch shift: s_new[b] + e
     __shared__ int s_k0[Tile::TILE + 1];   // the batch list of segment b, narrowed to
     __shared__ int s_k1[Tile::TILE + 1];   // the old values this tile holds: [k0, k1)
     __shared__ int s_kb[Tile::TILE + 1];   // batch entries of the segment before k0
@@ -308,18 +356,32 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
         int n = lb_tile_load(t, prefix, nseg, total, tile, splits, split_tiles);
         for (int b = threadIdx.x; b <= t.nends; b += kSB) {
             long long s = t.seg0 + b;
+            s_k0[b] = 0;
+            s_k1[b] = -1;   // marks a segment this tile does not move
             if (s < nseg) {
                 const long long st0 = t.seg_start(b);
-                const long long old_off = seg_old_off[s];
+                const long long en = t.ends[b], tend = t.item0 + n;
+                if (seg_ncap[s] == kInPlace && (st0 < t.item0 || en > tend)) {
+                    // in place and spanning tiles: listed once, by the tile
+                    // holding its first item
+                    if (st0 >= t.item0 && st0 < tend) {
+                        // one vertex per tile boundary at most, so the
+                        // list (one entry per tile) never fills
+                        const int at = atomicAdd(nspan, 1);
+                        if (at < span_cap) span_list[at] = (int)s;
+                    }
+                    continue;
+                }
+                const int base = seg_base[s];
+                const long long old_off = seg_old_off[s] + base;
                 s_old[b] = old_off - st0;
-                s_new[b] = seg_new_off[s] - st0;
+                s_new[b] = seg_new_off[s] + base - st0;
                 const int k0 = seg_kstart[s], k1 = seg_kstart[s + 1];
                 // a segment with a long batch list (a hub hit by many
                 // updates) searches only the batch entries that can fall
                 // between this tile's first and last old value; short lists
                 // are searched whole
                 const long long lo_e = st0 > t.item0 ? st0 : t.item0;
-                const long long en = t.ends[b], tend = t.item0 + n;
                 const long long hi_e = en < tend ? en : tend;
                 int blo = 0, bhi = k1 - k0;
                 if (lo_e < hi_e && k1 - k0 > 8) {   // short batch lists: searched whole
@@ -349,9 +411,12 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             bs[k] = -1;
             ws[k] = 0;
             if (i < n) {
-                bs[k] = t.seg[i];
-                xs[k] = pool[s_old[bs[k]] + t.item0 + i];
-                if (wpool) ws[k] = wpool[s_old[bs[k]] + t.item0 + i];
+                const int b = t.seg[i];
+                if (s_k1[b] >= s_k0[b]) {
+                    bs[k] = b;
+                    xs[k] = pool[s_old[b] + t.item0 + i];
+                    if (wpool) ws[k] = wpool[s_old[b] + t.item0 + i];
+                }
             }
         }
         // stage the tile's batch run while those loads are in flight
@@ -361,8 +426,10 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             for (int i = threadIdx.x; i < K1 - K0; i += kSB) s_cd[i] = cdst[K0 + i];
             __syncthreads();
         }
+        long long to[IPT];   // destination slot, -1 = the entry is deleted
 #pragma unroll
         for (int k = 0; k < IPT; k++) {
+            to[k] = -1;
             if (bs[k] < 0) continue;
             const int b = bs[k];
             const int x = xs[k];
@@ -371,32 +438,81 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
             // read only when nb > 0, and then [s_k0[b], s_k1[b]) lies in [K0, K1)
             const int32_t* B = staged ? s_cd + (s_k0[b] - K0) : cdst + s_k0[b];
             if (INSERT) {
-                long long j = s_kb[b] + lower_bound32(B, nb, x);
-                pool[s_new[b] + e + j] = x;
-                if (wpool) wpool[s_new[b] + e + j] = ws[k];
+                to[k] = s_new[b] + e + s_kb[b] + lower_bound32(B, nb, x);
             } else {
                 // every batch copy of x lies inside the narrowed range
                 long long ubl = upper_bound32(B, nb, x);
                 long long lbl = ubl;
                 if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound32(B, (int)ubl, x);
                 long long cnt = ubl - lbl;  // copies of x to delete
-                long long ub = s_kb[b] + ubl;
                 bool keep = true;
                 if (cnt > 0) {
                     // rank of this copy among equal values of the old list
+                    // (the entries before seg_base are all below x)
                     long long r = e - t.seg_start(b);
                     const int32_t* A = pool + s_old[b] + t.seg_start(b);
                     long long first = r;
                     if (r > 0 && A[r - 1] == x) first = lower_bound_dev(A, r, x);
                     keep = (r - first) >= cnt;
                 }
-                if (keep) {
-                    pool[s_new[b] + e - ub] = x;
-                    if (wpool) wpool[s_new[b] + e - ub] = ws[k];
-                }
+                if (keep) to[k] = s_new[b] + e - (s_kb[b] + ubl);
             }
         }
+        __syncthreads();   // every read of this tile's lists before any write
+#pragma unroll
+        for (int k = 0; k < IPT; k++) {
+            if (to[k] < 0) continue;
+            pool[to[k]] = xs[k];
+            if (wpool) wpool[to[k]] = ws[k];
+        }
         __syncthreads();
+    }
+}
+
+// Vertices updated in place whose moved entries span two or more scatter
+// tiles: a warp each stages the moved part [base, deg) (at most kInPlaceMax
+// entries) in shared memory, then writes every entry to its new slot, so
+// all reads precede all writes.  Same slot rules as k_scatter_old.
+constexpr int kSpanWarps = 4;
+
+template <bool INSERT>
+__global__ void __launch_bounds__(kSpanWarps * 32)
+k_inplace_span(const int32_t* __restrict__ span_list, const int* __restrict__ nspan,
+               const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
+               const int32_t* __restrict__ seg_base, const long long* __restrict__ seg_old_off,
+               const int32_t* __restrict__ cdst, const VRec* __restrict__ vtab,
+               int32_t* __restrict__ pool, long long span_cap) {
+    __shared__ int32_t sA[kSpanWarps][kInPlaceMax];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int32_t* A = sA[w];
+    const int count = *nspan < span_cap ? *nspan : (int)span_cap;
+    for (int i = blockIdx.x * kSpanWarps + w; i < count; i += gridDim.x * kSpanWarps) {
+        const int s = span_list[i];
+        const int base = seg_base[s];
+        const int n = vtab[seg_u[s]].deg - base;   // the old degree: commit runs later
+        const long long off = seg_old_off[s] + base;
+        for (int j = lane; j < n; j += 32) A[j] = pool[off + j];
+        __syncwarp();
+        const int k0 = seg_kstart[s], nb = seg_kstart[s + 1] - k0;
+        const int32_t* B = cdst + k0;
+        for (int j = lane; j < n; j += 32) {
+            const int32_t x = A[j];
+            if (INSERT) {
+                pool[off + j + lower_bound32(B, nb, x)] = x;
+            } else {
+                const int ubl = upper_bound32(B, nb, x);
+                int lbl = ubl;
+                if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound32(B, ubl, x);
+                bool keep = true;
+                if (ubl > lbl) {
+                    int first = j;
+                    if (j > 0 && A[j - 1] == x) first = lower_bound32(A, j, x);
+                    keep = (j - first) >= ubl - lbl;
+                }
+                if (keep) pool[off + j - ubl] = x;
+            }
+        }
+        __syncwarp();   // A is restaged for the next vertex
     }
 }
 
@@ -518,23 +634,23 @@ k_scatter_big(const int32_t* __restrict__ big_list, int nbig, const int32_t* __r
     }
 }
 
-// Batch edges -> their slot in the new block (insert only).
+// Batch edges -> their slot in the merged list (insert only; after the old
+// entries have moved): rank among the vertex's kept batch entries + the old
+// entries <= it (capos, recorded by k_mark_insert before any list moved).
 __global__ void k_scatter_new(const int32_t* __restrict__ cdst, const int32_t* __restrict__ cseg,
+                              const int32_t* __restrict__ capos,
                               const long long* __restrict__ totals,
-                              const int32_t* __restrict__ seg_u,
                               const int32_t* __restrict__ seg_kstart,
                               const long long* __restrict__ seg_new_off,
-                              const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
+                              int32_t* __restrict__ pool,
                               const uint32_t* __restrict__ cw, uint32_t* __restrict__ wpool) {
     long long kept = totals[0];
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < kept;
          p += (long long)gridDim.x * blockDim.x) {
-        int s = cseg[p];
-        int x = cdst[p];
-        VRec r = vtab[seg_u[s]];
-        long long pos = upper_bound_dev(pool + r.off, (long long)r.deg, x);
-        pool[seg_new_off[s] + (p - seg_kstart[s]) + pos] = x;
-        if (wpool) wpool[seg_new_off[s] + (p - seg_kstart[s]) + pos] = cw ? cw[p] : 0u;
+        const int s = cseg[p];
+        const long long at = seg_new_off[s] + (p - seg_kstart[s]) + capos[p];
+        pool[at] = cdst[p];
+        if (wpool) wpool[at] = cw ? cw[p] : 0u;
     }
 }
 
@@ -551,7 +667,7 @@ k_commit(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_ksta
     long long s0, s1;
     cta_range(nseg, s0, s1);
     for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-        if (seg_ncap[s] < 0) continue;
+        if (seg_ncap[s] < 0) continue;   // unchanged or in place: no block released
         int cap = vtab[seg_u[s]].cap;
         if (cap > 0) atomicAdd(&s_cnt[cap_class(cap)], 1);
     }
@@ -563,6 +679,12 @@ k_commit(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_ksta
     __syncthreads();
     for (long long s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
         int ncap = seg_ncap[s];
+        if (ncap == kInPlace) {
+            const int u = seg_u[s];
+            const int k = seg_kstart[s + 1] - seg_kstart[s];
+            vtab[u].deg += insert ? k : -k;
+            continue;
+        }
         if (ncap < 0) continue;
         int u = seg_u[s];
         int k = seg_kstart[s + 1] - seg_kstart[s];
@@ -733,9 +855,14 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     wv2.release();
     // 2. mark  (keys2 reused as the counter values)
     unsigned long long* val = keys2.get();
+    DevBuf<int32_t> apos, capos;   // insert: each entry's place in its old list
+    if (insert) {
+        apos.alloc(n, s);
+        capos.alloc(n, s);
+    }
     if (insert)
         HN_LAUNCH(k_mark_insert, grid_for(g, n, kB), kB, 0, s, keys.get(), n, L, flags, g->vtab,
-                  g->pool, val);
+                  g->pool, val, apos.get());
     else
         HN_LAUNCH(k_mark_erase, grid_for(g, n, kB), kB, 0, s, keys.get(), n, L, flags, g->vtab,
                   g->pool, val);
@@ -749,15 +876,17 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, val, scan.get(), (int)n, s));
         count_launch();
     }
-    DevBuf<int32_t> cdst(n, s), cseg(n, s), seg_u(n, s), seg_kstart(n + 1, s), seg_ncap(n, s);
+    DevBuf<int32_t> cdst(n, s), cseg(n, s), seg_u(n, s), seg_kstart(n + 1, s), seg_ncap(n, s),
+        seg_base(n, s);
     DevBuf<long long> seg_work(n + 1, s), seg_new_off(n, s), seg_old_off(n, s);
     long long* totals = g->d_scalar;
     DevBuf<uint32_t> cw;
     if (carry_w) cw.alloc(n, s);
     HN_LAUNCH(k_compact, grid_for(g, n, kB), kB, 0, s, keys.get(), val, scan.get(), n, L,
               cdst.get(), cseg.get(), seg_u.get(), seg_kstart.get(), totals,
-              (const uint32_t*)wv.get(), cw.get());
+              (const uint32_t*)wv.get(), cw.get(), (const int32_t*)apos.get(), capos.get());
     wv.release();
+    apos.release();
     keys2.release();
     scan.release();
     // 4. plan (weighted graphs keep every list on the tile path, which moves
@@ -766,8 +895,11 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     DevBuf<int32_t> big_list(n + 1, s);
     DevBuf<int> big_ctr(1, s);   // hubs listed
     HN_CUDA(cudaMemsetAsync(big_ctr.get(), 0, sizeof(int), s));
+    // weighted graphs move every touched list (the weights travel with it)
+    const bool in_place = !g->weighted && knob(kKnobUpdateInPlace) != 0;
     HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
-              insert, g->vtab, seg_work.get(), seg_ncap.get(), seg_old_off.get(), st, big_min,
+              insert, g->vtab, (const int32_t*)g->pool, (const int32_t*)cdst.get(), in_place,
+              seg_work.get(), seg_ncap.get(), seg_base.get(), seg_old_off.get(), st, big_min,
               big_list.get(), big_ctr.get());
     // 5. host plan (the one synchronisation of the batch)
     cudaEvent_t plan_ev = nullptr;   // profiled: the stream's idle time across the plan
@@ -817,7 +949,8 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     if (plan_ev) profile_end("host_plan_round_trip", s, plan_ev);
     // 6. assign blocks
     HN_LAUNCH(k_assign, grid_for(g, nseg, kB, 4), kB, 0, s, seg_ncap.get(), nseg, plan,
-              (long long* const*)g->d_fl, st, seg_new_off.get());
+              (long long* const*)g->d_fl, st, (const long long*)seg_old_off.get(),
+              seg_new_off.get());
     // 7. scatter-merge
     {
         ProfileScope ps("cub_scan_work", s);
@@ -860,17 +993,32 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
                       seg_u.get(), seg_kstart.get(), seg_old_off.get(), seg_new_off.get(),
                       cdst.get(), g->vtab, g->pool, (const int*)chunk_pre.get());
     }
+    // in-place vertices whose moved entries span tiles: at most one per
+    // tile boundary, and the work is at most nE entries
+    const long long span_cap = (g->nE + nseg) / Tile::TILE + 2;
+    DevBuf<int32_t> span_list(span_cap, s);
+    DevBuf<int> nspan(1, s);
+    HN_CUDA(cudaMemsetAsync(nspan.get(), 0, sizeof(int), s));
+    const long long grid_span = (long long)g->info.sms * 8;
     if (insert) {
         HN_LAUNCH(k_scatter_old<true>, grid_sc, kSB, 0, s, seg_work.get(), nseg,
                   seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  seg_old_off.get(), g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
-        HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(), totals,
-                  seg_u.get(), seg_kstart.get(), seg_new_off.get(), g->vtab, g->pool,
-                  (const uint32_t*)cw.get(), g->wpool);
+                  seg_old_off.get(), seg_ncap.get(), seg_base.get(), g->pool, splits.get(),
+                  (long long)splits.n - 1, g->wpool, span_list.get(), nspan.get(), span_cap);
+        HN_LAUNCH(k_inplace_span<true>, grid_span, kSpanWarps * 32, 0, s, span_list.get(),
+                  nspan.get(), seg_u.get(), seg_kstart.get(), seg_base.get(), seg_old_off.get(),
+                  cdst.get(), g->vtab, g->pool, span_cap);
+        HN_LAUNCH(k_scatter_new, grid_for(g, kept, kB), kB, 0, s, cdst.get(), cseg.get(),
+                  (const int32_t*)capos.get(), totals, seg_kstart.get(), seg_new_off.get(),
+                  g->pool, (const uint32_t*)cw.get(), g->wpool);
     } else {
         HN_LAUNCH(k_scatter_old<false>, grid_sc, kSB, 0, s, seg_work.get(),
                   nseg, seg_u.get(), seg_kstart.get(), seg_new_off.get(), cdst.get(),
-                  seg_old_off.get(), g->pool, splits.get(), (long long)splits.n - 1, g->wpool);
+                  seg_old_off.get(), seg_ncap.get(), seg_base.get(), g->pool, splits.get(),
+                  (long long)splits.n - 1, g->wpool, span_list.get(), nspan.get(), span_cap);
+        HN_LAUNCH(k_inplace_span<false>, grid_span, kSpanWarps * 32, 0, s, span_list.get(),
+                  nspan.get(), seg_u.get(), seg_kstart.get(), seg_base.get(), seg_old_off.get(),
+                  cdst.get(), g->vtab, g->pool, span_cap);
     }
     // 8. commit
     HN_LAUNCH(k_commit, grid_for(g, nseg, kB, 4), kB, 0, s, seg_u.get(), seg_kstart.get(),
@@ -1037,6 +1185,7 @@ int hn_insert(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
     HN_REQUIRE(b->g == g, "batch belongs to another graph");
     HN_REQUIRE((flags & ~(HN_DEDUP_BATCH | HN_DEDUP_GRAPH)) == 0, "unknown flags");
     require_owner(g);
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     run_update(g, b, flags, true, applied);
     HN_API_END
@@ -1048,6 +1197,7 @@ int hn_insert_count_triangles(hn_graph_t* g, hn_batch_t* b, int64_t* applied,
     HN_REQUIRE(g && b && new_triangles, "null argument");
     HN_REQUIRE(b->g == g, "batch belongs to another graph");
     require_owner(g);
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     unsigned long long t = 0;
     run_update(g, b, HN_DEDUP_BATCH | HN_DEDUP_GRAPH, true, applied, &t);
@@ -1061,6 +1211,7 @@ int hn_erase(hn_graph_t* g, hn_batch_t* b, unsigned flags, int64_t* applied) {
     HN_REQUIRE(b->g == g, "batch belongs to another graph");
     HN_REQUIRE((flags & ~HN_DEDUP_BATCH) == 0, "unknown flags");
     require_owner(g);
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     run_update(g, b, flags, false, applied);
     HN_API_END
@@ -1077,6 +1228,7 @@ int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int3
     if (inserted) *inserted = 0;
     if (erased) *erased = 0;
     if (n == 0) return HN_OK;
+    HandleUse use(g);
     HN_CUDA(cudaSetDevice(g->device));
     cudaStream_t s = g->stream;
     const int L = g->key_bits;

@@ -142,6 +142,14 @@ int hn_profile_report(char* buf, int64_t len);
  *                       (WHILE node, no host round trip per round); 0: one
  *                       host round trip per round, launches sized to the
  *                       frontier (0..1, 1)
+ *   update.big_min      old lists of at least this many entries (hubs) are
+ *                       moved in 4096-entry chunks by their own kernel
+ *                       (4..2^30, 2048)
+ *   update.in_place     1: a vertex whose block class does not change is
+ *                       updated inside its block, rewriting only its entries
+ *                       from the first one that moves (at most 2048 of
+ *                       them); 0: every touched vertex moves to a new block
+ *                       (0..1, 1)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);
@@ -191,6 +199,10 @@ int hn_graph_set_stream(hn_graph_t* g, void* stream);
  * host threads.  The reference has one HornetGraph and synchronous calls,
  * so concurrent queries on one resident graph have no counterpart there.
  * Updates go to the graph itself; a view rejects them (HN_ERR_STATE).
+ * Any handle, graph or view, serves one host thread at a time: a
+ * traversal, count or update called on a handle that another thread's call
+ * is using returns HN_ERR_STATE without touching it; concurrent queries
+ * use one view per thread.
  * While the graph is being updated no call may run on its views; after the
  * update, hn_graph_view_refresh takes the graph's new edge count (it waits
  * for the graph's stream).  hn_graph_destroy frees a view; a view must be

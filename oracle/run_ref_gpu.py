@@ -1,6 +1,7 @@
 """TEST INFRASTRUCTURE — times the reference's own GPU programs on this GPU.
 
-    python oracle/run_ref_gpu.py [out.json] [--scale 22]
+    python oracle/run_ref_gpu.py [out.json] [--scale 22] [--only bfs,tc,cc]
+    python oracle/run_ref_gpu.py [out.json] --only update [--scale 24]
 
 The programs are the reference's hornetsnest test drivers (BFSTest.cu,
 TriangleTest2.cu, CCTest.cu) with their algorithm sources, built as
@@ -23,7 +24,18 @@ written in the reference's GraphStd .bin format:
     BlockArray/BlockArray.i.cuh:150-153, HornetInitialize.i.cuh:126-129).
     A relabelled acyclic orientation counts every triangle once all the
     same, so the total is the graph's;
-  * CC (CC.cu) on the symmetric graph: its time.
+  * CC (CC.cu) on the symmetric graph: its time;
+  * update (`--only update`, scale 24 by default): gpu::Hornet::insert and
+    erase through this repository's driver oracle/ref_gpu_update.cu, on the
+    dynamic-update configuration's graph (R-MAT scale 24, edge factor 16,
+    seed 1, built with the library's device generator, which the CPU tests
+    pin bit-identical to the oracle's) and its ten batches (uniform and
+    R-MAT, 1K..10M directed entries, as bench.py's c3_batch makes them),
+    each inserted (both de-duplications) then erased (batch
+    de-duplication) in order on one graph.  The same sequence then runs
+    through this library, and the edge count after every call is compared:
+    equal counts after all twenty calls are a full-size check of the
+    update semantics against the reference's own GPU code.
 
 The .bin files are written by this repository's writer, which the CPU tests
 pin byte-identical to the reference's own writeBinary output.  Results
@@ -48,7 +60,9 @@ sys.path[:] = [ROOT] + [x for x in sys.path if os.path.abspath(x or ".") != HERE
 
 from oracle import oracle as O  # noqa: E402
 
-BIN = {k: os.path.join(HERE, "_ref", f"ref_gpu_{k}") for k in ("bfs", "triangle2", "cc")}
+BIN = {k: os.path.join(HERE, "_ref", f"ref_gpu_{k}")
+       for k in ("bfs", "triangle2", "cc", "update")}
+C3_BATCHES = [1_000, 10_000, 100_000, 1_000_000, 10_000_000]
 ANSI = re.compile(r"\x1b\[[0-9;]*m")
 
 
@@ -82,17 +96,124 @@ def relabel_first_vertex(g: "O.Csr") -> "O.Csr":
     return O.Csr(np.cumsum(off), (keys & 0xFFFFFFFF).astype(np.int32))
 
 
+def json_lines(text):
+    out = []
+    for line in text.splitlines():
+        line = line.strip()
+        if line.startswith("{"):
+            try:
+                out.append(json.loads(line))
+            except ValueError:
+                pass
+    return out
+
+
+def run_update(scale, out_path):
+    """The reference's GPU insert / erase and this library's on the same
+    graph and batch sequence; edge counts compared after every call."""
+    import ctypes
+    import types
+    import torch
+    import hornet_b200 as H
+    import bench
+    h0, csr = bench.make_graph_device(H, scale, 16, 1, 0)
+    nV_full = h0.nV()
+    off_full, adj_full = h0.getCSR()
+    del h0, csr
+    # The reference's HornetInit cannot start a block array with an isolated
+    # vertex: it sizes the array as 1 << ceil_log2(degree), and ceil_log2(0)
+    # asserts (hornet/include/Core/HornetInitialize/HornetInitialize.i.cuh:
+    # 126-129 -> xlib/include/Host/impl/Numeric.i.hpp:432), which the
+    # scale-24 graph's isolated vertices reach.  Both arms therefore run on
+    # the graph without its isolated vertices, ids compacted in order (lists
+    # stay sorted, the edges are the same); the batches are drawn on the
+    # compacted ids (R-MAT pairs with an isolated endpoint are dropped).
+    deg = np.diff(np.asarray(off_full, np.int64))
+    keep_v = deg > 0
+    newid = np.cumsum(keep_v) - 1
+    off = np.concatenate([[0], np.cumsum(deg[keep_v])]).astype(np.int64)
+    adj = newid[np.asarray(adj_full)].astype(np.int32)
+    del off_full, adj_full
+    nV = int(keep_v.sum())
+    rng = np.random.default_rng(2024)
+    gen = types.SimpleNamespace(gen_rmat_host=O.gen_rmat)
+    batches = []
+    for kind in ("uniform", "rmat"):
+        for i, b in enumerate(C3_BATCHES):
+            if kind == "uniform":
+                bs, bd = bench.c3_batch(gen, rng, kind, b, nV, scale, 77 + i)
+            else:
+                bs, bd = bench.c3_batch(gen, rng, kind, b, nV_full, scale, 77 + i)
+                ok = keep_v[bs] & keep_v[bd]
+                bs, bd = newid[bs[ok]].astype(np.int32), newid[bd[ok]].astype(np.int32)
+            batches.append((kind, bs, bd))
+    h = H.Hornet(H.HornetInit(nV, len(adj), off, adj, sorted_adjacency=True))
+    nE0 = h.nE()
+    res = {"graph": {"scale": scale, "nV_with_isolated": nV_full, "nV": nV, "nE": nE0,
+                     "note": "isolated vertices removed (ids compacted) for the reference's "
+                             "HornetInit"}}
+    with tempfile.TemporaryDirectory() as tmp:
+        gb = os.path.join(tmp, "g.bin")
+        H.write_bin(gb, off.astype(np.int32), adj)
+        files = []
+        for j, (kind, bs, bd) in enumerate(batches):
+            f = os.path.join(tmp, f"b{j}.bin")
+            with open(f, "wb") as fh:
+                fh.write(np.int64(len(bs)).tobytes())
+                fh.write(bs.astype("<i4").tobytes())
+                fh.write(bd.astype("<i4").tobytes())
+            files.append(f)
+        r = run([BIN["update"], gb] + files, 1800)
+        lines = json_lines(r.get("out", ""))
+        res["reference_run"] = {k: v for k, v in r.items() if k != "out"}
+        res["reference_out"] = r.get("out", "")[-3000:]
+    ref_rows = [x for x in lines if "batch" in x]
+    # this library, same sequence, timed the same way (CUDA events around
+    # each call, the graph's own stream)
+    stream = torch.cuda.Stream()
+    H.lib().hn_graph_set_stream(h.handle, ctypes.c_void_p(stream.cuda_stream))
+    ours, ours_ms = [], []
+    for kind, bs, bd in batches:
+        b = H.BatchUpdate(h, torch.from_numpy(bs).cuda(), torch.from_numpy(bd).cuda())
+        torch.cuda.synchronize()
+        ti = bench.event_time(stream, lambda: h.insert(b, True, True))
+        ne_i = h.nE()
+        te = bench.event_time(stream, lambda: h.erase(b, True))
+        ours.append((ne_i, h.nE()))
+        ours_ms.append((round(ti * 1e3, 4), round(te * 1e3, 4)))
+    rows = []
+    for j, (kind, bs, bd) in enumerate(batches):
+        row = {"kind": kind, "batch": len(bs), "ours_nE": list(ours[j]),
+               "ours_insert_ms": ours_ms[j][0], "ours_erase_ms": ours_ms[j][1]}
+        if j < len(ref_rows):
+            x = ref_rows[j]
+            row.update({"ref_insert_ms": x["insert_ms"], "ref_erase_ms": x["erase_ms"],
+                        "ref_nE": [x["nE_after_insert"], x["nE_after_erase"]]})
+            row["nE_equal"] = row["ref_nE"] == row["ours_nE"]
+        rows.append(row)
+    res["update"] = rows
+    res["all_nE_equal"] = len(ref_rows) == len(batches) and all(r.get("nE_equal") for r in rows)
+    with open(out_path, "w") as f:
+        json.dump(res, f, indent=1)
+    print(json.dumps({"rows": len(ref_rows), "all_nE_equal": res["all_nE_equal"],
+                      "ref_ms": [(r.get("ref_insert_ms"), r.get("ref_erase_ms")) for r in rows]}))
+
+
 def main():
     out_path = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith("--") else \
         "ref_gpu.json"
-    scale = 22
-    if "--scale" in sys.argv:
-        scale = int(sys.argv[sys.argv.index("--scale") + 1])
     only = sys.argv[sys.argv.index("--only") + 1].split(",") if "--only" in sys.argv else \
         ["bfs", "tc", "cc"]
-    for k, b in BIN.items():
-        if not os.path.exists(b):
-            raise SystemExit(f"{b} missing: make -C oracle ref_gpu")
+    scale = 24 if only == ["update"] else 22
+    if "--scale" in sys.argv:
+        scale = int(sys.argv[sys.argv.index("--scale") + 1])
+    need = {"bfs": "bfs", "tc": "triangle2", "cc": "cc", "update": "update"}
+    for k in only:
+        if not os.path.exists(BIN[need[k]]):
+            raise SystemExit(f"{BIN[need[k]]} missing: make -C oracle ref_gpu")
+    if only == ["update"]:
+        run_update(scale, out_path)
+        return
     import hornet_b200 as H   # only its .bin writer (pinned to the reference's bytes)
     s, d = O.gen_rmat(scale, 16 << scale, 1)
     g = O.build_csr_undirected(1 << scale, s, d)

@@ -688,6 +688,65 @@ def test_ktruss_round_drivers(device_rounds):
         H.tune_reset()
 
 
+@pytest.mark.parametrize("in_place", [1, 0])
+def test_in_place_updates_on_long_suffixes(in_place):
+    """Updates of vertices whose block class does not change rewrite their
+    list inside the block from the first entry that moves (update.in_place
+    1), or move it to a new block (0); both equal the oracle's multiset
+    model.  64 lists of 1,500 entries (block class 2048) beside an R-MAT
+    graph get batch entries below most of their values, so the moved parts
+    (up to ~1,500 entries) span scatter tiles and take the whole-vertex
+    path; a multigraph stage and an erase with batch duplicates exercise
+    the rank rule for equal entries in place; a last insert pushes some of
+    the lists past 2,048 entries (a class change, a new block)."""
+    rng = np.random.default_rng(21)
+    g = T.rmat_graph(14, 8, seed=3)
+    heads = np.arange(8000, 8064, dtype=np.int32)
+    hs = np.repeat(heads, 1500)
+    hd = np.concatenate([rng.choice(np.arange(1000, g.nV), 1500, replace=False)
+                         for _ in heads]).astype(np.int32)
+    g, _ = O.insert(g, hs, hd, 3)
+    try:
+        H.tune_set("update.in_place", in_place)
+        h = build(g)
+        # 1: small ids into the long lists (moved parts ~1,500) + random edges
+        s = np.concatenate([np.repeat(heads, 3), rng.integers(0, g.nV, 3000).astype(np.int32)])
+        d = np.concatenate([rng.integers(0, 500, 3 * len(heads)).astype(np.int32),
+                            rng.integers(0, g.nV, 3000).astype(np.int32)])
+        assert h.insert(H.BatchUpdate(h, s, d), True, True) == O.insert(g, s, d, 3)[1]
+        g, _ = O.insert(g, s, d, 3)
+        assert_same_graph(h, g)
+        # 2: a multigraph: existing entries of the long lists inserted again
+        es, ed = g.coo()
+        mine = np.nonzero((es >= 8000) & (es < 8064))[0]
+        pick = rng.choice(mine, 2000, replace=False)
+        h.insert(H.BatchUpdate(h, es[pick], ed[pick]), False, False)
+        g, _ = O.insert(g, es[pick], ed[pick], 0)
+        assert_same_graph(h, g)
+        # 3: erase with batch duplicates: some of the doubled entries lose one
+        # copy, some both
+        s = np.concatenate([es[pick[:800]], es[pick[:300]], es[rng.choice(mine, 500)]])
+        d = np.concatenate([ed[pick[:800]], ed[pick[:300]], ed[rng.choice(mine, 500)]])
+        assert h.erase(H.BatchUpdate(h, s, d), False) == O.erase(g, s, d, 0)[1]
+        g, _ = O.erase(g, s, d, 0)
+        assert_same_graph(h, g)
+        # 4: erase low entries (moved parts start near the front) with dedup
+        es, ed = g.coo()
+        low = np.nonzero((es >= 8000) & (es < 8064) & (ed < 3000))[0]
+        s, d = es[low], ed[low]
+        h.erase(H.BatchUpdate(h, s, d), True)
+        g, _ = O.erase(g, s, d, 1)
+        assert_same_graph(h, g)
+        # 5: some lists past 2,048 entries (class change) beside in-place ones
+        s = np.repeat(heads[:8], 1000)
+        d = rng.integers(0, g.nV, len(s)).astype(np.int32)
+        h.insert(H.BatchUpdate(h, s, d), True, True)
+        g, _ = O.insert(g, s, d, 3)
+        assert_same_graph(h, g)
+    finally:
+        H.tune_reset()
+
+
 @pytest.mark.parametrize("big_min", [2048, 4, 1 << 30])
 def test_updates_on_long_lists(big_min):
     """Insert and erase batches that reach long adjacency lists (a star with

@@ -154,8 +154,15 @@ def test_query_views_run_concurrently_and_reject_updates():
         d = H.BfsTopDown(v).run_multi([srcs[i]], direction_optimizing=bool(i & 1))[0][0]
         return d, H.TriangleCounting2(v).local(np.array([srcs[i]], np.int32))
 
+    def per_view(j):
+        # a handle serves one host thread at a time: thread j owns view j
+        return {i: one(i) for i in range(j, len(srcs), 3)}
+
     with ThreadPoolExecutor(3) as ex:
-        outs = list(ex.map(one, range(len(srcs))))
+        done = {}
+        for part in ex.map(per_view, range(3)):
+            done.update(part)
+    outs = [done[i] for i in range(len(srcs))]
     _, pv = O.tc(g, per_vertex=True)
     for s, (d, t) in zip(srcs, outs):
         np.testing.assert_array_equal(d, O.bfs(g, s)[0])
