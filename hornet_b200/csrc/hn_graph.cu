@@ -65,6 +65,7 @@ const KnobDef kKnobs[kNumKnobs] = {
     {"ktruss.device_rounds", 1, 0, 1, false},
     {"update.big_min", 2048, 4, 1 << 30, false},
     {"update.in_place", 1, 0, 1, false},
+    {"update.own_sort", 1, 0, 1, false},
 };
 std::atomic<long long> g_knob[kNumKnobs];
 // every knob starts at its default (static initialisation, in definition

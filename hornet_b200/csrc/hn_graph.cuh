@@ -140,6 +140,7 @@ enum Knob {
     kKnobKtDeviceRounds,
     kKnobUpdateBigMin,
     kKnobUpdateInPlace,
+    kKnobUpdateOwnSort,
     kNumKnobs
 };
 long long knob(Knob k);
@@ -221,6 +222,15 @@ struct hn_graph {
 };
 
 namespace hn {
+// Stable LSD radix sort of 64-bit keys by their low `bits` bits, carrying
+// optional 32-bit values (vals may be null); the *_alt buffers are scratch
+// of the same size, and on return keys / vals point at the sorted data.
+// A bounded device wait that gave up stores HN_ERR_TIMEOUT in *err (device
+// memory).  Defined in hn_sort.cu.
+void radix_sort_u64(hn_graph* g, unsigned long long*& keys, unsigned long long*& keys_alt,
+                    uint32_t*& vals, uint32_t*& vals_alt, long long n, int bits, int* err,
+                    cudaStream_t s);
+
 // Update entry points call this: a query view never changes the graph.
 inline void require_owner(const hn_graph* g) {
     if (g->parent) throw Error(HN_ERR_STATE, "a query view cannot update the graph");

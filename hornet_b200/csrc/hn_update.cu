@@ -8,7 +8,8 @@
 // (insert) or tail-refill of holes (erase), with >= 6 host round trips.
 //
 // Here (one host synchronisation per batch, to size the pool):
-//   1. pack (src,dst) into one key of 2*key_bits bits; radix sort;
+//   1. pack (src,dst) into one key of 2*key_bits bits; stable LSD radix sort
+//      (hn_sort.cu);
 //   2. mark: batch / graph duplicates (insert) or per-run deletions
 //      (erase) — graph membership by binary search in the SORTED adjacency;
 //   3. one scan of packed (kept, source-head) counters gives compacted
@@ -78,10 +79,16 @@ __global__ void k_pack(const int32_t* __restrict__ src, const int32_t* __restric
 __global__ void k_mark_insert(const unsigned long long* __restrict__ keys, long long n, int L,
                               unsigned flags, const VRec* __restrict__ vtab,
                               const int32_t* __restrict__ pool,
-                              unsigned long long* __restrict__ val, int32_t* __restrict__ apos) {
+                              unsigned long long* __restrict__ val, int32_t* __restrict__ apos,
+                              const AllocState* st) {
     const unsigned long long mask = (1ull << L) - 1;
+    const bool failed = st->error != 0;   // bad ids or a failed sort: the batch is refused
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
+        if (failed) {
+            val[i] = 0;
+            continue;
+        }
         unsigned long long k = keys[i];
         unsigned long long kp = i ? keys[i - 1] : ~0ull;
         bool first = (i == 0) || (k != kp);
@@ -103,14 +110,21 @@ __global__ void k_mark_insert(const unsigned long long* __restrict__ keys, long 
 // Erase marking: element i of a run of equal (u,x) deletes a copy iff its
 // rank in the run (after batch de-duplication) is below the graph
 // multiplicity c_g, so each run removes min(c_b, c_g) copies
-// (BatchUpdateKernels.cuh:263-300, :335-393).
+// (BatchUpdateKernels.cuh:263-300, :335-393).  apos[i] = the old list's
+// entries below x.
 __global__ void k_mark_erase(const unsigned long long* __restrict__ keys, long long n, int L,
                              unsigned flags, const VRec* __restrict__ vtab,
                              const int32_t* __restrict__ pool,
-                             unsigned long long* __restrict__ val) {
+                             unsigned long long* __restrict__ val, int32_t* __restrict__ apos,
+                             const AllocState* st) {
     const unsigned long long mask = (1ull << L) - 1;
+    const bool failed = st->error != 0;   // bad ids or a failed sort: the batch is refused
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
+        if (failed) {
+            val[i] = 0;
+            continue;
+        }
         unsigned long long k = keys[i];
         unsigned long long kp = i ? keys[i - 1] : ~0ull;
         bool first = (i == 0) || (k != kp);
@@ -128,6 +142,7 @@ __global__ void k_mark_erase(const unsigned long long* __restrict__ keys, long l
             long long cg = 0;
             if (lo < r.deg && a[lo] == x) cg = upper_bound_dev(a, (long long)r.deg, x) - lo;
             del = rank < cg;
+            apos[i] = (int32_t)lo;   // the old list's first copy of x
         }
         val[i] = ((unsigned long long)head << 32) | (unsigned long long)del;
     }
@@ -192,7 +207,7 @@ constexpr int kInPlaceMax = 2048;
 __global__ void __launch_bounds__(kB)
 k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
        const long long* __restrict__ totals, bool insert, const VRec* __restrict__ vtab,
-       const int32_t* __restrict__ pool, const int32_t* __restrict__ cdst, bool in_place,
+       const int32_t* __restrict__ capos, bool in_place,
        long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap,
        int32_t* __restrict__ seg_base, long long* __restrict__ seg_old_off, AllocState* st,
        int big_min, int32_t* __restrict__ big_list, int* __restrict__ nbig) {
@@ -216,10 +231,9 @@ k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart
             ncap = pow2_ceil(nd);
             bool here = in_place && !big && nd > 0 && ncap == r.cap;
             if (here) {
-                const int32_t b0 = cdst[k0];
-                const int32_t* a = pool + r.off;
-                base = insert ? (int)upper_bound_dev(a, (long long)r.deg, b0)
-                              : (int)lower_bound_dev(a, (long long)r.deg, b0);
+                // the smallest batch entry's place in the old list, recorded
+                // at marking
+                base = capos[k0];
                 here = r.deg - base <= kInPlaceMax;
             }
             if (here) {
@@ -834,7 +848,16 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         wv2.alloc(n, s);
         HN_CUDA(cudaMemcpyAsync(wv.get(), b->w, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
     }
-    {
+    if (knob(kKnobUpdateOwnSort)) {
+        unsigned long long* kc = keys.get();
+        unsigned long long* ka = keys2.get();
+        uint32_t* vc = carry_w ? wv.get() : nullptr;
+        uint32_t* va = carry_w ? wv2.get() : nullptr;
+        radix_sort_u64(g, kc, ka, vc, va, n, 2 * L, &st->error, s);
+        if (kc != keys.get()) std::swap(keys.p, keys2.p);
+        if (carry_w && vc != wv.get()) std::swap(wv.p, wv2.p);
+    } else {
+        // the library sort, kept for comparison (update.own_sort 0)
         ProfileScope ps("cub_sort_keys", s);
         cub::DoubleBuffer<unsigned long long> db(keys.get(), keys2.get());
         size_t tb = 0;
@@ -855,17 +878,15 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     wv2.release();
     // 2. mark  (keys2 reused as the counter values)
     unsigned long long* val = keys2.get();
-    DevBuf<int32_t> apos, capos;   // insert: each entry's place in its old list
-    if (insert) {
-        apos.alloc(n, s);
-        capos.alloc(n, s);
-    }
+    // each entry's place in its old list (insert: old entries <= it; erase:
+    // old entries below it), kept for the compacted entries
+    DevBuf<int32_t> apos(n, s), capos(n, s);
     if (insert)
         HN_LAUNCH(k_mark_insert, grid_for(g, n, kB), kB, 0, s, keys.get(), n, L, flags, g->vtab,
-                  g->pool, val, apos.get());
+                  g->pool, val, apos.get(), (const AllocState*)st);
     else
         HN_LAUNCH(k_mark_erase, grid_for(g, n, kB), kB, 0, s, keys.get(), n, L, flags, g->vtab,
-                  g->pool, val);
+                  g->pool, val, apos.get(), (const AllocState*)st);
     // 3. scan + compact
     DevBuf<unsigned long long> scan(n, s);
     {
@@ -898,7 +919,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     // weighted graphs move every touched list (the weights travel with it)
     const bool in_place = !g->weighted && knob(kKnobUpdateInPlace) != 0;
     HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
-              insert, g->vtab, (const int32_t*)g->pool, (const int32_t*)cdst.get(), in_place,
+              insert, g->vtab, (const int32_t*)capos.get(), in_place,
               seg_work.get(), seg_ncap.get(), seg_base.get(), seg_old_off.get(), st, big_min,
               big_list.get(), big_ctr.get());
     // 5. host plan (the one synchronisation of the batch)
@@ -911,8 +932,9 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
                             cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
     const int nbig = *(const int*)(g->h_scalar + 2);
-    if (g->h_alloc->error) {
+    if (const int e = g->h_alloc->error) {
         HN_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(int), s));
+        if (e == HN_ERR_TIMEOUT) throw Error(HN_ERR_TIMEOUT, "batch sort: a bounded wait gave up");
         throw Error(HN_ERR_INVALID, "batch vertex id outside [0, nV)");
     }
     const long long kept = g->h_scalar[0];
@@ -948,7 +970,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     }
     if (plan_ev) profile_end("host_plan_round_trip", s, plan_ev);
     // 6. assign blocks
-    HN_LAUNCH(k_assign, grid_for(g, nseg, kB, 4), kB, 0, s, seg_ncap.get(), nseg, plan,
+    HN_LAUNCH(k_assign, grid_for(g, nseg, kB), kB, 0, s, seg_ncap.get(), nseg, plan,
               (long long* const*)g->d_fl, st, (const long long*)seg_old_off.get(),
               seg_new_off.get());
     // 7. scatter-merge
@@ -1021,7 +1043,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
                   cdst.get(), g->vtab, g->pool, span_cap);
     }
     // 8. commit
-    HN_LAUNCH(k_commit, grid_for(g, nseg, kB, 4), kB, 0, s, seg_u.get(), seg_kstart.get(),
+    HN_LAUNCH(k_commit, grid_for(g, nseg, kB), kB, 0, s, seg_u.get(), seg_kstart.get(),
               seg_ncap.get(), seg_new_off.get(), nseg, insert, plan, (long long* const*)g->d_fl,
               st, g->vtab);
     for (int c = 0; c < kNumClasses; c++)
@@ -1047,11 +1069,23 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
 // the packed keys (ops carried as values), the last entry of each key's run
 // holds the op that decides the edge's final presence.  Packed scan value:
 // (erase << 32) | insert.
+__global__ void k_widen_ops(const unsigned char* __restrict__ ops, long long n,
+                            uint32_t* __restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = ops[i];
+}
+
 __global__ void k_net_mark(const unsigned long long* __restrict__ keys,
-                           const unsigned char* __restrict__ ops, long long n,
-                           unsigned long long* __restrict__ val) {
+                           const uint32_t* __restrict__ ops, long long n,
+                           unsigned long long* __restrict__ val, const AllocState* st) {
+    const bool failed = st->error != 0;   // bad ids or a failed sort: the run is refused
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
+        if (failed) {
+            val[i] = 0;
+            continue;
+        }
         const bool last = i == n - 1 || keys[i + 1] != keys[i];
         const unsigned long long ins = last && ops[i] != 0;
         const unsigned long long del = last && ops[i] == 0;
@@ -1250,24 +1284,23 @@ int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int3
     }
     AllocState* st = g->alloc;
     DevBuf<unsigned long long> keys((size_t)n, s), keys2((size_t)n, s);
-    DevBuf<unsigned char> ops2((size_t)n, s), ops1((size_t)n, s);
+    DevBuf<uint32_t> ops2((size_t)n, s), ops1((size_t)n, s);
     HN_CUDA(cudaMemsetAsync(st, 0, sizeof(AllocState), s));
     HN_LAUNCH(k_pack, grid_for(g, n, kB), kB, 0, s, d_src, d_dst, n, g->nV, L, keys.get(), st);
-    HN_CUDA(cudaMemcpyAsync(ops1.get(), d_ops, (size_t)n, cudaMemcpyDeviceToDevice, s));
+    HN_LAUNCH(k_widen_ops, grid_for(g, n, kB), kB, 0, s, d_ops, n, ops1.get());
     {
         // LSD radix sort is stable: equal keys keep their batch order
-        cub::DoubleBuffer<unsigned long long> dk(keys.get(), keys2.get());
-        cub::DoubleBuffer<unsigned char> dv(ops1.get(), ops2.get());
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, (int)n, 0, 2 * L, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, dk, dv, (int)n, 0, 2 * L, s));
-        count_launch();
-        if (dk.Current() != keys.get()) std::swap(keys.p, keys2.p);
-        if (dv.Current() != ops1.get()) std::swap(ops1.p, ops2.p);
+        unsigned long long* kc = keys.get();
+        unsigned long long* ka = keys2.get();
+        uint32_t* vc = ops1.get();
+        uint32_t* va = ops2.get();
+        radix_sort_u64(g, kc, ka, vc, va, n, 2 * L, &st->error, s);
+        if (kc != keys.get()) std::swap(keys.p, keys2.p);
+        if (vc != ops1.get()) std::swap(ops1.p, ops2.p);
     }
     unsigned long long* val = keys2.get();
-    HN_LAUNCH(k_net_mark, grid_for(g, n, kB), kB, 0, s, keys.get(), ops1.get(), n, val);
+    HN_LAUNCH(k_net_mark, grid_for(g, n, kB), kB, 0, s, keys.get(), ops1.get(), n, val,
+              (const AllocState*)st);
     DevBuf<unsigned long long> scan((size_t)n, s);
     {
         size_t tb = 0;
@@ -1286,8 +1319,9 @@ int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int3
                             cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaMemcpyAsync(g->h_alloc, st, sizeof(AllocState), cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
-    if (g->h_alloc->error) {
+    if (const int e = g->h_alloc->error) {
         HN_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(int), s));
+        if (e == HN_ERR_TIMEOUT) throw Error(HN_ERR_TIMEOUT, "batch sort: a bounded wait gave up");
         throw Error(HN_ERR_INVALID, "batch vertex id outside [0, nV)");
     }
     bi.n = g->h_scalar[0];

@@ -150,6 +150,8 @@ int hn_profile_report(char* buf, int64_t len);
  *                       from the first one that moves (at most 2048 of
  *                       them); 0: every touched vertex moves to a new block
  *                       (0..1, 1)
+ *   update.own_sort     1: the batch keys are sorted by this library's LSD
+ *                       radix sort; 0: by CUB's DeviceRadixSort (0..1, 1)
  * hn_tune_name(i) enumerates the names (NULL past the last one). */
 int hn_tune_set(const char* name, int64_t value);
 int hn_tune_get(const char* name, int64_t* value);
