@@ -193,9 +193,10 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
 // BatchUpdateKernels.cuh:150-198) is updated in place (seg_ncap = kInPlace):
 // only the part of its list from the first entry that moves, [base, deg),
 // is rewritten (insert: base = the old entries <= the smallest batch entry;
-// erase: base = the old entries below the smallest deleted one), and only
-// when that part has at most kInPlaceMax entries, so that one warp can stage
-// it.  Other vertices move to a new block (seg_ncap = new capacity, 0 for
+// erase: base = the old entries below the smallest deleted one); a list
+// moved by the tiles only when that part has at most kInPlaceMax entries,
+// so that one warp can stage it, a hub only when it has at most kHubSnap
+// batch entries (the slots snapshotted per chunk boundary).  Other vertices move to a new block (seg_ncap = new capacity, 0 for
 // an emptied list, -1 for a vertex without batch entries) and their whole
 // list is the work.  seg_work[s] = entries the scatter moves (0 for hubs,
 // which k_scatter_big moves).  The per-class counts are gathered in shared
@@ -203,6 +204,8 @@ __global__ void k_compact(const unsigned long long* __restrict__ keys,
 // the few popular classes).
 constexpr int kInPlace = -2;
 constexpr int kInPlaceMax = 2048;
+constexpr int kBigChunk = 4096;       // hub lists move in chunks of this many entries
+constexpr int kHubSnap = 256;         // most batch entries of a hub updated in place
 
 __global__ void __launch_bounds__(kB)
 k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart,
@@ -210,7 +213,8 @@ k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart
        const int32_t* __restrict__ capos, bool in_place,
        long long* __restrict__ seg_work, int32_t* __restrict__ seg_ncap,
        int32_t* __restrict__ seg_base, long long* __restrict__ seg_old_off, AllocState* st,
-       int big_min, int32_t* __restrict__ big_list, int* __restrict__ nbig) {
+       int big_min, int32_t* __restrict__ big_list, int* __restrict__ nbig,
+       unsigned long long* __restrict__ snap_words) {
     __shared__ int s_need[kNumClasses], s_push[kNumClasses];
     for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_need[c] = s_push[c] = 0;
     __syncthreads();
@@ -229,12 +233,19 @@ k_plan(const int32_t* __restrict__ seg_u, const int32_t* __restrict__ seg_kstart
         if (k > 0) {
             int nd = insert ? r.deg + k : r.deg - k;
             ncap = pow2_ceil(nd);
-            bool here = in_place && !big && nd > 0 && ncap == r.cap;
+            bool here = in_place && nd > 0 && ncap == r.cap && (!big || k <= kHubSnap);
             if (here) {
                 // the smallest batch entry's place in the old list, recorded
                 // at marking
                 base = capos[k0];
-                here = r.deg - base <= kInPlaceMax;
+                if (big) {
+                    // hub chunk boundaries inside the moved part keep k
+                    // slots each in the snapshot
+                    const int nch = (r.deg - base + kBigChunk - 1) / kBigChunk;
+                    if (nch > 1) atomicAdd(snap_words, (unsigned long long)(nch - 1) * k);
+                } else {
+                    here = r.deg - base <= kInPlaceMax;
+                }
             }
             if (here) {
                 ncap = kInPlace;
@@ -535,116 +546,198 @@ k_inplace_span(const int32_t* __restrict__ span_list, const int* __restrict__ ns
 // shift for all its entries (insert: + the batch entries below it; erase:
 // - the deleted entries below it), so it is moved as a block: 16-byte
 // loads into shared memory, 16-byte stores at the shifted place (scalar
-// stores at the unaligned ends).  A chunk with batch entries inside uses the
-// per-entry rule of k_scatter_old on the few entries that fall in it.  The
-// hubs' chunks are numbered through an exclusive scan of their chunk counts
-// (chunk_pre, nbig + 1 entries), and CTAs take chunk numbers round-robin.
-constexpr int kBigChunk = 4096;
+// stores at the unaligned ends).  A chunk with batch entries inside places
+// each entry by the merge rule, with the batch entries it needs staged in
+// shared memory.  The hubs' chunks are numbered through an exclusive scan
+// of their chunk counts, and CTAs take chunk numbers round-robin.
+//
+// A hub whose block class stays and that has at most kHubSnap batch entries
+// is updated in place, its chunks covering only the moved part [base, deg).
+// A chunk stages all its entries in shared memory before it writes, but a
+// neighbouring chunk (another CTA) may write into its range first: on an
+// insert an entry moves right by at most k (the hub's batch entries), so
+// chunk c writes into at most the first k slots of chunk c+1; on an erase
+// it moves left by at most k, into the last k slots of chunk c-1.  Those k
+// slots of every chunk boundary are copied to a snapshot (k_big_snap)
+// before any chunk moves, and the chunk whose slots they are reads them
+// from there.  The erase rule for equal entries uses the old list's first
+// copy of the value, recorded at marking, instead of reading old slots
+// that may already be overwritten.  Packed per-hub prefix (chunk_pre):
+// high 32 bits chunks, low 32 bits snapshot slots.
+
+struct BigHub {   // one hub as the chunk kernels see it
+    long long old_off, new_off;
+    int deg, k0, nb, base, nch;
+    bool in_place;
+};
+
+__device__ __forceinline__ BigHub big_hub(int sg, const int32_t* seg_u, const int32_t* seg_kstart,
+                                          const int32_t* seg_ncap, const int32_t* seg_base,
+                                          const long long* seg_old_off,
+                                          const long long* seg_new_off, const VRec* vtab) {
+    BigHub h;
+    h.deg = vtab[seg_u[sg]].deg;   // the old degree: the commit runs later
+    h.k0 = seg_kstart[sg];
+    h.nb = seg_kstart[sg + 1] - h.k0;
+    h.in_place = seg_ncap[sg] == kInPlace;
+    h.base = h.in_place ? seg_base[sg] : 0;
+    h.old_off = seg_old_off[sg];
+    h.new_off = seg_new_off[sg];
+    h.nch = (h.deg - h.base + kBigChunk - 1) / kBigChunk;
+    return h;
+}
 
 __global__ void k_big_chunks(const int32_t* __restrict__ big_list, int nbig,
-                             const int32_t* __restrict__ seg_u, const VRec* __restrict__ vtab,
-                             int* __restrict__ nch) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nbig; i += gridDim.x * blockDim.x)
-        nch[i] = i < nbig ? (vtab[seg_u[big_list[i]]].deg + kBigChunk - 1) / kBigChunk : 0;
+                             const int32_t* __restrict__ seg_u,
+                             const int32_t* __restrict__ seg_kstart,
+                             const int32_t* __restrict__ seg_ncap,
+                             const int32_t* __restrict__ seg_base,
+                             const long long* __restrict__ seg_old_off,
+                             const long long* __restrict__ seg_new_off,
+                             const VRec* __restrict__ vtab, unsigned long long* __restrict__ pre) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= nbig; i += gridDim.x * blockDim.x) {
+        unsigned long long v = 0;
+        if (i < nbig) {
+            const BigHub h = big_hub(big_list[i], seg_u, seg_kstart, seg_ncap, seg_base,
+                                     seg_old_off, seg_new_off, vtab);
+            const unsigned long long snaps =
+                h.in_place && h.nch > 1 ? (unsigned long long)(h.nch - 1) * h.nb : 0;
+            v = ((unsigned long long)h.nch << 32) | snaps;
+        }
+        pre[i] = v;
+    }
+}
+
+// The hub and chunk of global chunk number q: last i with pre[i].chunks <= q.
+__device__ __forceinline__ int big_hub_of(const unsigned long long* pre, int nbig, int q) {
+    int lo = 0, hi = nbig;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if ((int)(pre[mid] >> 32) <= q) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Snapshot of every in-place hub's chunk boundaries: boundary c (between
+// chunks c and c+1, at old slot r1 = base + (c+1) * kBigChunk) keeps k slots:
+// insert [r1, r1 + k) clipped to the list, erase [r1 - k, r1).
+template <bool INSERT>
+__global__ void k_big_snap(const int32_t* __restrict__ big_list, int nbig,
+                           const int32_t* __restrict__ seg_u,
+                           const int32_t* __restrict__ seg_kstart,
+                           const int32_t* __restrict__ seg_ncap,
+                           const int32_t* __restrict__ seg_base,
+                           const long long* __restrict__ seg_old_off,
+                           const long long* __restrict__ seg_new_off,
+                           const VRec* __restrict__ vtab, const unsigned long long* __restrict__ pre,
+                           const int32_t* __restrict__ pool, int32_t* __restrict__ snap) {
+    // a thread per chunk: a boundary keeps only k (<= kHubSnap) slots
+    const int total = (int)(pre[nbig] >> 32);
+    for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += gridDim.x * blockDim.x) {
+        const int i = big_hub_of(pre, nbig, q);
+        const int c = q - (int)(pre[i] >> 32);
+        const BigHub h = big_hub(big_list[i], seg_u, seg_kstart, seg_ncap, seg_base, seg_old_off,
+                                 seg_new_off, vtab);
+        if (!h.in_place || c + 1 >= h.nch) continue;   // no boundary after this chunk
+        const long long r1 = (long long)h.base + (long long)(c + 1) * kBigChunk;
+        int32_t* out = snap + (pre[i] & 0xFFFFFFFFull) + (long long)c * h.nb;
+        for (int t = 0; t < h.nb; t++) {
+            const long long r = INSERT ? r1 + t : r1 - h.nb + t;
+            if (r < h.deg) out[t] = pool[h.old_off + r];
+        }
+    }
 }
 
 template <bool INSERT>
 __global__ void __launch_bounds__(kSB)
 k_scatter_big(const int32_t* __restrict__ big_list, int nbig, const int32_t* __restrict__ seg_u,
-              const int32_t* __restrict__ seg_kstart, const long long* __restrict__ seg_old_off,
+              const int32_t* __restrict__ seg_kstart, const int32_t* __restrict__ seg_ncap,
+              const int32_t* __restrict__ seg_base, const long long* __restrict__ seg_old_off,
               const long long* __restrict__ seg_new_off, const int32_t* __restrict__ cdst,
-              const VRec* __restrict__ vtab, int32_t* __restrict__ pool,
-              const int* __restrict__ chunk_pre) {
-    __shared__ __align__(16) int32_t sbuf[kBigChunk];
-    const int total = chunk_pre[nbig];
+              const int32_t* __restrict__ capos, const VRec* __restrict__ vtab,
+              int32_t* __restrict__ pool, const unsigned long long* __restrict__ pre,
+              const int32_t* __restrict__ snap) {
+    __shared__ __align__(16) int32_t sA[kBigChunk];   // the chunk's old entries
+    __shared__ int32_t sB[kBigChunk];                 // the batch entries inside it
+    const int total = (int)(pre[nbig] >> 32);
     for (int q = blockIdx.x; q < total; q += gridDim.x) {
-        // the hub of chunk q: last i with chunk_pre[i] <= q (uniform in the CTA)
-        int lo_i = 0, hi_i = nbig;
-        while (hi_i - lo_i > 1) {
-            const int mid = (lo_i + hi_i) >> 1;
-            if (chunk_pre[mid] <= q) lo_i = mid; else hi_i = mid;
+        const int i = big_hub_of(pre, nbig, q);   // uniform in the CTA
+        const int c = q - (int)(pre[i] >> 32);
+        const BigHub h = big_hub(big_list[i], seg_u, seg_kstart, seg_ncap, seg_base,
+                                 seg_old_off, seg_new_off, vtab);
+        const int32_t* B = cdst + h.k0;
+        const int32_t* A = pool + h.old_off;
+        const int r0 = h.base + c * kBigChunk;
+        const int n = h.deg - r0 < kBigChunk ? h.deg - r0 : kBigChunk;
+        // stage the chunk (in place: the slots a neighbour may overwrite
+        // come from the snapshot)
+        int snap_lo = 0, snap_hi = 0;   // chunk-relative slots read from snap
+        const int32_t* sn = nullptr;
+        if (h.in_place) {
+            const long long sbase = (long long)(pre[i] & 0xFFFFFFFFull);
+            if (INSERT && c > 0) {
+                snap_hi = h.nb < n ? h.nb : n;
+                sn = snap + sbase + (long long)(c - 1) * h.nb;
+            } else if (!INSERT && c + 1 < h.nch) {
+                snap_lo = n - h.nb;
+                snap_hi = n;
+                sn = snap + sbase + (long long)c * h.nb - snap_lo;
+            }
         }
-        const int i = lo_i, c = q - chunk_pre[lo_i];
-        const int sg = big_list[i];
-        const int deg = vtab[seg_u[sg]].deg;
-        const long long old_off = seg_old_off[sg], new_off = seg_new_off[sg];
-        const int k0 = seg_kstart[sg], nb = seg_kstart[sg + 1] - k0;
-        const int32_t* B = cdst + k0;
-        const int32_t* A = pool + old_off;
-        const int r0 = c * kBigChunk;
-        const int n = deg - r0 < kBigChunk ? deg - r0 : kBigChunk;
-        const int32_t a_lo = A[r0], a_hi = A[r0 + n - 1];
-        const int lo = lower_bound32(B, nb, a_lo);   // batch entries below the chunk
-        const int hi = upper_bound32(B, nb, a_hi);   // ... and up to its last entry
+        if ((((h.old_off + r0) & 3) == 0)) {
+            const int4* a4 = reinterpret_cast<const int4*>(A + r0);
+            for (int v = threadIdx.x; v < n / 4; v += kSB)
+                reinterpret_cast<int4*>(sA)[v] = __ldcs(a4 + v);
+            for (int v = (n & ~3) + threadIdx.x; v < n; v += kSB) sA[v] = A[r0 + v];
+        } else {
+            for (int v = threadIdx.x; v < n; v += kSB) sA[v] = A[r0 + v];
+        }
+        __syncthreads();
+        for (int v = snap_lo + threadIdx.x; v < snap_hi; v += kSB) sA[v] = sn[v];
+        __syncthreads();
+        const int lo = lower_bound32(B, h.nb, sA[0]);       // batch entries below the chunk
+        const int hi = upper_bound32(B, h.nb, sA[n - 1]);   // ... and up to its last entry
+        const long long out0 = h.new_off + r0;             // the chunk's slot before the shift
         if (lo == hi) {
             // one shift for the whole chunk
-            const long long d0 = new_off + r0 + (INSERT ? lo : -lo);
-            if ((old_off & 3) == 0) {
-                const int4* a4 = reinterpret_cast<const int4*>(A + r0);
-                for (int v = threadIdx.x; v < n / 4; v += kSB)
-                    reinterpret_cast<int4*>(sbuf)[v] = __ldcs(a4 + v);
-                for (int v = (n & ~3) + threadIdx.x; v < n; v += kSB) sbuf[v] = A[r0 + v];
-            } else {
-                for (int v = threadIdx.x; v < n; v += kSB) sbuf[v] = A[r0 + v];
-            }
-            __syncthreads();
+            const long long d0 = out0 + (INSERT ? lo : -lo);
             const int lead = (int)((4 - (d0 & 3)) & 3) < n ? (int)((4 - (d0 & 3)) & 3) : n;
-            if (threadIdx.x < lead) pool[d0 + threadIdx.x] = sbuf[threadIdx.x];
+            if (threadIdx.x < lead) pool[d0 + threadIdx.x] = sA[threadIdx.x];
             const int nq = (n - lead) / 4;
             int4* o4 = reinterpret_cast<int4*>(pool + d0 + lead);
-            for (int q = threadIdx.x; q < nq; q += kSB) {
-                const int b = lead + 4 * q;
-                o4[q] = make_int4(sbuf[b], sbuf[b + 1], sbuf[b + 2], sbuf[b + 3]);
+            for (int t = threadIdx.x; t < nq; t += kSB) {
+                const int b = lead + 4 * t;
+                o4[t] = make_int4(sA[b], sA[b + 1], sA[b + 2], sA[b + 3]);
             }
-            for (int v = lead + 4 * nq + threadIdx.x; v < n; v += kSB) pool[d0 + v] = sbuf[v];
+            for (int v = lead + 4 * nq + threadIdx.x; v < n; v += kSB) pool[d0 + v] = sA[v];
         } else {
-            // batch entries inside the chunk: the per-entry rule on [lo, hi),
-            // searched in shared memory when they fit there; each thread
-            // takes four consecutive entries of the old list
+            // batch entries inside the chunk: the merge rule on [lo, hi),
+            // searched in shared memory when they fit there
             const int m = hi - lo;
             const bool staged = m <= kBigChunk;   // uniform in the CTA
-            if (staged) {
-                for (int v = threadIdx.x; v < m; v += kSB) sbuf[v] = B[lo + v];
-                __syncthreads();
-            }
-            const int32_t* Bn = staged ? sbuf : B + lo;
-            const bool vec = (old_off & 3) == 0;
-            for (int v4 = threadIdx.x; 4 * v4 < n; v4 += kSB) {
-                const int rb = r0 + 4 * v4;
-                int32_t xs[4];
-                if (vec && 4 * v4 + 4 <= n) {
-                    const int4 q = __ldcs(reinterpret_cast<const int4*>(A + rb));
-                    xs[0] = q.x; xs[1] = q.y; xs[2] = q.z; xs[3] = q.w;
+            if (staged)
+                for (int v = threadIdx.x; v < m; v += kSB) sB[v] = B[lo + v];
+            __syncthreads();
+            const int32_t* Bn = staged ? sB : B + lo;
+            for (int v = threadIdx.x; v < n; v += kSB) {
+                const int32_t x = sA[v];
+                const long long r = (long long)r0 + v;   // old slot in the list
+                if (INSERT) {
+                    pool[h.new_off + r + lo + lower_bound32(Bn, m, x)] = x;
                 } else {
-#pragma unroll
-                    for (int t = 0; t < 4; t++) xs[t] = 4 * v4 + t < n ? A[rb + t] : 0;
-                }
-#pragma unroll
-                for (int t = 0; t < 4; t++) {
-                    if (4 * v4 + t >= n) break;
-                    const int r = rb + t;
-                    const int32_t x = xs[t];
-                    if (INSERT) {
-                        pool[new_off + r + lo + lower_bound32(Bn, m, x)] = x;
-                    } else {
-                        const int ubl = upper_bound32(Bn, m, x);
-                        int lbl = ubl;
-                        if (ubl > 0 && Bn[ubl - 1] == x) lbl = lower_bound32(Bn, ubl, x);
-                        const int cnt = ubl - lbl;   // copies of x this batch deletes
-                        bool keep = true;
-                        if (cnt > 0) {
-                            // rank of this copy among the equal values of the old list
-                            long long first = r;
-                            if (r > 0 && A[r - 1] == x)
-                                first = lower_bound_dev(A, (long long)r, x);
-                            keep = (r - first) >= cnt;
-                        }
-                        if (keep) pool[new_off + r - (lo + ubl)] = x;
-                    }
+                    const int ubl = upper_bound32(Bn, m, x);
+                    int lbl = ubl;
+                    if (ubl > 0 && Bn[ubl - 1] == x) lbl = lower_bound32(Bn, ubl, x);
+                    const int cnt = ubl - lbl;   // copies of x this batch deletes
+                    // the first cnt copies of x go: keep this one if its rank
+                    // among the old copies (from the first copy's slot,
+                    // recorded at marking) is at least cnt
+                    const bool keep = cnt == 0 || r - capos[h.k0 + lo + lbl] >= cnt;
+                    if (keep) pool[h.new_off + r - (lo + ubl)] = x;
                 }
             }
         }
-        __syncthreads();   // sbuf is reused by the next chunk
+        __syncthreads();   // sA / sB are restaged by the next chunk
     }
 }
 
@@ -914,24 +1007,25 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     // the weights with their neighbours)
     const int big_min = g->weighted ? INT_MAX : (int)knob(kKnobUpdateBigMin);
     DevBuf<int32_t> big_list(n + 1, s);
-    DevBuf<int> big_ctr(1, s);   // hubs listed
-    HN_CUDA(cudaMemsetAsync(big_ctr.get(), 0, sizeof(int), s));
+    DevBuf<unsigned long long> big_ctr(2, s);   // [0] hubs listed, [1] snapshot slots
+    HN_CUDA(cudaMemsetAsync(big_ctr.get(), 0, 2 * sizeof(unsigned long long), s));
     // weighted graphs move every touched list (the weights travel with it)
     const bool in_place = !g->weighted && knob(kKnobUpdateInPlace) != 0;
     HN_LAUNCH(k_plan, grid_for(g, n + 1, kB), kB, 0, s, seg_u.get(), seg_kstart.get(), totals,
               insert, g->vtab, (const int32_t*)capos.get(), in_place,
               seg_work.get(), seg_ncap.get(), seg_base.get(), seg_old_off.get(), st, big_min,
-              big_list.get(), big_ctr.get());
+              big_list.get(), (int*)big_ctr.get(), big_ctr.get() + 1);
     // 5. host plan (the one synchronisation of the batch)
     cudaEvent_t plan_ev = nullptr;   // profiled: the stream's idle time across the plan
     if (g_profiling) profile_begin(s, &plan_ev);
     HN_CUDA(cudaMemcpyAsync(g->h_scalar, totals, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
                             s));
     HN_CUDA(cudaMemcpyAsync(g->h_alloc, st, sizeof(AllocState), cudaMemcpyDeviceToHost, s));
-    HN_CUDA(cudaMemcpyAsync((int*)(g->h_scalar + 2), big_ctr.get(), sizeof(int),
+    HN_CUDA(cudaMemcpyAsync(g->h_scalar + 2, big_ctr.get(), 2 * sizeof(unsigned long long),
                             cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
     const int nbig = *(const int*)(g->h_scalar + 2);
+    const long long snap_words = g->h_scalar[3];
     if (const int e = g->h_alloc->error) {
         HN_CUDA(cudaMemsetAsync(&st->error, 0, sizeof(int), s));
         if (e == HN_ERR_TIMEOUT) throw Error(HN_ERR_TIMEOUT, "batch sort: a bounded wait gave up");
@@ -990,11 +1084,13 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
     const long long grid_sc = (long long)g->info.sms * kScatterCtas;
     DevBuf<long long> splits;
     lb_splits(g, seg_work.get(), nseg, g->nE, Tile::TILE, splits);
-    DevBuf<int> chunk_pre;
+    DevBuf<unsigned long long> chunk_pre;
+    DevBuf<int32_t> snap;
     if (nbig > 0) {
         chunk_pre.alloc((size_t)nbig + 1, s);
         HN_LAUNCH(k_big_chunks, grid_for(g, (long long)nbig + 1, kB), kB, 0, s, big_list.get(),
-                  nbig, seg_u.get(), g->vtab, chunk_pre.get());
+                  nbig, seg_u.get(), seg_kstart.get(), seg_ncap.get(), seg_base.get(),
+                  seg_old_off.get(), seg_new_off.get(), g->vtab, chunk_pre.get());
         {
             ProfileScope ps("cub_scan_big", s);
             size_t tb = 0;
@@ -1006,14 +1102,33 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
             count_launch();
         }
         const long long grid_big = (long long)g->info.sms * 8;
+        if (snap_words > 0) {
+            snap.alloc((size_t)snap_words, s);
+            const long long grid_snap = grid_for(g, nbig * 8ll, kB);   // ~8 chunks a hub
+            if (insert)
+                HN_LAUNCH(k_big_snap<true>, grid_snap, kB, 0, s, big_list.get(), nbig, seg_u.get(),
+                          seg_kstart.get(), seg_ncap.get(), seg_base.get(), seg_old_off.get(),
+                          seg_new_off.get(), g->vtab, (const unsigned long long*)chunk_pre.get(),
+                          (const int32_t*)g->pool, snap.get());
+            else
+                HN_LAUNCH(k_big_snap<false>, grid_snap, kB, 0, s, big_list.get(), nbig,
+                          seg_u.get(), seg_kstart.get(), seg_ncap.get(), seg_base.get(),
+                          seg_old_off.get(), seg_new_off.get(), g->vtab,
+                          (const unsigned long long*)chunk_pre.get(), (const int32_t*)g->pool,
+                          snap.get());
+        }
         if (insert)
             HN_LAUNCH(k_scatter_big<true>, grid_big, kSB, 0, s, big_list.get(), nbig, seg_u.get(),
-                      seg_kstart.get(), seg_old_off.get(), seg_new_off.get(), cdst.get(),
-                      g->vtab, g->pool, (const int*)chunk_pre.get());
+                      seg_kstart.get(), seg_ncap.get(), seg_base.get(), seg_old_off.get(),
+                      seg_new_off.get(), cdst.get(), (const int32_t*)capos.get(), g->vtab,
+                      g->pool, (const unsigned long long*)chunk_pre.get(),
+                      (const int32_t*)snap.get());
         else
             HN_LAUNCH(k_scatter_big<false>, grid_big, kSB, 0, s, big_list.get(), nbig,
-                      seg_u.get(), seg_kstart.get(), seg_old_off.get(), seg_new_off.get(),
-                      cdst.get(), g->vtab, g->pool, (const int*)chunk_pre.get());
+                      seg_u.get(), seg_kstart.get(), seg_ncap.get(), seg_base.get(),
+                      seg_old_off.get(), seg_new_off.get(), cdst.get(),
+                      (const int32_t*)capos.get(), g->vtab, g->pool,
+                      (const unsigned long long*)chunk_pre.get(), (const int32_t*)snap.get());
     }
     // in-place vertices whose moved entries span tiles: at most one per
     // tile boundary, and the work is at most nE entries

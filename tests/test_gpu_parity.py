@@ -747,6 +747,50 @@ def test_in_place_updates_on_long_suffixes(in_place):
         H.tune_reset()
 
 
+@pytest.mark.parametrize("in_place", [1, 0])
+def test_in_place_hub_updates(in_place):
+    """A hub (20,000 leaves, then a run of 5,000 copies of one neighbour that
+    spans chunk boundaries) updated with at most 256 batch entries at a
+    time keeps its block and is rewritten chunk by chunk in place (the slots
+    a neighbouring chunk may overwrite first come from the boundary
+    snapshot), or moved to a new block (update.in_place 0); both equal the
+    oracle's multiset model.  Batches: entries spread over every chunk,
+    entries only at the front (the later chunks move as blocks), erasing
+    three copies of the long run (the first-copy rule across chunks), and
+    random erases."""
+    rng = np.random.default_rng(33)
+    n_star = 20001
+    star = O.build_csr_undirected(n_star, np.zeros(n_star - 1, np.int32),
+                                  np.arange(1, n_star, dtype=np.int32))
+    g, _ = T.disjoint_union([star, T.rmat_graph(11, 8, seed=2)])
+    g, _ = O.insert(g, np.zeros(5000, np.int32), np.full(5000, 12345, np.int32), 0)
+    try:
+        H.tune_set("update.in_place", in_place)
+        h = build(g)
+        assert_same_graph(h, g)
+        holes = rng.choice(np.arange(1, n_star, dtype=np.int32), 150, replace=False)
+        steps = [
+            ("erase", holes, True),                                    # spread over the chunks
+            ("insert", np.concatenate([holes, rng.integers(n_star, g.nV, 50).astype(np.int32)]),
+             (True, True)),                                            # spread again
+            ("insert", rng.integers(1, 40, 10).astype(np.int32), (False, False)),   # front only
+            ("erase", np.full(3, 12345, np.int32), False),             # the long run
+            ("insert", np.full(7, 12345, np.int32), (False, False)),
+            ("erase", np.array([12345] * 5 + [3, 3], np.int32), False),
+        ]
+        for kind, d, flags in steps:
+            src = np.zeros(len(d), np.int32)
+            if kind == "insert":
+                h.insert(H.BatchUpdate(h, src, d), *flags)
+                g, _ = O.insert(g, src, d, (1 if flags[0] else 0) | (2 if flags[1] else 0))
+            else:
+                h.erase(H.BatchUpdate(h, src, d), flags)
+                g, _ = O.erase(g, src, d, 1 if flags else 0)
+            assert_same_graph(h, g)
+    finally:
+        H.tune_reset()
+
+
 @pytest.mark.parametrize("big_min", [2048, 4, 1 << 30])
 def test_updates_on_long_lists(big_min):
     """Insert and erase batches that reach long adjacency lists (a star with
