@@ -108,8 +108,11 @@ class GraphBatch:
         total = ctypes.c_uint64()
         _check(lib().hn_tc_owner(self.hornet.handle, ctypes.c_void_p(per_vertex.data_ptr()),
                                  HN_MEM_DEVICE, ctypes.byref(total)))
-        csum = torch.cumsum(per_vertex, 0)
-        ends = torch.as_tensor(self.bases + self.sizes - 1, device=per_vertex.device)
-        at_end = csum[ends]
-        prev = torch.cat([at_end.new_zeros(1), at_end[:-1]])
-        return at_end - prev, total.value
+        off = np.ascontiguousarray(np.concatenate([self.bases, self.bases[-1:] + self.sizes[-1:]]),
+                                   np.int64)
+        out = torch.empty(self.n_graphs, dtype=torch.int64, device=per_vertex.device)
+        _check(lib().hn_segment_sum_u64(self.hornet.handle,
+                                        ctypes.c_void_p(per_vertex.data_ptr()),
+                                        off.ctypes.data_as(ctypes.c_void_p), self.n_graphs,
+                                        ctypes.c_void_p(out.data_ptr())))
+        return out, total.value

@@ -129,6 +129,48 @@ extern "C" int hn_graph_adjacency_hash(hn_graph_t* g, uint64_t* hash) {
     HN_API_END
 }
 
+// out[i] = sum of values[off[i] .. off[i+1]), a CTA per range (per-graph
+// sums of per-vertex counts over a batch of graphs laid out side by side).
+__global__ void __launch_bounds__(256)
+k_segment_sum_u64(const unsigned long long* __restrict__ values,
+                  const long long* __restrict__ off, long long nseg,
+                  unsigned long long* __restrict__ out) {
+    __shared__ unsigned long long wsum[8];
+    for (long long sg = blockIdx.x; sg < nseg; sg += gridDim.x) {
+        unsigned long long acc = 0;
+        for (long long i = off[sg] + threadIdx.x; i < off[sg + 1]; i += 256) acc += values[i];
+#pragma unroll
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+        if ((threadIdx.x & 31) == 0) wsum[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long t = 0;
+            for (int w = 0; w < 8; w++) t += wsum[w];
+            out[sg] = t;
+        }
+        __syncthreads();
+    }
+}
+
+extern "C" int hn_segment_sum_u64(hn_graph_t* g, const uint64_t* values, const int64_t* off,
+                                  int64_t nseg, uint64_t* out) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && (nseg == 0 || (values && off && out)) && nseg >= 0, "null argument");
+    if (nseg == 0) return HN_OK;
+    for (int64_t i = 0; i < nseg; i++)
+        HN_REQUIRE(off[i] >= 0 && off[i] <= off[i + 1], "ranges must be increasing");
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    DevBuf<long long> d_off((size_t)nseg + 1, s);
+    HN_CUDA(cudaMemcpyAsync(d_off.get(), off, sizeof(long long) * (nseg + 1),
+                            cudaMemcpyHostToDevice, s));
+    HN_LAUNCH(k_segment_sum_u64, grid_for(g, nseg, 1, 16), 256, 0, s,
+              (const unsigned long long*)values, (const long long*)d_off.get(), (long long)nseg,
+              (unsigned long long*)out);
+    HN_CUDA(cudaStreamSynchronize(s));
+    HN_API_END
+}
+
 extern "C" int hn_gather_int32(hn_graph_t* g, const int32_t* src, const int64_t* idx, int64_t n,
                                int32_t* out) {
     HN_API_BEGIN

@@ -216,6 +216,12 @@ int hn_graph_view_refresh(hn_graph_t* view);
  * distances) and host index / output arrays, on g's stream. */
 int hn_gather_int32(hn_graph_t* g, const int32_t* src, const int64_t* idx, int64_t n,
                     int32_t* out);
+/* out[i] = sum of values[off[i] .. off[i+1]) for i < nseg: device uint64
+ * values and out, host ranges (nseg + 1 increasing offsets), on g's stream
+ * (synchronised).  Per-graph sums of per-vertex counts for a batch of graphs
+ * laid out side by side (hn_tc_owner's counts over a disjoint union). */
+int hn_segment_sum_u64(hn_graph_t* g, const uint64_t* values, const int64_t* off, int64_t nseg,
+                       uint64_t* out);
 
 /* ---- queries (hornet/include/Core/Hornet.cuh:113-127,
  *               HornetOperations/HornetQuery.i.cuh) ------------------------ */
