@@ -98,6 +98,7 @@ _SIGNATURES = {
     "hn_graph_view_refresh": [_P],
     "hn_gather_int32": [_P, _P, _P, _I64, _P],
     "hn_segment_sum_u64": [_P, _P, _P, _I64, _P],
+    "hn_read_bandwidth": [_P, _P, _I64, ctypes.c_int32, _P],
     "hn_batch_create": [_P, _I64, _P, _P, _INT, _P],
     "hn_batch_reset": [_P, _I64, _P, _P, _INT],
     "hn_batch_size": [_P, _P],

@@ -171,6 +171,57 @@ extern "C" int hn_segment_sum_u64(hn_graph_t* g, const uint64_t* values, const i
     HN_API_END
 }
 
+// Read bandwidth of a buffer that stays in L2: every CTA streams the whole
+// buffer `reps` times with 16-byte loads (rotated by CTA so that CTAs do not
+// walk in step); the XOR of everything read is kept so that no load is
+// dropped.
+__global__ void __launch_bounds__(256)
+k_read_probe(const int4* __restrict__ buf, long long n16, int reps,
+             unsigned* __restrict__ sink) {
+    unsigned acc = 0;
+    const long long per = n16 / gridDim.x;   // this CTA's share of one pass
+    const long long first = (long long)blockIdx.x * per;
+    for (int r = 0; r < reps; r++) {
+        const long long start = (first + (long long)r * per) % n16;
+        for (long long i = threadIdx.x; i < per; i += 256) {
+            long long j = start + i;
+            if (j >= n16) j -= n16;
+            const int4 v = __ldcg(buf + j);
+            acc ^= (unsigned)(v.x ^ v.y ^ v.z ^ v.w);
+        }
+    }
+    if (acc == 0x9E3779B9u) atomicAdd(sink, 1u);
+}
+
+extern "C" int hn_read_bandwidth(hn_graph_t* g, const void* buf, int64_t bytes, int32_t reps,
+                                 double* gbs) {
+    HN_API_BEGIN
+    HN_REQUIRE(g && buf && gbs && bytes >= 16 * 256 && reps >= 1, "bad argument");
+    HN_REQUIRE(((uintptr_t)buf & 15) == 0, "buffer must be 16-byte aligned");
+    HN_CUDA(cudaSetDevice(g->device));
+    cudaStream_t s = g->stream;
+    const long long n16 = bytes / 16;
+    const long long grid = (long long)g->info.sms * 8;
+    DevBuf<unsigned> sink(1, s);
+    cudaEvent_t a, b;
+    HN_CUDA(cudaEventCreate(&a));
+    HN_CUDA(cudaEventCreate(&b));
+    // one pass to bring the buffer into L2, then the timed passes
+    HN_LAUNCH(k_read_probe, grid, 256, 0, s, (const int4*)buf, n16, 1, sink.get());
+    HN_CUDA(cudaEventRecord(a, s));
+    HN_LAUNCH(k_read_probe, grid, 256, 0, s, (const int4*)buf, n16, (int)reps, sink.get());
+    HN_CUDA(cudaEventRecord(b, s));
+    HN_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    HN_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    // each CTA reads per * reps 16-byte words
+    const double read = 16.0 * (double)(n16 / grid) * (double)grid * (double)reps;
+    *gbs = ms > 0 ? read / (ms * 1e-3) / 1e9 : 0.0;
+    HN_API_END
+}
+
 extern "C" int hn_gather_int32(hn_graph_t* g, const int32_t* src, const int64_t* idx, int64_t n,
                                int32_t* out) {
     HN_API_BEGIN

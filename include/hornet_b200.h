@@ -222,6 +222,12 @@ int hn_gather_int32(hn_graph_t* g, const int32_t* src, const int64_t* idx, int64
  * laid out side by side (hn_tc_owner's counts over a disjoint union). */
 int hn_segment_sum_u64(hn_graph_t* g, const uint64_t* values, const int64_t* off, int64_t nseg,
                        uint64_t* out);
+/* Measured read bandwidth (GB/s) of a device buffer of `bytes` (16-byte
+ * aligned, at least 4 KB) read `reps` times after a first pass: a buffer that
+ * fits in L2 gives the L2 read bandwidth that L2-served kernels (the
+ * triangle count's list intersections) are measured against.  Diagnostic;
+ * synchronises g's stream. */
+int hn_read_bandwidth(hn_graph_t* g, const void* buf, int64_t bytes, int32_t reps, double* gbs);
 
 /* ---- queries (hornet/include/Core/Hornet.cuh:113-127,
  *               HornetOperations/HornetQuery.i.cuh) ------------------------ */
