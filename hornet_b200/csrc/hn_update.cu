@@ -743,7 +743,7 @@ k_scatter_big(const int32_t* __restrict__ big_list, int nbig, const int32_t* __r
 
 // Batch edges -> their slot in the merged list (insert only; after the old
 // entries have moved): rank among the vertex's kept batch entries + the old
-// entries <= it (capos, recorded by k_mark_insert before any list moved).
+// entries <= it (capos, recorded at marking before any list moved).
 __global__ void k_scatter_new(const int32_t* __restrict__ cdst, const int32_t* __restrict__ cseg,
                               const int32_t* __restrict__ capos,
                               const long long* __restrict__ totals,
