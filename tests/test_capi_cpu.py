@@ -98,3 +98,20 @@ def test_no_device_reports_cuda_error_without_exiting():
     with pytest.raises(H.HornetError) as ei:
         H.Hornet(H.HornetInit(2, 2, off, adj))
     assert ei.value.code in (H.HN_ERR_CUDA, H.HN_ERR_OOM)
+
+
+def test_oracle_generator_equals_library_generator_for_update_batches():
+    """The reference GPU update run (oracle/run_ref_gpu.py) draws the
+    dynamic-update configuration's R-MAT batches with the oracle's
+    generator; they equal the benchmark's, drawn with the library's."""
+    import types
+    import bench
+    from oracle import oracle as O
+    for kind, b, seed in (("uniform", 10000, 77), ("rmat", 10000, 78), ("rmat", 4001, 80)):
+        r1 = np.random.default_rng(2024)
+        r2 = np.random.default_rng(2024)
+        a = bench.c3_batch(H, r1, kind, b, 1 << 20, 20, seed)
+        o = bench.c3_batch(types.SimpleNamespace(gen_rmat_host=O.gen_rmat), r2, kind, b,
+                           1 << 20, 20, seed)
+        np.testing.assert_array_equal(a[0], o[0])
+        np.testing.assert_array_equal(a[1], o[1])
