@@ -155,17 +155,49 @@ k_rs_pass(const unsigned long long* __restrict__ kin, const uint32_t* __restrict
             wcnt[ww][d] = (unsigned short)cnt;
             cnt += c;
         }
-        // publish the counts, then look back for the earlier tiles' counts
-        unsigned long long* my = status + (long long)tile * kBins + d;
+        // publish the counts now; the look-back for the earlier tiles'
+        // counts waits until this tile's keys are reordered, so that the
+        // tiles before it have had that long to publish theirs
+        *(volatile unsigned long long*)(status + (long long)tile * kBins + d) =
+            (tile == 0 ? kFlagIncl : kFlagAgg) | cnt;
+        // this tile's digit starts (exclusive scan of cnt over d) and the
+        // digits' bases in the output (exclusive scan of the pass histogram)
+        tot = ss->ghist[pass][d];
+        ci = warp_incl(cnt, lane);
+        ti = warp_incl(tot, lane);
+        if (lane == 31) {
+            s_wsum[w] = ci;
+            s_bsum[w] = ti;
+        }
+    }
+    __syncthreads();
+    unsigned tpre = 0;
+    if (d < kBins) {
+        unsigned cpre = 0;
+        for (int ww = 0; ww < w; ww++) {
+            cpre += s_wsum[ww];
+            tpre += s_bsum[ww];
+        }
+        s_start[d] = cpre + ci - cnt;
+    }
+    __syncthreads();
+    // reorder in shared memory
+#pragma unroll
+    for (int r = 0; r < kOsIpt; r++) {
+        if (t0 + r * 32 + lane < n) {
+            const unsigned dd = digit_of(k[r], shift);
+            const unsigned at = s_start[dd] + wcnt[w][dd] + rank[r];
+            skey[at] = k[r];
+            if (VALS) sval[at] = v[r];
+        }
+    }
+    if (d < kBins) {
         bool fail = false;
-        if (tile == 0) {
-            *(volatile unsigned long long*)my = kFlagIncl | cnt;
-        } else {
-            *(volatile unsigned long long*)my = kFlagAgg | cnt;
+        if (tile > 0) {
             // kLook statuses read at once (tiles j, j-1, ...), consumed in
-            // order up to the first inclusive one, or up to the first that is
-            // not ready, which is then polled; tile 0 is always inclusive,
-            // so the walk never passes it
+            // order up to the first inclusive one, or up to the first that
+            // is not ready, which is then polled; tile 0 is always
+            // inclusive, so the walk never passes it
             long long j = tile - 1;
             long long polls = 0;
             bool done = false;
@@ -196,27 +228,10 @@ k_rs_pass(const unsigned long long* __restrict__ kin, const uint32_t* __restrict
                     __nanosleep(32);
                 }
             }
-            *(volatile unsigned long long*)my = kFlagIncl | (excl + cnt);
+            *(volatile unsigned long long*)(status + (long long)tile * kBins + d) =
+                kFlagIncl | (excl + cnt);
         }
         if (fail) s_fail = 1;
-        // this tile's digit starts (exclusive scan of cnt over d) and the
-        // digits' bases in the output (exclusive scan of the pass histogram)
-        tot = ss->ghist[pass][d];
-        ci = warp_incl(cnt, lane);
-        ti = warp_incl(tot, lane);
-        if (lane == 31) {
-            s_wsum[w] = ci;
-            s_bsum[w] = ti;
-        }
-    }
-    __syncthreads();
-    if (d < kBins) {
-        unsigned cpre = 0, tpre = 0;
-        for (int ww = 0; ww < w; ww++) {
-            cpre += s_wsum[ww];
-            tpre += s_bsum[ww];
-        }
-        s_start[d] = cpre + ci - cnt;
         s_out[d] = tpre + ti - tot + (unsigned)excl;
     }
     __syncthreads();
@@ -224,17 +239,6 @@ k_rs_pass(const unsigned long long* __restrict__ kin, const uint32_t* __restrict
         if (threadIdx.x == 0) atomicExch(err, HN_ERR_TIMEOUT);
         return;
     }
-    // reorder in shared memory
-#pragma unroll
-    for (int r = 0; r < kOsIpt; r++) {
-        if (t0 + r * 32 + lane < n) {
-            const unsigned dd = digit_of(k[r], shift);
-            const unsigned at = s_start[dd] + wcnt[w][dd] + rank[r];
-            skey[at] = k[r];
-            if (VALS) sval[at] = v[r];
-        }
-    }
-    __syncthreads();
     const long long rem = n - (long long)tile * TILE;
     const int tile_n = rem < TILE ? (int)rem : TILE;
     for (int j = threadIdx.x; j < tile_n; j += NT) {
