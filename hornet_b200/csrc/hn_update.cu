@@ -466,9 +466,10 @@ k_scatter_old(const long long* __restrict__ prefix, long long nseg,
                 to[k] = s_new[b] + e + s_kb[b] + lower_bound32(B, nb, x);
             } else {
                 // every batch copy of x lies inside the narrowed range
-                long long ubl = upper_bound32(B, nb, x);
-                long long lbl = ubl;
-                if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound32(B, (int)ubl, x);
+                // batch entries below x, then its copies (few): one search
+                const long long lbl = lower_bound32(B, nb, x);
+                long long ubl = lbl;
+                while (ubl < nb && B[ubl] == x) ubl++;
                 long long cnt = ubl - lbl;  // copies of x to delete
                 bool keep = true;
                 if (cnt > 0) {
@@ -525,9 +526,9 @@ k_inplace_span(const int32_t* __restrict__ span_list, const int* __restrict__ ns
             if (INSERT) {
                 pool[off + j + lower_bound32(B, nb, x)] = x;
             } else {
-                const int ubl = upper_bound32(B, nb, x);
-                int lbl = ubl;
-                if (ubl > 0 && B[ubl - 1] == x) lbl = lower_bound32(B, ubl, x);
+                const int lbl = lower_bound32(B, nb, x);
+                int ubl = lbl;
+                while (ubl < nb && B[ubl] == x) ubl++;
                 bool keep = true;
                 if (ubl > lbl) {
                     int first = j;
@@ -725,9 +726,9 @@ k_scatter_big(const int32_t* __restrict__ big_list, int nbig, const int32_t* __r
                 if (INSERT) {
                     pool[h.new_off + r + lo + lower_bound32(Bn, m, x)] = x;
                 } else {
-                    const int ubl = upper_bound32(Bn, m, x);
-                    int lbl = ubl;
-                    if (ubl > 0 && Bn[ubl - 1] == x) lbl = lower_bound32(Bn, ubl, x);
+                    const int lbl = lower_bound32(Bn, m, x);
+                    int ubl = lbl;
+                    while (ubl < m && Bn[ubl] == x) ubl++;
                     const int cnt = ubl - lbl;   // copies of x this batch deletes
                     // the first cnt copies of x go: keep this one if its rank
                     // among the old copies (from the first copy's slot,
