@@ -550,13 +550,7 @@ void ensure_free_list(hn_graph* g, int c, long long count) {
 void degree_prefix(hn_graph* g, const int32_t* verts, int32_t n, long long* prefix) {
     HN_LAUNCH(k_degrees, grid_for(g, (long long)n + 1, 256), 256, 0, g->stream, g->vtab, verts,
               n, prefix);
-    size_t tb = 0;
-    HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, prefix, prefix, (long long)n + 1,
-                                          g->stream));
-    DevBuf<char> tmp(tb, g->stream);
-    HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, prefix, prefix, (long long)n + 1,
-                                          g->stream));
-    count_launch();
+    exclusive_scan(g, (const long long*)prefix, prefix, (long long)n + 1, g->stream);
 }
 
 void lb_splits(hn_graph* g, const long long* prefix, long long nseg, long long max_total,

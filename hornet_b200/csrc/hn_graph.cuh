@@ -231,6 +231,12 @@ void radix_sort_u64(hn_graph* g, unsigned long long*& keys, unsigned long long*&
                     uint32_t*& vals, uint32_t*& vals_alt, long long n, int bits, int* err,
                     cudaStream_t s);
 
+// out[i] = in[0] + ... + in[i-1] (out may be in), on stream s, in OutT.
+// Defined in hn_scan.cu for (int, int), (int, long long), (long long,
+// long long) and (unsigned long long, unsigned long long).
+template <typename InT, typename OutT>
+void exclusive_scan(hn_graph* g, const InT* in, OutT* out, long long n, cudaStream_t s);
+
 // Update entry points call this: a query view never changes the graph.
 inline void require_owner(const hn_graph* g) {
     if (g->parent) throw Error(HN_ERR_STATE, "a query view cannot update the graph");

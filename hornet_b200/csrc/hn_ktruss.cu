@@ -406,12 +406,8 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
             HN_CUDA(cub::DeviceSegmentedReduce::Sum(tmp.get(), tb, cflag.get(), noff.get(), nV,
                                                     loff, loff + 1, s));
             HN_CUDA(cudaMemsetAsync(noff.get() + nV, 0, sizeof(long long), s));
-            tb = 0;
-            HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, noff.get(), noff.get(), nV + 1, s));
-            DevBuf<char> tmp2(tb, s);
-            HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp2.get(), tb, noff.get(), noff.get(), nV + 1,
-                                                  s));
-            count_launch(2);
+            count_launch();
+            exclusive_scan(g, (const long long*)noff.get(), noff.get(), (long long)nV + 1, s);
         }
         DevBuf<int32_t> nadj((size_t)keep + 1, s), ncanon((size_t)keep + 1, s);
         {
@@ -619,13 +615,7 @@ extern "C" int hn_ktruss_keep(hn_graph_t* g, int32_t K, int32_t* max_k, int64_t*
     int rc = hn_graph_export_coo(g, 1, src.get(), dst.get(), HN_MEM_DEVICE);
     if (rc != HN_OK) return rc;
     HN_LAUNCH(k_kt_below, grid_for(g, m, kB), kB, 0, s, truss.get(), m, K, flag.get());
-    {
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag.get(), pos.get(), (int)m, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, flag.get(), pos.get(), (int)m, s));
-        count_launch();
-    }
+    exclusive_scan(g, (const int32_t*)flag.get(), pos.get(), m, s);
     DevBuf<int32_t> esrc((size_t)m, s), edst((size_t)m, s);
     long long* total = (long long*)(g->d_scalar + 6);
     HN_LAUNCH(k_kt_gather, grid_for(g, m, kB), kB, 0, s, flag.get(), pos.get(), src.get(),

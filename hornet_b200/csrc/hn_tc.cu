@@ -773,13 +773,7 @@ void build_oriented(hn_graph* g, Oriented& o, const int32_t* canon) {
     lb_splits(g, o.prefix.get(), nV, m, Tile::TILE, splits);
     HN_LAUNCH(k_orient_flags, grid, kB, 0, s, o.prefix.get(), nV, g->vtab, g->pool, pos.get(),
               splits.get(), (long long)splits.n - 1);
-    {
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, pos.get(), pos.get(), (int)(m + 1), s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, pos.get(), pos.get(), (int)(m + 1), s));
-        count_launch();
-    }
+    exclusive_scan(g, (const int32_t*)pos.get(), pos.get(), m + 1, s);
     o.offp.alloc((size_t)nV + 1, s);
     o.fwd.alloc((size_t)(m + 4), s);
     if (canon) o.feid.alloc((size_t)(m + 4), s);
@@ -804,13 +798,7 @@ void build_candidates(hn_graph* g, const Oriented& o, DevBuf<long long>& coff,
     HN_LAUNCH(k_cand<false>, grid, kB, 0, s, o.offp.get(), nV, o.fwd.get(), cnt.get(),
               (const long long*)nullptr, (int32_t*)nullptr, splits.get(), (long long)splits.n - 1,
               (const int32_t*)nullptr, (int32_t*)nullptr);
-    {
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, cnt.get(), coff.get(), nV + 1, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, cnt.get(), coff.get(), nV + 1, s));
-        count_launch();
-    }
+    exclusive_scan(g, (const int*)cnt.get(), coff.get(), (long long)nV + 1, s);
     HN_CUDA(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * ((size_t)nV + 1), s));
     if (ceid) ceid->alloc((size_t)m + 4, s);
     HN_LAUNCH(k_cand<true>, grid, kB, 0, s, o.offp.get(), nV, o.fwd.get(), cnt.get(),

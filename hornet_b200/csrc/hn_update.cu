@@ -983,14 +983,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
                   g->pool, val, apos.get(), (const AllocState*)st);
     // 3. scan + compact
     DevBuf<unsigned long long> scan(n, s);
-    {
-        ProfileScope ps("cub_scan_keep", s);
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, val, scan.get(), (int)n, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, val, scan.get(), (int)n, s));
-        count_launch();
-    }
+    exclusive_scan(g, (const unsigned long long*)val, scan.get(), n, s);
     DevBuf<int32_t> cdst(n, s), cseg(n, s), seg_u(n, s), seg_kstart(n + 1, s), seg_ncap(n, s),
         seg_base(n, s);
     DevBuf<long long> seg_work(n + 1, s), seg_new_off(n, s), seg_old_off(n, s);
@@ -1069,16 +1062,7 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
               (long long* const*)g->d_fl, st, (const long long*)seg_old_off.get(),
               seg_new_off.get());
     // 7. scatter-merge
-    {
-        ProfileScope ps("cub_scan_work", s);
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, seg_work.get(), seg_work.get(),
-                                              (int)(nseg + 1), s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, seg_work.get(), seg_work.get(),
-                                              (int)(nseg + 1), s));
-        count_launch();
-    }
+    exclusive_scan(g, (const long long*)seg_work.get(), seg_work.get(), nseg + 1, s);
     // tiles are read from the device prefix; the grid is persistent
     // five CTAs per SM (the shared-memory limit of the tile): each tile waits
     // on a short chain of dependent loads, so more resident tiles hide it
@@ -1092,16 +1076,8 @@ void run_update(hn_graph* g, hn_batch* b, unsigned flags, bool insert, int64_t* 
         HN_LAUNCH(k_big_chunks, grid_for(g, (long long)nbig + 1, kB), kB, 0, s, big_list.get(),
                   nbig, seg_u.get(), seg_kstart.get(), seg_ncap.get(), seg_base.get(),
                   seg_old_off.get(), seg_new_off.get(), g->vtab, chunk_pre.get());
-        {
-            ProfileScope ps("cub_scan_big", s);
-            size_t tb = 0;
-            HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, chunk_pre.get(), chunk_pre.get(),
-                                                  nbig + 1, s));
-            DevBuf<char> tmp(tb, s);
-            HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, chunk_pre.get(), chunk_pre.get(),
-                                                  nbig + 1, s));
-            count_launch();
-        }
+        exclusive_scan(g, (const unsigned long long*)chunk_pre.get(), chunk_pre.get(),
+                       (long long)nbig + 1, s);
         const long long grid_big = (long long)g->info.sms * 8;
         if (snap_words > 0) {
             snap.alloc((size_t)snap_words, s);
@@ -1418,13 +1394,7 @@ int hn_update_coalesced(hn_graph_t* g, int64_t n, const int32_t* src, const int3
     HN_LAUNCH(k_net_mark, grid_for(g, n, kB), kB, 0, s, keys.get(), ops1.get(), n, val,
               (const AllocState*)st);
     DevBuf<unsigned long long> scan((size_t)n, s);
-    {
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, val, scan.get(), (int)n, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), tb, val, scan.get(), (int)n, s));
-        count_launch();
-    }
+    exclusive_scan(g, (const unsigned long long*)val, scan.get(), n, s);
     hn_batch bi, bd;
     bi.g = bd.g = g;
     bi.device = bd.device = g->device;
