@@ -20,8 +20,6 @@
 // surviving edge sets, truss numbers and max_K are those of the reference
 // loop.  Edge ids are positions in the sorted CSR; undirected edge state
 // lives on the (u < v) position.
-#include <cub/cub.cuh>
-
 #include <optional>
 
 #include <algorithm>
@@ -103,6 +101,28 @@ __global__ void k_kt_live_pos(const int32_t* __restrict__ canon, long long n,
     for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x)
         flag[p] = alive[canon[p]] ? 1 : 0;
+}
+
+// List shrinking: a vertex's new offset is the new slot of its first old
+// entry (noff[v] = pos[off[v]], v = 0..nV), and every live entry moves to
+// its new slot, in order.
+__global__ void k_kt_shrink_off(const long long* __restrict__ off, int nV,
+                                const long long* __restrict__ pos, long long* __restrict__ noff) {
+    for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v <= nV;
+         v += (long long)gridDim.x * blockDim.x)
+        noff[v] = pos[off[v]];
+}
+
+__global__ void k_kt_shrink_copy(const int32_t* __restrict__ adj, const int32_t* __restrict__ canon,
+                                 const int32_t* __restrict__ flag, const long long* __restrict__ pos,
+                                 long long m, int32_t* __restrict__ nadj,
+                                 int32_t* __restrict__ ncanon) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+         i += (long long)gridDim.x * blockDim.x)
+        if (flag[i]) {
+            nadj[pos[i]] = adj[i];
+            ncanon[pos[i]] = canon[i];
+        }
 }
 
 // Frontier of round K: alive edges of the list L with support < K - 2.
@@ -394,34 +414,20 @@ int ktruss_run(hn_graph* g, int32_t* d_edge_truss) {
     auto shrink_lists = [&]() {
         const long long keep = 2LL * n_alive;
         if (keep * 2 > lm) return;
-        cflag.alloc((size_t)lm, s);
+        cflag.alloc((size_t)lm + 1, s);
+        HN_CUDA(cudaMemsetAsync(cflag.get() + lm, 0, sizeof(int32_t), s));
         HN_LAUNCH(k_kt_live_pos, grid_for(g, lm, kB), kB, 0, s, (const int32_t*)lcanon, lm,
                   alive.get(), cflag.get());
-        DevBuf<long long> noff((size_t)nV + 1, s);
-        {
-            size_t tb = 0;
-            HN_CUDA(cub::DeviceSegmentedReduce::Sum(nullptr, tb, cflag.get(), noff.get(), nV, loff,
-                                                    loff + 1, s));
-            DevBuf<char> tmp(tb, s);
-            HN_CUDA(cub::DeviceSegmentedReduce::Sum(tmp.get(), tb, cflag.get(), noff.get(), nV,
-                                                    loff, loff + 1, s));
-            HN_CUDA(cudaMemsetAsync(noff.get() + nV, 0, sizeof(long long), s));
-            count_launch();
-            exclusive_scan(g, (const long long*)noff.get(), noff.get(), (long long)nV + 1, s);
-        }
+        // new slot of every live entry: an exclusive scan of the live flags;
+        // a vertex's new offset is the new slot of its first old entry
+        DevBuf<long long> pos((size_t)lm + 1, s), noff((size_t)nV + 1, s);
+        exclusive_scan(g, (const int32_t*)cflag.get(), pos.get(), lm + 1, s);
         DevBuf<int32_t> nadj((size_t)keep + 1, s), ncanon((size_t)keep + 1, s);
-        {
-            int* nsel = cnt + 6;
-            size_t tb = 0;
-            HN_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, ladj, cflag.get(), nadj.get(), nsel,
-                                               lm, s));
-            DevBuf<char> tmp(tb, s);
-            HN_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, ladj, cflag.get(), nadj.get(), nsel,
-                                               lm, s));
-            HN_CUDA(cub::DeviceSelect::Flagged(tmp.get(), tb, lcanon, cflag.get(), ncanon.get(),
-                                               nsel, lm, s));
-            count_launch(2);
-        }
+        HN_LAUNCH(k_kt_shrink_off, grid_for(g, (long long)nV + 1, kB), kB, 0, s,
+                  (const long long*)loff, nV, (const long long*)pos.get(), noff.get());
+        HN_LAUNCH(k_kt_shrink_copy, grid_for(g, lm, kB), kB, 0, s, (const int32_t*)ladj,
+                  (const int32_t*)lcanon, (const int32_t*)cflag.get(), (const long long*)pos.get(),
+                  lm, nadj.get(), ncanon.get());
         coff = std::move(noff);
         cadj = std::move(nadj);
         ccanon = std::move(ncanon);
