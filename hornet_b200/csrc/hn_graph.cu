@@ -148,6 +148,36 @@ __device__ __forceinline__ int pow2_ceil_int(int d) {
 }
 
 // Degrees, capacities and the class histogram.
+// Sorting an unsorted CSR's lists: the row of entry i is the number of
+// vertices v >= 1 whose list starts at or before i, an inclusive scan of the
+// row-start marks; entries become keys row << L | neighbour, which the
+// batch radix sort orders (stably, weights carried), and the neighbours
+// are read back out of the sorted keys.
+__global__ void k_row_marks(const long long* __restrict__ off, int nV, long long nE,
+                            int* __restrict__ mark) {
+    for (long long v = 1 + blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
+         v += (long long)gridDim.x * blockDim.x)
+        if (off[v] < nE) atomicAdd(mark + off[v], 1);
+}
+
+__global__ void k_csr_keys(const int* __restrict__ mark, const int* __restrict__ rows_excl,
+                           const int32_t* __restrict__ adj, long long nE, int L,
+                           unsigned long long* __restrict__ keys) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nE;
+         i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long row = (unsigned)(rows_excl[i] + mark[i]);
+        keys[i] = (row << L) | (unsigned)adj[i];
+    }
+}
+
+__global__ void k_keys_dst(const unsigned long long* __restrict__ keys, long long nE, int L,
+                           int32_t* __restrict__ adj) {
+    const unsigned long long mask = (1ull << L) - 1;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nE;
+         i += (long long)gridDim.x * blockDim.x)
+        adj[i] = (int32_t)(keys[i] & mask);
+}
+
 __global__ void k_class_hist(const long long* __restrict__ off, int nV, VRec* vtab,
                              AllocState* st) {
     for (long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x; v < nV;
@@ -615,7 +645,46 @@ void build_from_csr(hn_graph* g, int32_t nV, int64_t nE, const long long* d_off,
     const uint32_t* src_w = d_w;
     DevBuf<int32_t> sorted_adj;
     DevBuf<uint32_t> sorted_w;
-    if (!sorted && nE > 0 && d_w) {
+    if (!sorted && nE > 0 && nE < (1ll << 32) && nV > 1) {
+        // the library's radix sort over (row, neighbour) keys; weights carried
+        const int L = g->key_bits;
+        DevBuf<int> mark((size_t)nE, s), rows((size_t)nE, s);
+        HN_CUDA(cudaMemsetAsync(mark.get(), 0, sizeof(int) * (size_t)nE, s));
+        HN_LAUNCH(k_row_marks, grid_for(g, nV, 256), 256, 0, s, d_off, nV, (long long)nE,
+                  mark.get());
+        exclusive_scan(g, (const int*)mark.get(), rows.get(), (long long)nE, s);
+        DevBuf<unsigned long long> keys((size_t)nE, s), keys2((size_t)nE, s);
+        HN_LAUNCH(k_csr_keys, grid_for(g, nE, 256), 256, 0, s, (const int*)mark.get(),
+                  (const int*)rows.get(), d_adj, (long long)nE, L, keys.get());
+        mark.release();
+        rows.release();
+        DevBuf<uint32_t> w2;
+        if (d_w) {
+            sorted_w.alloc((size_t)nE, s);
+            w2.alloc((size_t)nE, s);
+            HN_CUDA(cudaMemcpyAsync(sorted_w.get(), d_w, sizeof(uint32_t) * (size_t)nE,
+                                    cudaMemcpyDeviceToDevice, s));
+        }
+        unsigned long long* kc = keys.get();
+        unsigned long long* ka = keys2.get();
+        uint32_t* vc = d_w ? sorted_w.get() : nullptr;
+        uint32_t* va = d_w ? w2.get() : nullptr;
+        HN_CUDA(cudaMemsetAsync(&g->alloc->error, 0, sizeof(int), s));
+        radix_sort_u64(g, kc, ka, vc, va, (long long)nE, 2 * L, &g->alloc->error, s);
+        if (d_w && vc != sorted_w.get()) std::swap(sorted_w.p, w2.p);
+        sorted_adj.alloc((size_t)nE, s);
+        HN_LAUNCH(k_keys_dst, grid_for(g, nE, 256), 256, 0, s, (const unsigned long long*)kc,
+                  (long long)nE, L, sorted_adj.get());
+        HN_CUDA(cudaMemcpyAsync(&g->h_alloc->error, &g->alloc->error, sizeof(int),
+                                cudaMemcpyDeviceToHost, s));
+        HN_CUDA(cudaStreamSynchronize(s));
+        if (g->h_alloc->error) {
+            HN_CUDA(cudaMemsetAsync(&g->alloc->error, 0, sizeof(int), s));
+            throw Error(HN_ERR_TIMEOUT, "adjacency sort: a bounded wait gave up");
+        }
+        src_adj = sorted_adj.get();
+        if (d_w) src_w = sorted_w.get();
+    } else if (!sorted && nE > 0 && d_w) {
         // weights follow their edges; equal neighbours keep their input order
         sorted_adj.alloc((size_t)nE, s);
         sorted_w.alloc((size_t)nE, s);

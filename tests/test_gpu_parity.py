@@ -60,6 +60,35 @@ def test_construct_unsorted_input_is_sorted():
     assert_same_graph(h, g)
 
 
+def test_construct_unsorted_large_multigraph():
+    """A larger unsorted CSR (2^17 vertices: five 8-bit sort passes over
+    34-bit keys), with empty lists first, in the middle and last, a hub, and
+    repeated neighbours: the lists come out sorted, multiplicities kept."""
+    rng = np.random.default_rng(4)
+    nV = 1 << 17
+    s, d = H.gen_rmat_host(16, 400_000, 3)
+    s = s.astype(np.int64) + 5          # vertices 0..4 empty
+    d = d.astype(np.int32) + 5
+    keep = (s < nV - 7) & (s != 40000)  # the last 7 and vertex 40000 empty
+    s, d = s[keep], d[keep]
+    dup = rng.choice(len(s), 20000)
+    s = np.concatenate([s, s[dup]])
+    d = np.concatenate([d, d[dup]])
+    order = np.argsort(s, kind="stable")   # grouped by source, neighbours unsorted
+    s, d = s[order], d[order]
+    off = np.zeros(nV + 1, np.int64)
+    np.add.at(off, s + 1, 1)
+    off = np.cumsum(off)
+    for v in rng.choice(nV, 50, replace=False):   # shuffle some lists more
+        a, b = off[v], off[v + 1]
+        rng.shuffle(d[a:b])
+    h = H.Hornet(H.HornetInit(nV, len(d), off.astype(np.int32), d, sorted_adjacency=False))
+    hs, hd = h.getCOO(True)
+    ref = np.lexsort((d, s))
+    np.testing.assert_array_equal(hs, s[ref])
+    np.testing.assert_array_equal(hd, d[ref])
+
+
 def test_construct_with_isolated_and_empty():
     # vertices 0, 5, 9 isolated
     s = np.array([1, 2, 3, 6, 7], np.int32)
