@@ -13,7 +13,6 @@
 // (xlib/src/Graph/GraphStd.cpp:174-206): mirror every pair, drop self
 // loops, sort, remove duplicates — as one radix sort of packed keys, one
 // unique pass and one offsets pass on the device.
-#include <cub/cub.cuh>
 
 #include <algorithm>
 #include <thread>
@@ -119,6 +118,27 @@ __global__ void k_sym_keys(const int32_t* __restrict__ src, const int32_t* __res
     }
 }
 
+// mark[i] = 1 where a run of equal sorted keys starts.
+__global__ void k_run_starts(const unsigned long long* __restrict__ k, long long n,
+                             int* __restrict__ mark) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        mark[i] = i == 0 || k[i] != k[i - 1];
+}
+
+// The first key of each run to its slot (pos: the exclusive scan of the
+// run starts); the run count to *nsel.
+__global__ void k_keep_run_starts(const unsigned long long* __restrict__ k, long long n,
+                                  const int* __restrict__ pos, unsigned long long* __restrict__ out,
+                                  long long* __restrict__ nsel) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const bool head = i == 0 || k[i] != k[i - 1];
+        if (head) out[pos[i]] = k[i];
+        if (i == n - 1) *nsel = (long long)pos[i] + (head ? 1 : 0);
+    }
+}
+
 __global__ void k_csr_from_keys(const unsigned long long* __restrict__ keys, long long m, int nV,
                                 int S, int32_t* __restrict__ off, int32_t* __restrict__ adj) {
     const unsigned long long mask = (1ull << S) - 1;
@@ -196,30 +216,37 @@ int hn_coo_to_csr_device(int32_t nV, int64_t np, const int32_t* src, const int32
     HN_CUDA(cudaMemsetAsync(err.get(), 0, 2 * sizeof(int), s));
     long long grid = std::min<long long>((np + 255) / 256, (long long)sms * 16);
     HN_LAUNCH(k_sym_keys, grid, 256, 0, s, src, dst, (long long)np, nV, S, k1.get(), err.get());
-    cub::DoubleBuffer<unsigned long long> db(k1.get(), k2.get());
+    // the library's radix sort (the sentinel of a self loop has every key
+    // bit set, so it sorts last), then the first key of every run of equal
+    // keys kept: its slot is an exclusive scan of the run-start marks
+    unsigned long long* sorted = k1.get();
+    unsigned long long* alt = k2.get();
     {
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)n2, 0, 2 * S, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceRadixSort::SortKeys(tmp.get(), tb, db, (int)n2, 0, 2 * S, s));
-        count_launch();
+        uint32_t* nv = nullptr;
+        uint32_t* nva = nullptr;
+        radix_sort_u64(nullptr, sorted, alt, nv, nva, n2, 2 * S, err.get() + 1, s);
     }
-    unsigned long long* sorted = db.Current();
-    unsigned long long* uniq = db.Alternate();
+    unsigned long long* uniq = alt;
     DevBuf<long long> nsel(1, s);
-    {
-        size_t tb = 0;
-        HN_CUDA(cub::DeviceSelect::Unique(nullptr, tb, sorted, uniq, nsel.get(), (int)n2, s));
-        DevBuf<char> tmp(tb, s);
-        HN_CUDA(cub::DeviceSelect::Unique(tmp.get(), tb, sorted, uniq, nsel.get(), (int)n2, s));
-        count_launch();
+    if (n2 > 0) {
+        DevBuf<int> mark((size_t)n2, s);
+        HN_LAUNCH(k_run_starts, grid, 256, 0, s, (const unsigned long long*)sorted, n2,
+                  mark.get());
+        exclusive_scan(nullptr, (const int*)mark.get(), mark.get(), n2, s);
+        HN_LAUNCH(k_keep_run_starts, grid, 256, 0, s, (const unsigned long long*)sorted, n2,
+                  (const int*)mark.get(), uniq, nsel.get());
+    } else {
+        HN_CUDA(cudaMemsetAsync(nsel.get(), 0, sizeof(long long), s));
     }
     long long nu = 0;
     int herr = 0;
     HN_CUDA(cudaMemcpyAsync(&nu, nsel.get(), sizeof(long long), cudaMemcpyDeviceToHost, s));
+    int herr2 = 0;
     HN_CUDA(cudaMemcpyAsync(&herr, err.get(), sizeof(int), cudaMemcpyDeviceToHost, s));
+    HN_CUDA(cudaMemcpyAsync(&herr2, err.get() + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
     HN_CUDA(cudaStreamSynchronize(s));
     if (herr) throw Error(HN_ERR_INVALID, "pair id outside [0, nV)");
+    if (herr2) throw Error(HN_ERR_TIMEOUT, "pair sort: a bounded wait gave up");
     unsigned long long last = 0;
     if (nu > 0) {
         HN_CUDA(cudaMemcpy(&last, uniq + nu - 1, sizeof(last), cudaMemcpyDeviceToHost));

@@ -226,7 +226,8 @@ namespace hn {
 // optional 32-bit values (vals may be null); the *_alt buffers are scratch
 // of the same size, and on return keys / vals point at the sorted data.
 // A bounded device wait that gave up stores HN_ERR_TIMEOUT in *err (device
-// memory).  Defined in hn_sort.cu.
+// memory).  g may be null (the current device is used).  Defined in
+// hn_sort.cu.
 void radix_sort_u64(hn_graph* g, unsigned long long*& keys, unsigned long long*& keys_alt,
                     uint32_t*& vals, uint32_t*& vals_alt, long long n, int bits, int* err,
                     cudaStream_t s);

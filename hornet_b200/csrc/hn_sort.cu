@@ -254,6 +254,15 @@ k_rs_pass(const unsigned long long* __restrict__ kin, const uint32_t* __restrict
         atomicAdd(&ss->ghist[pass + 1][d], s_next[d]);
 }
 
+// SMs of the graph's device, or of the current device without a graph.
+int sm_count(const hn_graph* g) {
+    if (g) return g->info.sms;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+
 }  // namespace
 
 // Sorts keys[0, n) by their low `bits` bits, stably, carrying vals (may be
@@ -277,7 +286,7 @@ void radix_sort_u64(hn_graph* g, unsigned long long*& keys, unsigned long long*&
     DevBuf<unsigned long long> status((size_t)ntiles * kBins, s);
     HN_CUDA(cudaMemsetAsync(ss.get(), 0, sizeof(SortState), s));
     const long long grid0 = std::min<long long>((n + kOsThreads - 1) / kOsThreads,
-                                                (long long)g->info.sms * 8);
+                                                (long long)sm_count(g) * 8);
     HN_LAUNCH(k_rs_hist0, grid0, kOsThreads, 0, s, keys, n, ss.get());
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
